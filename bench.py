@@ -1,0 +1,313 @@
+#!/usr/bin/env python3
+"""Benchmark of the batched isolated-route engine (fields + canonical paths).
+
+Workload (default): the congestion board — 512x512x4, 256 nets, directed edge
+prices, exact polygon outline, windows by net_window — one "step" routes every
+net of the batch (complete u32 fields over every window + canonical paths).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0.  `value` is whole-job nets/s with the board and nets
+resident in HBM (device time from CUDA events on the launching stream, L2
+flushed between steps, max over ranks); `e2e` is the same metric through the
+public call with host buffers (upload, solve, download of paths and costs).
+Under torchrun every rank routes its own net set on the same board (weak
+scaling; no collective on the data path).  `--impl reference` times the CPU
+restatement of the reference's own isolated search (window A*, full-board
+retry) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "metal-route_b200"))
+
+METRIC = "nets routed/sec & HBM GB/s (batched vs per-net, bit-exact); /solve p50/p99 ms"
+UNIT = "nets/s"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_per_launch(kernel_profile: str):
+    """Bytes per relax launch from the committed ncu summary, when present."""
+    path = os.path.join(ROOT, "profiles", kernel_profile)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return int(float(line.split(":", 1)[1].strip().split()[0]))
+    except OSError:
+        pass
+    return None
+
+
+def _workload(name: str, rank: int):
+    from mrcuda import workloads as W
+
+    if name == "plain":
+        return W.plain_board(seed=1 + 1000 * rank)
+    return W.congestion_board(seed=2, net_seed=None if rank == 0 else 2 + 1000 * rank)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _cpu_sample_rate(wl, n_sample: int, threads: int = 0):
+    """The oracle's A* alone-path search (window, then full board) on a sample of
+    nets, all host threads: nets/s.  Checker code only; never the measured GPU path."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from mrcuda.types import IsolatedRouteRequest
+
+    o = orc.get()
+    req = wl.request()
+    sub = IsolatedRouteRequest(req.grid, req.nets[:n_sample], req.windows[:n_sample], req.x_edge_costs,
+                               req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+    t0 = time.perf_counter()
+    o.isolated_batch(sub, retry_full=True, mode="astar", threads=threads)
+    dt = time.perf_counter() - t0
+    return n_sample / dt, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = _workload(args.workload, 0)
+    cores = os.cpu_count() or 1
+    n_sample = min(args.cpu_sample, len(wl.nets))
+    for _ in range(args.warmup):
+        _cpu_sample_rate(wl, max(n_sample // 4, 1))
+    rates = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        r, _ = _cpu_sample_rate(wl, n_sample)
+        rates.append(r)
+    wall = time.perf_counter() - t_all
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl.meta["workload"], "windows": wl.meta.get("windows")},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n_sample} of {len(wl.nets)} nets per step: A* alone-path search "
+                                   f"(window, then full board), {cores} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_engine(args):
+    import numpy as np
+    import torch
+
+    import mrcuda
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    wl = _workload(args.workload, rank)
+    eng = mrcuda.Engine(local)
+    board = eng.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
+    batch = mrcuda.Batch(board, wl.nets, wl.windows, retry_full=True, time_kernels=True)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    # warm-up (also checks that the batch completes without any status error)
+    first = None
+    for _ in range(max(args.warmup, 1)):
+        batch.launch(stream.cuda_stream)
+        stream.synchronize()
+        if first is None:
+            first = batch.finish()
+    path_cells = sum(len(p) for p in first.paths if p)
+    routed = sum(p is not None for p in first.paths)
+
+    # timed region: barrier + synchronize on both sides, per-step CUDA events
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms, relax_ms = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        batch.launch(stream.cuda_stream)
+        e.record(stream)
+        stream.synchronize()
+        step_ms.append(s.elapsed_time(e))
+        relax_ms.append(batch.relax_ms())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = statistics.fmean(step_ms)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = len(wl.nets) * world / (ms_max / 1000.0)
+
+    # end to end through the public call with host buffers
+    req = wl.request()
+    e2e_steps = max(1, min(args.steps, 5))
+    eng.route_isolated_batch(req)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        out = eng.route_isolated_batch(req)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = len(wl.nets) * world / float(e2e_t.item())
+    h2d = (wl.grid.cost.nbytes + (wl.grid.board_constraint.nbytes if wl.grid.board_constraint is not None else 0)
+           + (wl.directed.nbytes if wl.directed is not None else 0) + 4 * (len(wl.x) + len(wl.y) + len(wl.vias))
+           + len(wl.vias) + 40 * len(wl.nets) + 16 * len(wl.windows)
+           + 4 * sum(len(nt.passable_pads) + len(nt.via_passable_pads) for nt in wl.nets))
+    d2h = 8 * (len(wl.nets) + 1) + 4 * len(wl.nets) + 4 * sum(len(p) for p in out.paths if p) + 4
+    assert out.paths == first.paths, "end-to-end call disagrees with the resident batch"
+
+    # roofline of the dominant kernel (relax_tiles_kernel)
+    peak, peak_kind = _peaks()
+    alg_bytes = wl.window_cells() * wl.bytes_per_cell() + 4 * path_cells
+    relax_avg = statistics.fmean(relax_ms) if relax_ms and min(relax_ms) > 0 else ms
+    achieved = alg_bytes / (relax_avg / 1000.0) / 1e9
+    traffic = _traffic_per_launch(f"relax_tiles_{args.workload}.md")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl.meta["workload"], "nets_per_rank": len(wl.nets), "window_cells": wl.window_cells(),
+                   "routed": routed, "retried": first.retried, "l2": "flushed between steps (512 MiB write)",
+                   "windows": wl.meta.get("windows")},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": batch.kernel_launches * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "relax_tiles_kernel",
+                     "kernel_ms": relax_avg, "algorithmic_bytes_per_launch": int(alg_bytes),
+                     "bytes_per_cell": wl.bytes_per_cell()},
+        "clocks": clk,
+    }
+
+    if rank == 0 and world == 1 and not args.no_plain:
+        ps = min(args.plain_sample, len(wl.nets))
+        sub = mrcuda.IsolatedRouteRequest(req.grid, req.nets[:ps], req.windows[:ps], req.x_edge_costs,
+                                          req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+        t0 = time.perf_counter()
+        pl = eng.route_isolated_plain(sub)
+        dt = time.perf_counter() - t0
+        assert pl.paths == first.paths[:ps], "plain form disagrees with the batched engine"
+        line["plain"] = {"value": ps / dt, "unit": UNIT, "sample": f"first {ps} nets, one net per launch sequence"}
+        line["vs_plain"] = value / (ps / dt)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n_sample = min(args.cpu_sample, len(wl.nets))
+        rate, dt = _cpu_sample_rate(wl, n_sample)
+        cores = os.cpu_count() or 1
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{n_sample} of {len(wl.nets)} nets, A* alone-path search (window, then "
+                                          f"full board), {cores} host threads, {dt:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line))
+    batch.close()
+    board.close()
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=["congestion", "plain"], default="congestion")
+    ap.add_argument("--cpu-sample", type=int, default=128)
+    ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_engine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,216 @@
+/*
+ * mr_cuda.h — C ABI of the B200 batched shortest-path engine for metalroute.
+ *
+ * Plain pointers and sizes only; no CUDA or torch types cross this boundary
+ * (streams travel as `void *` holding a cudaStream_t).  Every entry point is
+ * all-or-error: on a non-zero status no result object is produced and
+ * mrc_last_error() describes the failure.  Nothing here ever falls back to a
+ * CPU search; the caller (metalroute's NegotiatedRouter) owns that fallback,
+ * exactly as with its Metal provider.
+ *
+ * Reference interfaces replaced (paths relative to the metal-route project):
+ *   - IsolatedRouteProvider::route_isolated_batch
+ *       crates/mr-cpu/src/negotiated.rs:554-560 (request :521-537, window :489-519)
+ *     as adapted by MetalIsolatedProvider, crates/mr-cli/src/lib.rs:549-625
+ *   - metal_route_isolated_batch / metal_route_isolated_batch_ragged
+ *       crates/mr-metal/src/lib.rs:414-558, 695-984
+ *   - metal_sweep_fields / metal_wavefront_field
+ *       crates/mr-metal/src/lib.rs:128-204
+ *   - MetalRouter::route (Router contract), crates/mr-metal/src/lib.rs:1143-1235,
+ *     and LeeRouter::route, crates/mr-cpu/src/lee.rs:68-110
+ *
+ * Data contract (crates/mr-core/src/lib.rs): Cost = uint32, OBSTACLE =
+ * 0xFFFFFFFF, CellIdx = uint32 with idx3(x, y, l) = (l*h + y)*w + x,
+ * board_constraint bits = Grid::BOARD_* (lib.rs:411-416).
+ * Canonical labels: (search cost, minimum hops, lowest predecessor CellIdx).
+ */
+#ifndef MR_CUDA_H
+#define MR_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MRC_ABI_VERSION 1u
+#define MRC_NO_PATH 0xFFFFFFFFu
+
+/* Status codes.  RouterError (crates/mr-core/src/lib.rs:698-708) maps onto
+ * MRC_ERR_MALFORMED_GRID, MRC_ERR_INVALID_ENDPOINT and, for everything the
+ * Metal provider reports as BackendUnavailable, the remaining codes. */
+typedef enum {
+    MRC_OK = 0,
+    MRC_ERR_INVALID_ARGUMENT = 1,    /* null pointer, shape mismatch, bad window */
+    MRC_ERR_MALFORMED_GRID = 2,      /* cost/mask lengths do not match dims */
+    MRC_ERR_INVALID_ENDPOINT = 3,    /* endpoint/pad out of bounds, foreign obstacle, board node */
+    MRC_ERR_BACKEND_UNAVAILABLE = 4, /* no CUDA device, launch or copy failure */
+    MRC_ERR_BUSY = 5,                /* context in use and MRC_FLAG_NO_WAIT given */
+    MRC_ERR_ITERATION_LIMIT = 6,     /* a device loop hit its bound; nothing returned */
+    MRC_ERR_OUT_OF_MEMORY = 7,       /* device or host allocation failed */
+    MRC_ERR_LIMIT = 8                /* request exceeds a documented size limit */
+} mrc_status;
+
+/* Request flags. */
+#define MRC_FLAG_RETRY_FULL 0x1u  /* unreachable-in-window nets are re-solved on the full board */
+#define MRC_FLAG_KEEP_FIELDS 0x2u /* return each net's u32 distance field over its solved window */
+#define MRC_FLAG_NO_WAIT 0x4u     /* fail with MRC_ERR_BUSY instead of waiting for the context */
+#define MRC_FLAG_TIME_KERNELS 0x8u /* batches record CUDA events around their relax kernel */
+
+typedef struct mrc_context mrc_context;
+typedef struct mrc_result mrc_result;
+typedef struct mrc_board mrc_board;
+typedef struct mrc_batch mrc_batch;
+
+/* Grid (crates/mr-core/src/lib.rs:393-408).  board_constraint and via_forbidden
+ * may be NULL (the reference's empty vectors). via_forbidden holds 0/1 bytes. */
+typedef struct {
+    uint32_t w, h, layers;
+    const uint32_t *cost;
+    const uint8_t *board_constraint;
+    const uint8_t *via_forbidden;
+} mrc_grid;
+
+/* NetEndpoints (crates/mr-core/src/lib.rs:519-537); the name stays with the caller. */
+typedef struct {
+    uint32_t src, dst;
+    const uint32_t *passable_pads;
+    uint32_t n_passable_pads;
+    const uint32_t *via_passable_pads;
+    uint32_t n_via_passable_pads;
+} mrc_net;
+
+/* IsolatedRouteWindow (crates/mr-cpu/src/negotiated.rs:494-500), inclusive. */
+typedef struct {
+    uint32_t x0, y0, x1, y1;
+} mrc_window;
+
+/* Already-rounded static edge prices (negotiated.rs:521-537).  The reference's
+ * `via_edge_costs: &[Option<Cost>]` is split into via_edge_costs + via_allowed
+ * (0 = None), as mr-metal does (crates/mr-metal/src/lib.rs:484-493).
+ * directed_in_costs (nullable) is this engine's superset form: 4 base prices per
+ * cell for the planar in-edges from its -y, -x, +x, +y neighbours, 0xFFFFFFFF =
+ * blocked edge; when given it replaces the per-axis gap price.  A planar or via
+ * step u->v costs min(base * enter(v), 0xFFFFFFFE) where enter(v) is 1 for an
+ * obstacle that is one of the net's own passable pads and cost[v] otherwise. */
+typedef struct {
+    const uint32_t *x_edge_costs;   /* w-1 */
+    uint32_t n_x_edge_costs;
+    const uint32_t *y_edge_costs;   /* h-1 */
+    uint32_t n_y_edge_costs;
+    const uint32_t *via_edge_costs; /* layers-1 */
+    const uint8_t *via_allowed;     /* layers-1 */
+    uint32_t n_via_edge_costs;
+    const uint32_t *directed_in_costs; /* nullable, 4*w*h*layers */
+} mrc_edges;
+
+/* IsolatedRouteRequest (negotiated.rs:529-537). */
+typedef struct {
+    const mrc_grid *grid;
+    const mrc_net *nets;
+    uint32_t n_nets;
+    const mrc_window *windows; /* n_nets */
+    mrc_edges edges;
+} mrc_isolated_request;
+
+/* ---- context -------------------------------------------------------------- */
+
+/* One context per process per device; thread-safe (calls serialise on it).
+ * Mirrors the process-global Metal context, crates/mr-metal/src/gpu.rs:865-878. */
+mrc_status mrc_context_create(int device, mrc_context **out);
+void mrc_context_destroy(mrc_context *ctx);
+/* Last error message of the calling thread's most recent failed call on ctx. */
+const char *mrc_last_error(const mrc_context *ctx);
+uint32_t mrc_abi_version(void);
+
+/* ---- the provider seam ------------------------------------------------------ */
+
+/* Solve an isolated batch: per net, the canonical path inside its window and,
+ * with MRC_FLAG_RETRY_FULL, a full-board re-solve of every net that was
+ * unreachable in its window (IsolatedRouteProvider contract,
+ * negotiated.rs:539-553; MetalIsolatedProvider retry, cli/src/lib.rs:574-607).
+ * Without the flag this is metal_route_isolated_batch (metal/src/lib.rs:398-412).
+ * Validation and its errors follow metal/src/lib.rs:433-467 and
+ * negotiated.rs:1392-1407. */
+mrc_status mrc_route_isolated_batch(mrc_context *ctx, const mrc_isolated_request *req, uint32_t flags,
+                                    mrc_result **out);
+
+/* ---- Router contract and plain fields (LeeRouter / MetalRouter / sweep fields) */
+
+/* LeeRouter::route / MetalRouter::route: every net on the whole board, planar
+ * moves only, step cost = enter cost of the destination (lee.rs:39-65), board
+ * masks honoured.  Unreachable nets get search cost MRC_NO_PATH. */
+mrc_status mrc_route_lee(mrc_context *ctx, const mrc_grid *grid, const mrc_net *nets, uint32_t n_nets,
+                         mrc_result **out);
+
+/* bfs_distance_field / metal_sweep_fields: one complete u32 field per source
+ * (sweep.rs:143-148, metal/src/lib.rs:166-192) written to fields[i*n_cells ..].
+ * An out-of-range, obstacle or board-forbidden source yields an all-0xFFFFFFFF
+ * field (metal/src/lib.rs:1500-1520). */
+mrc_status mrc_distance_fields(mrc_context *ctx, const mrc_grid *grid, const uint32_t *sources, uint32_t n_sources,
+                               uint32_t *fields);
+
+/* ---- results ---------------------------------------------------------------- */
+
+uint32_t mrc_result_count(const mrc_result *r);
+/* CSR paths: cells of net i are cells[offsets[i] .. offsets[i+1]) as global CellIdx. */
+const uint64_t *mrc_result_path_offsets(const mrc_result *r);
+const uint32_t *mrc_result_path_cells(const mrc_result *r);
+/* Fixed-point search cost per net (MetalIsolatedRoute::search_cost), MRC_NO_PATH if none. */
+const uint32_t *mrc_result_search_costs(const mrc_result *r);
+/* With MRC_FLAG_KEEP_FIELDS: net i's field covers window windows[i] (the full
+ * board when its retry ran), laid out (l, y-y0, x-x0) row-major, at
+ * fields[field_offsets[i] ..].  NULL otherwise. */
+const uint64_t *mrc_result_field_offsets(const mrc_result *r);
+const uint32_t *mrc_result_fields(const mrc_result *r);
+const mrc_window *mrc_result_field_windows(const mrc_result *r);
+/* Number of nets that needed the full-board retry. */
+uint32_t mrc_result_retried(const mrc_result *r);
+void mrc_result_free(mrc_result *r);
+
+/* ---- device-resident boards and prepared batches -------------------------- */
+
+/* Upload a board once (cost, masks, edge prices) and keep it in HBM. */
+mrc_status mrc_board_create(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *edges, mrc_board **out);
+void mrc_board_destroy(mrc_board *board);
+
+/* Validate and stage a batch of nets against a resident board (descriptors,
+ * pads and label storage in HBM).  Windows may be NULL: each net then gets
+ * net_window (negotiated.rs:568-594). */
+mrc_status mrc_batch_create(mrc_context *ctx, const mrc_board *board, const mrc_net *nets, uint32_t n_nets,
+                            const mrc_window *windows, uint32_t flags, mrc_batch **out);
+/* Enqueue the whole window solve (fields + canonical paths) on `stream`
+ * (a cudaStream_t, NULL = the context's stream) without any host sync. */
+mrc_status mrc_batch_launch(mrc_context *ctx, mrc_batch *batch, void *stream);
+/* Wait for the batch, run the full-board retry if flagged, copy results out. */
+mrc_status mrc_batch_finish(mrc_context *ctx, mrc_batch *batch, mrc_result **out);
+/* Kernels launched by the last mrc_batch_launch (for launch accounting). */
+uint32_t mrc_batch_kernel_launches(const mrc_batch *batch);
+/* Device milliseconds of the relax kernel of the last launch, from CUDA events
+ * recorded on the launching stream (batch created with MRC_FLAG_TIME_KERNELS;
+ * call after the stream has been synchronised).  Negative when unavailable. */
+float mrc_batch_relax_ms(const mrc_batch *batch);
+/* Cells in all windows of the batch (the per-launch work unit). */
+uint64_t mrc_batch_window_cells(const mrc_batch *batch);
+void mrc_batch_destroy(mrc_batch *batch);
+
+/* ---- the plain form (one net per launch sequence) --------------------------- */
+
+/* The reference's plain GPU method restated on CUDA: per net, Jacobi relaxation
+ * rounds of one thread per window cell, each round followed by a host read of
+ * the changed flag (crates/mr-metal/src/gpu.rs:22-87,1242-1303 for the planar
+ * wavefront, extended here to the isolated edge/via model).  Same results as
+ * mrc_route_isolated_batch; kept as the baseline the batched engine is
+ * measured against. */
+mrc_status mrc_route_isolated_plain(mrc_context *ctx, const mrc_isolated_request *req, uint32_t flags,
+                                    mrc_result **out);
+
+/* net_window (negotiated.rs:568-594) for a batch of nets. */
+mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
+                           mrc_window *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

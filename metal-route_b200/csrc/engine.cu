@@ -1,0 +1,1039 @@
+// engine.cu — host runtime behind include/mr_cuda.h.
+//
+// Owns devices buffers (a per-context caching pool), request validation,
+// window computation, batch packing, the window-then-full-board retry and the
+// result objects.  Nothing here searches on the CPU: every path and field is
+// computed by the kernels in relax.cu, and any device failure is returned as a
+// status so the caller can take its own CPU fallback (the contract of
+// crates/mr-cpu/src/negotiated.rs:539-553).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "kernels.h"
+#include "mr_cuda.h"
+
+using namespace mrc;
+
+namespace {
+
+thread_local std::string g_err;
+
+mrc_status fail(mrc_status s, std::string msg) {
+    g_err = std::move(msg);
+    return s;
+}
+
+#define MRC_CUDA(call, what)                                                                        \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? MRC_ERR_OUT_OF_MEMORY : MRC_ERR_BACKEND_UNAVAILABLE, \
+                        std::string(what) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+#define MRC_TRY(expr)                 \
+    do {                              \
+        mrc_status s_ = (expr);       \
+        if (s_ != MRC_OK) return s_;  \
+    } while (0)
+
+// Grow-and-reuse device allocator; callers hold the context mutex.
+class Pool {
+   public:
+    ~Pool() { trim(); }
+    cudaError_t alloc(size_t bytes, void **out) {
+        bytes = std::max<size_t>((bytes + 255) & ~(size_t)255, 256);
+        auto it = free_.lower_bound(bytes);
+        if (it != free_.end() && it->first <= 2 * bytes + (8u << 20)) {
+            *out = it->second;
+            used_[it->second] = it->first;
+            free_.erase(it);
+            return cudaSuccess;
+        }
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            trim();
+            e = cudaMalloc(&p, bytes);
+            if (e != cudaSuccess) {
+                (void)cudaGetLastError();
+                return e;
+            }
+        }
+        used_[p] = bytes;
+        *out = p;
+        return cudaSuccess;
+    }
+    void release(void *p) {
+        if (!p) return;
+        auto it = used_.find(p);
+        if (it == used_.end()) return;
+        free_.emplace(it->second, p);
+        used_.erase(it);
+    }
+    void trim() {
+        for (auto &kv : free_) cudaFree(kv.second);
+        free_.clear();
+    }
+
+   private:
+    std::multimap<size_t, void *> free_;
+    std::unordered_map<void *, size_t> used_;
+};
+
+}  // namespace
+
+struct mrc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    Pool pool;
+    int sms = 148;
+    size_t smem_optin = 0;
+};
+
+namespace {
+
+// RAII handle on a pool block.
+struct DBuf {
+    mrc_context *ctx = nullptr;
+    void *p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { reset(); }
+    void reset() {
+        if (ctx && p) ctx->pool.release(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    mrc_status get(mrc_context *c, size_t n, const char *what) {
+        reset();
+        ctx = c;
+        bytes = n;
+        MRC_CUDA(c->pool.alloc(n, &p), what);
+        return MRC_OK;
+    }
+    template <class T>
+    T *as() const {
+        return reinterpret_cast<T *>(p);
+    }
+};
+
+struct GridView {
+    uint32_t w = 0, h = 0, layers = 0;
+    uint64_t n = 0;
+    const uint32_t *cost = nullptr;
+    const uint8_t *board = nullptr;
+    const uint8_t *via_forbidden = nullptr;
+    bool obstacle(uint32_t c) const { return cost[c] == kMax; }
+    bool board_forbidden(uint32_t c) const { return board && (board[c] & kTraceNode); }
+};
+
+mrc_status view_grid(const mrc_grid *g, GridView *v) {
+    if (!g) return fail(MRC_ERR_INVALID_ARGUMENT, "grid is NULL");
+    v->w = g->w;
+    v->h = g->h;
+    v->layers = g->layers == 0 ? 1 : g->layers;  // Dims::with_layers clamps to >= 1
+    v->n = (uint64_t)v->w * v->h * v->layers;
+    if (v->n > 0xFFFFFFFFull) return fail(MRC_ERR_MALFORMED_GRID, "grid exceeds the 32-bit CellIdx domain");
+    if (v->n && !g->cost) return fail(MRC_ERR_MALFORMED_GRID, "grid cost is NULL");
+    if (v->layers > 32) return fail(MRC_ERR_LIMIT, "more than 32 layers");
+    v->cost = g->cost;
+    v->board = g->board_constraint;
+    v->via_forbidden = g->via_forbidden;
+    return MRC_OK;
+}
+
+struct NetCopy {
+    uint32_t src, dst;
+    std::vector<uint32_t> pads, vpads;  // sorted, unique
+};
+
+bool sorted_contains(const std::vector<uint32_t> &v, uint32_t c) { return std::binary_search(v.begin(), v.end(), c); }
+
+// Endpoint/pad validation: metal/src/lib.rs:446-467 and negotiated.rs:1392-1407,
+// plus the board trace-node rule of route_variant (negotiated.rs:1483-1492).
+mrc_status validate_nets(const GridView &g, const mrc_net *nets, uint32_t n, std::vector<NetCopy> *out) {
+    if (n && !nets) return fail(MRC_ERR_INVALID_ARGUMENT, "nets is NULL");
+    out->resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const mrc_net &nt = nets[i];
+        NetCopy &c = (*out)[i];
+        c.src = nt.src;
+        c.dst = nt.dst;
+        if ((nt.n_passable_pads && !nt.passable_pads) || (nt.n_via_passable_pads && !nt.via_passable_pads))
+            return fail(MRC_ERR_INVALID_ARGUMENT, "net " + std::to_string(i) + ": pad list pointer is NULL");
+        c.pads.assign(nt.passable_pads, nt.passable_pads + nt.n_passable_pads);
+        c.vpads.assign(nt.via_passable_pads, nt.via_passable_pads + nt.n_via_passable_pads);
+        std::sort(c.pads.begin(), c.pads.end());
+        c.pads.erase(std::unique(c.pads.begin(), c.pads.end()), c.pads.end());
+        std::sort(c.vpads.begin(), c.vpads.end());
+        c.vpads.erase(std::unique(c.vpads.begin(), c.vpads.end()), c.vpads.end());
+        auto bad = [&](const char *why) {
+            return fail(MRC_ERR_INVALID_ENDPOINT, "net " + std::to_string(i) + ": " + why);
+        };
+        for (uint32_t p : c.pads)
+            if (p >= g.n) return bad("passable pad out of bounds");
+        for (uint32_t p : c.vpads)
+            if (p >= g.n || !sorted_contains(c.pads, p)) return bad("via pad out of bounds or not an own pad");
+        if (c.src >= g.n || c.dst >= g.n) return bad("endpoint out of bounds");
+        if (g.board_forbidden(c.src) || g.board_forbidden(c.dst)) return bad("endpoint outside the board outline");
+        if (g.obstacle(c.src) && !sorted_contains(c.pads, c.src)) return bad("source on a foreign obstacle");
+        if (g.obstacle(c.dst) && !sorted_contains(c.pads, c.dst)) return bad("target on a foreign obstacle");
+    }
+    return MRC_OK;
+}
+
+mrc_window full_window(uint32_t w, uint32_t h) { return mrc_window{0, 0, w ? w - 1 : 0, h ? h - 1 : 0}; }
+
+// net_window, crates/mr-cpu/src/negotiated.rs:568-594.
+mrc_window net_window(uint32_t w, uint32_t h, const NetCopy &n) {
+    const uint32_t plane = w * h;
+    auto xy = [&](uint32_t c, uint32_t *x, uint32_t *y) {
+        const uint32_t r = c % plane;
+        *x = r % w;
+        *y = r / w;
+    };
+    uint32_t sx, sy, dx, dy;
+    xy(n.src, &sx, &sy);
+    xy(n.dst, &dx, &dy);
+    uint32_t x0 = std::min(sx, dx), y0 = std::min(sy, dy), x1 = std::max(sx, dx), y1 = std::max(sy, dy);
+    for (uint32_t p : n.pads) {
+        uint32_t px, py;
+        xy(p, &px, &py);
+        x0 = std::min(x0, px);
+        y0 = std::min(y0, py);
+        x1 = std::max(x1, px);
+        y1 = std::max(y1, py);
+    }
+    const uint32_t span = std::max(x1 - x0, y1 - y0);
+    const uint32_t margin = std::max<uint32_t>(16, (3 * span + 9) / 10);
+    mrc_window win;
+    win.x0 = x0 > margin ? x0 - margin : 0;
+    win.y0 = y0 > margin ? y0 - margin : 0;
+    win.x1 = std::min<uint64_t>((uint64_t)x1 + margin, w ? w - 1 : 0);
+    win.y1 = std::min<uint64_t>((uint64_t)y1 + margin, h ? h - 1 : 0);
+    return win;
+}
+
+bool window_valid(const mrc_window &win, uint32_t w, uint32_t h) {
+    return w > 0 && h > 0 && win.x0 <= win.x1 && win.y0 <= win.y1 && win.x1 < w && win.y1 < h;
+}
+
+bool is_full(const mrc_window &win, uint32_t w, uint32_t h) {
+    return win.x0 == 0 && win.y0 == 0 && win.x1 + 1 == w && win.y1 + 1 == h;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Boards
+
+struct mrc_board {
+    mrc_context *ctx = nullptr;
+    GridView view;                 // points into the host copies below
+    std::vector<uint32_t> cost;    // host copy for endpoint validation
+    std::vector<uint8_t> board;    // host copy of the board mask (may be empty)
+    std::vector<uint8_t> viaf;     // host copy of the static via mask (may be empty)
+    bool directed = false;
+    DBuf d_cost, d_flags, d_x, d_y, d_via, d_dir;
+    DevBoard dev{};
+};
+
+namespace mrc {
+cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, uint64_t n, cudaStream_t st);
+}
+
+namespace {
+
+mrc_status upload(mrc_context *ctx, DBuf &buf, const void *src, size_t bytes, const char *what) {
+    MRC_TRY(buf.get(ctx, std::max<size_t>(bytes, 4), what));
+    if (bytes) MRC_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream), what);
+    return MRC_OK;
+}
+
+// Upload the board and its edge prices; `keep_host` keeps the validation copies.
+mrc_status board_build(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *edges, bool keep_host,
+                       mrc_board *b) {
+    MRC_TRY(view_grid(grid, &b->view));
+    GridView &g = b->view;
+    if (!edges) return fail(MRC_ERR_INVALID_ARGUMENT, "edges is NULL");
+    const uint32_t ex = g.w ? g.w - 1 : 0, ey = g.h ? g.h - 1 : 0, ev = g.layers - 1;
+    if (edges->n_x_edge_costs != ex || edges->n_y_edge_costs != ey || edges->n_via_edge_costs != ev)
+        return fail(MRC_ERR_INVALID_ARGUMENT, "isolated batch shape does not match grid/nets");
+    if ((ex && !edges->x_edge_costs) || (ey && !edges->y_edge_costs) ||
+        (ev && (!edges->via_edge_costs || !edges->via_allowed)))
+        return fail(MRC_ERR_INVALID_ARGUMENT, "edge price pointer is NULL");
+    b->ctx = ctx;
+    b->directed = edges->directed_in_costs != nullptr;
+    if (keep_host) {
+        b->cost.assign(g.cost, g.cost + g.n);
+        if (g.board) b->board.assign(g.board, g.board + g.n);
+        if (g.via_forbidden) b->viaf.assign(g.via_forbidden, g.via_forbidden + g.n);
+        g.cost = b->cost.data();
+        g.board = g.board ? b->board.data() : nullptr;
+        g.via_forbidden = g.via_forbidden ? b->viaf.data() : nullptr;
+    }
+    const size_t n = (size_t)g.n;
+    MRC_TRY(upload(ctx, b->d_cost, g.cost, n * 4, "upload cost"));
+    const bool has_flags = g.board || g.via_forbidden;
+    if (has_flags) {
+        if (g.board) {
+            MRC_TRY(upload(ctx, b->d_flags, g.board, n, "upload board mask"));
+        } else {
+            MRC_TRY(b->d_flags.get(ctx, std::max<size_t>(n, 4), "board flags"));
+            MRC_CUDA(cudaMemsetAsync(b->d_flags.p, 0, n, ctx->stream), "clear flags");
+        }
+        if (g.via_forbidden) {
+            DBuf tmp;
+            MRC_TRY(upload(ctx, tmp, g.via_forbidden, n, "upload via mask"));
+            MRC_CUDA(combine_flags_launch(b->d_flags.as<uint8_t>(), tmp.as<uint8_t>(), n, ctx->stream), "combine masks");
+            MRC_CUDA(cudaStreamSynchronize(ctx->stream), "combine masks");
+        }
+    }
+    std::vector<uint32_t> vias(std::max<uint32_t>(ev, 1), 0);
+    uint32_t via_mask = 0;
+    for (uint32_t k = 0; k < ev; ++k) {
+        vias[k] = edges->via_edge_costs[k];
+        if (edges->via_allowed[k]) via_mask |= 1u << k;
+    }
+    MRC_TRY(upload(ctx, b->d_x, edges->x_edge_costs, (size_t)ex * 4, "upload x edges"));
+    MRC_TRY(upload(ctx, b->d_y, edges->y_edge_costs, (size_t)ey * 4, "upload y edges"));
+    MRC_TRY(upload(ctx, b->d_via, vias.data(), vias.size() * 4, "upload via edges"));
+    if (b->directed) MRC_TRY(upload(ctx, b->d_dir, edges->directed_in_costs, n * 16, "upload directed prices"));
+    b->dev.w = g.w;
+    b->dev.h = g.h;
+    b->dev.layers = g.layers;
+    b->dev.via_mask = via_mask;
+    b->dev.cost = b->d_cost.as<uint32_t>();
+    b->dev.flags = has_flags ? b->d_flags.as<uint8_t>() : nullptr;
+    b->dev.x_edge = b->d_x.as<uint32_t>();
+    b->dev.y_edge = b->d_y.as<uint32_t>();
+    b->dev.via_edge = b->d_via.as<uint32_t>();
+    b->dev.directed = b->directed ? b->d_dir.as<uint4>() : nullptr;
+    return MRC_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Results
+
+struct mrc_result {
+    uint32_t n = 0;
+    uint32_t retried = 0;
+    std::vector<uint64_t> offsets;
+    std::vector<uint32_t> cells;
+    std::vector<uint32_t> costs;
+    bool has_fields = false;
+    std::vector<uint64_t> field_offsets;
+    std::vector<uint32_t> fields;
+    std::vector<mrc_window> field_windows;
+};
+
+// ---------------------------------------------------------------------------
+// Batches
+
+struct mrc_batch {
+    mrc_context *ctx = nullptr;
+    const mrc_board *board = nullptr;
+    uint32_t flags = 0;
+    std::vector<NetCopy> nets;
+    std::vector<mrc_window> windows;
+    std::vector<DevField> fields;  // processing order
+    uint64_t total_cells = 0;
+    uint32_t max_tiles = 0, tile_h = 32, grid = 1;
+    size_t smem = 0;
+    DBuf d_fields, d_pads, d_dist, d_hops, d_scratch, d_costs, d_lens, d_offsets, d_cells, d_ctl;
+    uint32_t launches = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~mrc_batch() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+constexpr uint32_t kActivationFactor = 256;
+
+mrc_status choose_tile(mrc_context *ctx, uint32_t layers, bool directed, uint32_t *tile_h, size_t *smem) {
+    const size_t budget_fast = 110u << 10;  // two CTAs per SM
+    const size_t budget_max = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
+    for (size_t budget : {budget_fast, budget_max}) {
+        for (uint32_t th : {32u, 16u, 8u}) {
+            const size_t s = relax_smem_bytes(layers, th, directed);
+            if (s <= budget) {
+                *tile_h = th;
+                *smem = s;
+                return MRC_OK;
+            }
+        }
+    }
+    return fail(MRC_ERR_LIMIT, "too many layers for one shared-memory tile");
+}
+
+mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> nets,
+                       std::vector<mrc_window> windows, uint32_t flags, mrc_batch *bt) {
+    const GridView &g = board->view;
+    bt->ctx = ctx;
+    bt->board = board;
+    bt->flags = flags;
+    bt->nets = std::move(nets);
+    bt->windows = std::move(windows);
+    const uint32_t n = (uint32_t)bt->nets.size();
+    MRC_TRY(choose_tile(ctx, g.layers, board->directed, &bt->tile_h, &bt->smem));
+    // largest windows first: the persistent CTAs then finish together
+    std::vector<uint32_t> order(n);
+    std::iota(order.begin(), order.end(), 0u);
+    auto cells_of = [&](uint32_t i) {
+        const mrc_window &w = bt->windows[i];
+        return (uint64_t)(w.x1 - w.x0 + 1) * (w.y1 - w.y0 + 1) * g.layers;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cells_of(a) > cells_of(b); });
+    std::vector<uint32_t> pads;
+    bt->fields.resize(n);
+    uint64_t off = 0;
+    uint32_t max_tiles = 1;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t i = order[k];
+        const NetCopy &nc = bt->nets[i];
+        const mrc_window &w = bt->windows[i];
+        DevField &f = bt->fields[k];
+        f.src = nc.src;
+        f.dst = nc.dst;
+        f.x0 = w.x0;
+        f.y0 = w.y0;
+        f.ww = w.x1 - w.x0 + 1;
+        f.wh = w.y1 - w.y0 + 1;
+        f.lab_off = off;
+        off += cells_of(i);
+        f.pad_off = (uint32_t)pads.size();
+        f.n_pads = (uint32_t)nc.pads.size();
+        pads.insert(pads.end(), nc.pads.begin(), nc.pads.end());
+        f.vpad_off = (uint32_t)pads.size();
+        f.n_vpads = (uint32_t)nc.vpads.size();
+        pads.insert(pads.end(), nc.vpads.begin(), nc.vpads.end());
+        f.out = i;
+        f.pad_ = 0;
+        const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + bt->tile_h - 1) / bt->tile_h);
+        if (tiles > (1u << 24)) return fail(MRC_ERR_LIMIT, "window has more than 2^24 tiles");
+        max_tiles = std::max<uint32_t>(max_tiles, (uint32_t)tiles);
+        if (pads.size() > 0xFFFFFFF0u) return fail(MRC_ERR_LIMIT, "pad lists exceed 2^32 entries");
+    }
+    bt->total_cells = off;
+    bt->max_tiles = max_tiles;
+    int per_sm = 1;
+    MRC_CUDA(relax_configure(board->directed, bt->smem), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(board->directed, bt->smem, &per_sm), "relax occupancy");
+    per_sm = std::max(per_sm, 1);
+    bt->grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n, (uint64_t)ctx->sms * per_sm));
+    const uint32_t stride = max_tiles + (max_tiles + 31) / 32;
+    MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
+    MRC_TRY(upload(ctx, bt->d_pads, pads.data(), pads.size() * 4, "upload pads"));
+    MRC_TRY(bt->d_dist.get(ctx, std::max<uint64_t>(off, 1) * 4, "dist labels"));
+    MRC_TRY(bt->d_hops.get(ctx, std::max<uint64_t>(off, 1) * 4, "hop labels"));
+    MRC_TRY(bt->d_scratch.get(ctx, (size_t)bt->grid * stride * 4, "tile queues"));
+    MRC_TRY(bt->d_costs.get(ctx, std::max<size_t>(n, 1) * 4, "costs"));
+    MRC_TRY(bt->d_lens.get(ctx, std::max<size_t>(n, 1) * 4, "lengths"));
+    MRC_TRY(bt->d_offsets.get(ctx, ((size_t)n + 1) * 8, "offsets"));
+    MRC_TRY(bt->d_cells.get(ctx, std::max<uint64_t>(off, 1) * 4, "path cells"));
+    MRC_TRY(bt->d_ctl.get(ctx, 64, "control words"));
+    if (flags & MRC_FLAG_TIME_KERNELS) {
+        MRC_CUDA(cudaEventCreate(&bt->ev0), "create event");
+        MRC_CUDA(cudaEventCreate(&bt->ev1), "create event");
+    }
+    return MRC_OK;
+}
+
+mrc_status batch_launch(mrc_batch *bt, cudaStream_t st) {
+    const uint32_t n = (uint32_t)bt->fields.size();
+    uint32_t *ctl = bt->d_ctl.as<uint32_t>();  // [0] work counter, [1] status
+    bt->stream = st;
+    bt->launches = 0;
+    MRC_CUDA(cudaMemsetAsync(ctl, 0, 64, st), "reset control words");
+    RelaxArgs ra;
+    ra.board = bt->board->dev;
+    ra.fields = bt->d_fields.as<DevField>();
+    ra.n_fields = n;
+    ra.pads = bt->d_pads.as<uint32_t>();
+    ra.dist = bt->d_dist.as<uint32_t>();
+    ra.hops = bt->d_hops.as<uint32_t>();
+    ra.work_counter = ctl;
+    ra.tile_scratch = bt->d_scratch.as<uint32_t>();
+    ra.scratch_stride = bt->max_tiles + (bt->max_tiles + 31) / 32;
+    ra.max_tiles = bt->max_tiles;
+    ra.tile_h = bt->tile_h;
+    ra.activation_factor = kActivationFactor;
+    ra.status = ctl + 1;
+    if (n) {
+        if (bt->ev0) MRC_CUDA(cudaEventRecord(bt->ev0, st), "record event");
+        MRC_CUDA(relax_launch(ra, bt->grid, bt->smem, st), "launch relax kernel");
+        if (bt->ev1) MRC_CUDA(cudaEventRecord(bt->ev1, st), "record event");
+        bt->launches++;
+    }
+    PathArgs pa;
+    pa.board = bt->board->dev;
+    pa.fields = ra.fields;
+    pa.n_fields = n;
+    pa.pads = ra.pads;
+    pa.dist = ra.dist;
+    pa.hops = ra.hops;
+    pa.costs = bt->d_costs.as<uint32_t>();
+    pa.lens = bt->d_lens.as<uint32_t>();
+    pa.offsets = bt->d_offsets.as<unsigned long long>();
+    pa.cells = bt->d_cells.as<uint32_t>();
+    pa.status = ctl + 1;
+    MRC_CUDA(path_launch(pa, st), "launch path kernels");
+    bt->launches += n ? 2 : 1;
+    return MRC_OK;
+}
+
+mrc_status status_error(uint32_t status) {
+    if (status & 3u) return fail(MRC_ERR_ITERATION_LIMIT, "a field hit its relaxation bound");
+    if (status & 4u) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "canonical path reconstruction failed");
+    return fail(MRC_ERR_BACKEND_UNAVAILABLE, "tile queue overflow");
+}
+
+// Copy one batch's outputs into `r` at the given result slots.
+mrc_status batch_collect(mrc_batch *bt, bool keep_fields, std::vector<uint32_t> *costs,
+                         std::vector<std::vector<uint32_t>> *paths, std::vector<std::vector<uint32_t>> *fields) {
+    cudaStream_t st = bt->stream;
+    const uint32_t n = (uint32_t)bt->fields.size();
+    uint32_t status = 0;
+    MRC_CUDA(cudaMemcpyAsync(&status, bt->d_ctl.as<uint32_t>() + 1, 4, cudaMemcpyDeviceToHost, st), "read status");
+    std::vector<uint64_t> off(n + 1);
+    costs->assign(n, kMax);
+    if (n) MRC_CUDA(cudaMemcpyAsync(costs->data(), bt->d_costs.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "read costs");
+    MRC_CUDA(cudaMemcpyAsync(off.data(), bt->d_offsets.p, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost, st), "read offsets");
+    MRC_CUDA(cudaStreamSynchronize(st), "batch execution");
+    if (status) return status_error(status);
+    std::vector<uint32_t> cells(off[n]);
+    if (off[n]) MRC_CUDA(cudaMemcpy(cells.data(), bt->d_cells.p, off[n] * 4, cudaMemcpyDeviceToHost), "read paths");
+    paths->assign(n, {});
+    for (uint32_t i = 0; i < n; ++i) (*paths)[i].assign(cells.begin() + off[i], cells.begin() + off[i + 1]);
+    if (keep_fields) {
+        fields->assign(n, {});
+        std::vector<uint32_t> all(bt->total_cells);
+        if (bt->total_cells)
+            MRC_CUDA(cudaMemcpy(all.data(), bt->d_dist.p, bt->total_cells * 4, cudaMemcpyDeviceToHost), "read fields");
+        for (const DevField &f : bt->fields) {
+            const uint64_t c = (uint64_t)f.ww * f.wh * bt->board->view.layers;
+            (*fields)[f.out].assign(all.begin() + f.lab_off, all.begin() + f.lab_off + c);
+        }
+    }
+    return MRC_OK;
+}
+
+// Run a batch synchronously and, with MRC_FLAG_RETRY_FULL, re-solve on the full
+// board every net whose window solve was unreachable (cli/src/lib.rs:574-607).
+mrc_status solve(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> nets, std::vector<mrc_window> wins,
+                 uint32_t flags, mrc_result **out, mrc_batch *prepared) {
+    const GridView &g = board->view;
+    const bool keep = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
+    std::unique_ptr<mrc_batch> own;
+    mrc_batch *bt = prepared;
+    if (!bt) {
+        own.reset(new mrc_batch());
+        bt = own.get();
+        MRC_TRY(batch_build(ctx, board, std::move(nets), std::move(wins), flags, bt));
+        MRC_TRY(batch_launch(bt, ctx->stream));
+    }
+    std::vector<uint32_t> costs;
+    std::vector<std::vector<uint32_t>> paths, fields;
+    MRC_TRY(batch_collect(bt, keep, &costs, &paths, &fields));
+    std::unique_ptr<mrc_result> r(new mrc_result());
+    const uint32_t n = (uint32_t)bt->nets.size();
+    r->n = n;
+    r->field_windows = bt->windows;
+    if (flags & MRC_FLAG_RETRY_FULL) {
+        std::vector<uint32_t> idx;
+        for (uint32_t i = 0; i < n; ++i)
+            if (costs[i] == kMax && !is_full(bt->windows[i], g.w, g.h)) idx.push_back(i);
+        if (!idx.empty()) {
+            std::vector<NetCopy> rn;
+            std::vector<mrc_window> rw;
+            for (uint32_t i : idx) {
+                rn.push_back(bt->nets[i]);
+                rw.push_back(full_window(g.w, g.h));
+            }
+            mrc_batch retry;
+            MRC_TRY(batch_build(ctx, board, std::move(rn), std::move(rw), flags, &retry));
+            MRC_TRY(batch_launch(&retry, bt->stream ? bt->stream : ctx->stream));
+            std::vector<uint32_t> c2;
+            std::vector<std::vector<uint32_t>> p2, f2;
+            MRC_TRY(batch_collect(&retry, keep, &c2, &p2, &f2));
+            for (size_t k = 0; k < idx.size(); ++k) {
+                costs[idx[k]] = c2[k];
+                paths[idx[k]] = std::move(p2[k]);
+                if (keep) fields[idx[k]] = std::move(f2[k]);
+                r->field_windows[idx[k]] = full_window(g.w, g.h);
+            }
+            r->retried = (uint32_t)idx.size();
+        }
+    }
+    r->costs = std::move(costs);
+    r->offsets.resize(n + 1);
+    uint64_t o = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        r->offsets[i] = o;
+        o += paths[i].size();
+    }
+    r->offsets[n] = o;
+    r->cells.reserve(o);
+    for (auto &p : paths) r->cells.insert(r->cells.end(), p.begin(), p.end());
+    if (keep) {
+        r->has_fields = true;
+        r->field_offsets.resize(n + 1);
+        uint64_t fo = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            r->field_offsets[i] = fo;
+            fo += fields[i].size();
+        }
+        r->field_offsets[n] = fo;
+        r->fields.reserve(fo);
+        for (auto &f : fields) r->fields.insert(r->fields.end(), f.begin(), f.end());
+    }
+    *out = r.release();
+    return MRC_OK;
+}
+
+mrc_status collect_windows(const GridView &g, const std::vector<NetCopy> &nets, const mrc_window *windows,
+                           std::vector<mrc_window> *out) {
+    out->resize(nets.size());
+    for (size_t i = 0; i < nets.size(); ++i) {
+        (*out)[i] = windows ? windows[i] : net_window(g.w, g.h, nets[i]);
+        if (!window_valid((*out)[i], g.w, g.h))
+            return fail(MRC_ERR_INVALID_ARGUMENT, "net " + std::to_string(i) + " has an invalid isolated-route window");
+    }
+    return MRC_OK;
+}
+
+struct Lock {
+    std::unique_lock<std::mutex> lk;
+    mrc_status st = MRC_OK;
+    Lock(mrc_context *ctx, uint32_t flags) : lk(ctx->mu, std::defer_lock) {
+        if (flags & MRC_FLAG_NO_WAIT) {
+            if (!lk.try_lock()) st = fail(MRC_ERR_BUSY, "CUDA isolated batch is busy");
+        } else {
+            lk.lock();
+        }
+    }
+};
+
+mrc_status set_device(mrc_context *ctx) {
+    MRC_CUDA(cudaSetDevice(ctx->device), "select device");
+    return MRC_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+uint32_t mrc_abi_version(void) { return MRC_ABI_VERSION; }
+
+const char *mrc_last_error(const mrc_context *) { return g_err.c_str(); }
+
+mrc_status mrc_context_create(int device, mrc_context **out) {
+    if (!out) return fail(MRC_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        return fail(MRC_ERR_BACKEND_UNAVAILABLE, "no CUDA device is available");
+    }
+    if (device < 0 || device >= count) return fail(MRC_ERR_INVALID_ARGUMENT, "device index out of range");
+    std::unique_ptr<mrc_context> ctx(new mrc_context());
+    ctx->device = device;
+    MRC_CUDA(cudaSetDevice(device), "select device");
+    cudaDeviceProp prop;
+    MRC_CUDA(cudaGetDeviceProperties(&prop, device), "device properties");
+    if (prop.major < 10) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "device is not sm_100 class");
+    ctx->sms = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    MRC_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "create stream");
+    *out = ctx.release();
+    return MRC_OK;
+}
+
+void mrc_context_destroy(mrc_context *ctx) {
+    if (!ctx) return;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        if (ctx->stream) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaStreamDestroy(ctx->stream);
+        }
+        ctx->pool.trim();
+    }
+    delete ctx;
+}
+
+mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
+                           mrc_window *out) {
+    if ((n_nets && (!nets || !out))) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    (void)layers;
+    for (uint32_t i = 0; i < n_nets; ++i) {
+        NetCopy c;
+        c.src = nets[i].src;
+        c.dst = nets[i].dst;
+        if (nets[i].n_passable_pads && !nets[i].passable_pads)
+            return fail(MRC_ERR_INVALID_ARGUMENT, "pad list pointer is NULL");
+        c.pads.assign(nets[i].passable_pads, nets[i].passable_pads + nets[i].n_passable_pads);
+        out[i] = net_window(w, h, c);
+    }
+    return MRC_OK;
+}
+
+mrc_status mrc_route_isolated_batch(mrc_context *ctx, const mrc_isolated_request *req, uint32_t flags,
+                                    mrc_result **out) {
+    if (!ctx || !req || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, flags);
+    if (lock.st != MRC_OK) return lock.st;
+    MRC_TRY(set_device(ctx));
+    GridView g;
+    MRC_TRY(view_grid(req->grid, &g));
+    if (req->n_nets && !req->windows) return fail(MRC_ERR_INVALID_ARGUMENT, "windows is NULL");
+    std::vector<NetCopy> nets;
+    MRC_TRY(validate_nets(g, req->nets, req->n_nets, &nets));
+    std::vector<mrc_window> wins;
+    MRC_TRY(collect_windows(g, nets, req->windows, &wins));
+    mrc_board board;
+    MRC_TRY(board_build(ctx, req->grid, &req->edges, false, &board));
+    if (nets.empty()) {
+        *out = new mrc_result();
+        (*out)->offsets.assign(1, 0);
+        (*out)->has_fields = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
+        (*out)->field_offsets.assign(1, 0);
+        return MRC_OK;
+    }
+    return solve(ctx, &board, std::move(nets), std::move(wins), flags, out, nullptr);
+}
+
+mrc_status mrc_route_lee(mrc_context *ctx, const mrc_grid *grid, const mrc_net *nets, uint32_t n_nets,
+                         mrc_result **out) {
+    if (!ctx || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    GridView g;
+    MRC_TRY(view_grid(grid, &g));
+    std::vector<NetCopy> nc;
+    MRC_TRY(validate_nets(g, nets, n_nets, &nc));
+    // LeeRouter: unit edge prices, no vias, the whole board (lee.rs:46-64)
+    std::vector<uint32_t> ones(std::max<uint32_t>(std::max(g.w, g.h), 1), 1u);
+    std::vector<uint32_t> via0(std::max<uint32_t>(g.layers, 1), 0u);
+    std::vector<uint8_t> noallow(std::max<uint32_t>(g.layers, 1), 0);
+    mrc_edges e{ones.data(), g.w ? g.w - 1 : 0, ones.data(), g.h ? g.h - 1 : 0, via0.data(), noallow.data(),
+                g.layers - 1, nullptr};
+    mrc_board board;
+    MRC_TRY(board_build(ctx, grid, &e, false, &board));
+    if (nc.empty()) {
+        *out = new mrc_result();
+        (*out)->offsets.assign(1, 0);
+        return MRC_OK;
+    }
+    std::vector<mrc_window> wins(nc.size(), full_window(g.w, g.h));
+    return solve(ctx, &board, std::move(nc), std::move(wins), 0, out, nullptr);
+}
+
+mrc_status mrc_distance_fields(mrc_context *ctx, const mrc_grid *grid, const uint32_t *sources, uint32_t n_sources,
+                               uint32_t *fields) {
+    if (!ctx || (n_sources && (!sources || !fields))) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    GridView g;
+    MRC_TRY(view_grid(grid, &g));
+    std::vector<NetCopy> nc;
+    std::vector<uint32_t> slot;
+    for (uint32_t i = 0; i < n_sources; ++i) {
+        const uint32_t s = sources[i];
+        if (g.n && s < g.n && !g.obstacle(s) && !g.board_forbidden(s)) {
+            NetCopy c;
+            c.src = s;
+            c.dst = s;
+            nc.push_back(std::move(c));
+            slot.push_back(i);
+        } else if (g.n) {
+            std::fill(fields + (size_t)i * g.n, fields + (size_t)(i + 1) * g.n, kMax);
+        }
+    }
+    if (nc.empty() || g.n == 0) return MRC_OK;
+    std::vector<uint32_t> ones(std::max<uint32_t>(std::max(g.w, g.h), 1), 1u);
+    std::vector<uint32_t> via0(std::max<uint32_t>(g.layers, 1), 0u);
+    std::vector<uint8_t> noallow(std::max<uint32_t>(g.layers, 1), 0);
+    mrc_edges e{ones.data(), g.w - 1, ones.data(), g.h - 1, via0.data(), noallow.data(), g.layers - 1, nullptr};
+    mrc_board board;
+    MRC_TRY(board_build(ctx, grid, &e, false, &board));
+    std::vector<mrc_window> wins(nc.size(), full_window(g.w, g.h));
+    mrc_result *r = nullptr;
+    MRC_TRY(solve(ctx, &board, std::move(nc), std::move(wins), MRC_FLAG_KEEP_FIELDS, &r, nullptr));
+    std::unique_ptr<mrc_result> hold(r);
+    for (size_t k = 0; k < slot.size(); ++k)
+        std::memcpy(fields + (size_t)slot[k] * g.n, r->fields.data() + r->field_offsets[k], (size_t)g.n * 4);
+    return MRC_OK;
+}
+
+uint32_t mrc_result_count(const mrc_result *r) { return r ? r->n : 0; }
+const uint64_t *mrc_result_path_offsets(const mrc_result *r) { return r ? r->offsets.data() : nullptr; }
+const uint32_t *mrc_result_path_cells(const mrc_result *r) { return r ? r->cells.data() : nullptr; }
+const uint32_t *mrc_result_search_costs(const mrc_result *r) { return r ? r->costs.data() : nullptr; }
+const uint64_t *mrc_result_field_offsets(const mrc_result *r) {
+    return r && r->has_fields ? r->field_offsets.data() : nullptr;
+}
+const uint32_t *mrc_result_fields(const mrc_result *r) { return r && r->has_fields ? r->fields.data() : nullptr; }
+const mrc_window *mrc_result_field_windows(const mrc_result *r) { return r ? r->field_windows.data() : nullptr; }
+uint32_t mrc_result_retried(const mrc_result *r) { return r ? r->retried : 0; }
+void mrc_result_free(mrc_result *r) { delete r; }
+
+mrc_status mrc_board_create(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *edges, mrc_board **out) {
+    if (!ctx || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    std::unique_ptr<mrc_board> b(new mrc_board());
+    MRC_TRY(board_build(ctx, grid, edges, true, b.get()));
+    MRC_CUDA(cudaStreamSynchronize(ctx->stream), "upload board");
+    *out = b.release();
+    return MRC_OK;
+}
+
+void mrc_board_destroy(mrc_board *board) {
+    if (!board) return;
+    mrc_context *ctx = board->ctx;
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        delete board;
+    } else {
+        delete board;
+    }
+}
+
+mrc_status mrc_batch_create(mrc_context *ctx, const mrc_board *board, const mrc_net *nets, uint32_t n_nets,
+                            const mrc_window *windows, uint32_t flags, mrc_batch **out) {
+    if (!ctx || !board || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, flags);
+    if (lock.st != MRC_OK) return lock.st;
+    MRC_TRY(set_device(ctx));
+    std::vector<NetCopy> nc;
+    MRC_TRY(validate_nets(board->view, nets, n_nets, &nc));
+    std::vector<mrc_window> wins;
+    MRC_TRY(collect_windows(board->view, nc, windows, &wins));
+    std::unique_ptr<mrc_batch> bt(new mrc_batch());
+    MRC_TRY(batch_build(ctx, board, std::move(nc), std::move(wins), flags, bt.get()));
+    MRC_CUDA(cudaStreamSynchronize(ctx->stream), "stage batch");
+    *out = bt.release();
+    return MRC_OK;
+}
+
+mrc_status mrc_batch_launch(mrc_context *ctx, mrc_batch *batch, void *stream) {
+    if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    return batch_launch(batch, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+mrc_status mrc_batch_finish(mrc_context *ctx, mrc_batch *batch, mrc_result **out) {
+    if (!ctx || !batch || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    if (!batch->stream) return fail(MRC_ERR_INVALID_ARGUMENT, "batch was never launched");
+    return solve(ctx, batch->board, {}, {}, batch->flags, out, batch);
+}
+
+uint32_t mrc_batch_kernel_launches(const mrc_batch *batch) { return batch ? batch->launches : 0; }
+uint64_t mrc_batch_window_cells(const mrc_batch *batch) { return batch ? batch->total_cells : 0; }
+
+float mrc_batch_relax_ms(const mrc_batch *batch) {
+    if (!batch || !batch->ev0 || !batch->ev1) return -1.0f;
+    float ms = -1.0f;
+    if (cudaEventElapsedTime(&ms, batch->ev0, batch->ev1) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return -1.0f;
+    }
+    return ms;
+}
+
+void mrc_batch_destroy(mrc_batch *batch) {
+    if (!batch) return;
+    mrc_context *ctx = batch->ctx;
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        delete batch;
+    } else {
+        delete batch;
+    }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The plain form: one net per launch sequence, a host read of the changed
+// flag after every Jacobi round (the reference's M3 loop, gpu.rs:1242-1303).
+
+namespace {
+
+mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &net, const mrc_window &win,
+                     uint32_t *cost, std::vector<uint32_t> *path, std::vector<uint32_t> *field) {
+    const GridView &g = board->view;
+    cudaStream_t st = ctx->stream;
+    DevField f{};
+    f.src = net.src;
+    f.dst = net.dst;
+    f.x0 = win.x0;
+    f.y0 = win.y0;
+    f.ww = win.x1 - win.x0 + 1;
+    f.wh = win.y1 - win.y0 + 1;
+    f.lab_off = 0;
+    f.pad_off = 0;
+    f.n_pads = (uint32_t)net.pads.size();
+    f.vpad_off = f.n_pads;
+    f.n_vpads = (uint32_t)net.vpads.size();
+    f.out = 0;
+    const uint64_t wc = (uint64_t)f.ww * f.wh * g.layers;
+    std::vector<uint32_t> pads(net.pads);
+    pads.insert(pads.end(), net.vpads.begin(), net.vpads.end());
+    DBuf d_pads, d_a, d_ha, d_b, d_hb, d_ctl, d_field, d_costs, d_lens, d_off, d_cells;
+    MRC_TRY(upload(ctx, d_pads, pads.data(), pads.size() * 4, "plain pads"));
+    MRC_TRY(upload(ctx, d_field, &f, sizeof(f), "plain field"));
+    MRC_TRY(d_a.get(ctx, wc * 4, "plain labels"));
+    MRC_TRY(d_ha.get(ctx, wc * 4, "plain labels"));
+    MRC_TRY(d_b.get(ctx, wc * 4, "plain labels"));
+    MRC_TRY(d_hb.get(ctx, wc * 4, "plain labels"));
+    MRC_TRY(d_ctl.get(ctx, 64, "plain flags"));
+    MRC_CUDA(cudaMemsetAsync(d_a.p, 0xFF, wc * 4, st), "plain init");
+    MRC_CUDA(cudaMemsetAsync(d_ha.p, 0xFF, wc * 4, st), "plain init");
+    MRC_CUDA(cudaMemsetAsync(d_ctl.p, 0, 64, st), "plain init");
+    const uint32_t plane = g.w * g.h;
+    const uint32_t sx = (net.src % plane) % g.w, sy = (net.src % plane) / g.w, sl = net.src / plane;
+    const bool src_ok = sx >= win.x0 && sx <= win.x1 && sy >= win.y0 && sy <= win.y1;
+    static const uint32_t zero = 0;
+    if (src_ok) {
+        const uint64_t lc = ((uint64_t)sl * f.wh + (sy - f.y0)) * f.ww + (sx - f.x0);
+        MRC_CUDA(cudaMemcpyAsync(d_a.as<uint32_t>() + lc, &zero, 4, cudaMemcpyHostToDevice, st), "plain seed");
+        MRC_CUDA(cudaMemcpyAsync(d_ha.as<uint32_t>() + lc, &zero, 4, cudaMemcpyHostToDevice, st), "plain seed");
+    }
+    PlainArgs pa;
+    pa.board = board->dev;
+    pa.field = f;
+    pa.pads = d_pads.as<uint32_t>();
+    pa.changed = d_ctl.as<uint32_t>();
+    uint32_t *in_d = d_a.as<uint32_t>(), *in_h = d_ha.as<uint32_t>();
+    uint32_t *out_d = d_b.as<uint32_t>(), *out_h = d_hb.as<uint32_t>();
+    const uint64_t round_limit = wc + 2;
+    for (uint64_t round = 0; src_ok; ++round) {
+        if (round > round_limit) return fail(MRC_ERR_ITERATION_LIMIT, "plain relaxation did not converge");
+        uint32_t changed = 0;
+        MRC_CUDA(cudaMemsetAsync(pa.changed, 0, 4, st), "plain round");
+        pa.in_dist = in_d;
+        pa.in_hops = in_h;
+        pa.out_dist = out_d;
+        pa.out_hops = out_h;
+        MRC_CUDA(plain_round_launch(pa, wc, st), "plain round");
+        MRC_CUDA(cudaMemcpyAsync(&changed, pa.changed, 4, cudaMemcpyDeviceToHost, st), "plain flag");
+        MRC_CUDA(cudaStreamSynchronize(st), "plain round");
+        std::swap(in_d, out_d);
+        std::swap(in_h, out_h);
+        if (!changed) break;
+    }
+    MRC_TRY(d_costs.get(ctx, 4, "plain cost"));
+    MRC_TRY(d_lens.get(ctx, 4, "plain len"));
+    MRC_TRY(d_off.get(ctx, 16, "plain offsets"));
+    MRC_TRY(d_cells.get(ctx, wc * 4, "plain path"));
+    PathArgs pt;
+    pt.board = board->dev;
+    pt.fields = d_field.as<DevField>();
+    pt.n_fields = 1;
+    pt.pads = d_pads.as<uint32_t>();
+    pt.dist = in_d;
+    pt.hops = in_h;
+    pt.costs = d_costs.as<uint32_t>();
+    pt.lens = d_lens.as<uint32_t>();
+    pt.offsets = d_off.as<unsigned long long>();
+    pt.cells = d_cells.as<uint32_t>();
+    pt.status = d_ctl.as<uint32_t>() + 1;
+    MRC_CUDA(path_launch(pt, st), "plain path");
+    uint32_t status = 0;
+    uint64_t off[2];
+    MRC_CUDA(cudaMemcpyAsync(&status, pt.status, 4, cudaMemcpyDeviceToHost, st), "plain status");
+    MRC_CUDA(cudaMemcpyAsync(cost, pt.costs, 4, cudaMemcpyDeviceToHost, st), "plain cost");
+    MRC_CUDA(cudaMemcpyAsync(off, pt.offsets, 16, cudaMemcpyDeviceToHost, st), "plain offsets");
+    MRC_CUDA(cudaStreamSynchronize(st), "plain path");
+    if (status) return status_error(status);
+    path->resize(off[1]);
+    if (off[1]) MRC_CUDA(cudaMemcpy(path->data(), pt.cells, off[1] * 4, cudaMemcpyDeviceToHost), "plain path");
+    if (field) {
+        field->resize(wc);
+        MRC_CUDA(cudaMemcpy(field->data(), in_d, wc * 4, cudaMemcpyDeviceToHost), "plain field");
+    }
+    return MRC_OK;
+}
+
+}  // namespace
+
+extern "C" mrc_status mrc_route_isolated_plain(mrc_context *ctx, const mrc_isolated_request *req, uint32_t flags,
+                                               mrc_result **out) {
+    if (!ctx || !req || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, flags);
+    if (lock.st != MRC_OK) return lock.st;
+    MRC_TRY(set_device(ctx));
+    GridView g;
+    MRC_TRY(view_grid(req->grid, &g));
+    if (req->n_nets && !req->windows) return fail(MRC_ERR_INVALID_ARGUMENT, "windows is NULL");
+    std::vector<NetCopy> nets;
+    MRC_TRY(validate_nets(g, req->nets, req->n_nets, &nets));
+    std::vector<mrc_window> wins;
+    MRC_TRY(collect_windows(g, nets, req->windows, &wins));
+    mrc_board board;
+    MRC_TRY(board_build(ctx, req->grid, &req->edges, false, &board));
+    const bool keep = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
+    std::unique_ptr<mrc_result> r(new mrc_result());
+    const uint32_t n = (uint32_t)nets.size();
+    r->n = n;
+    r->costs.assign(n, kMax);
+    r->offsets.assign(n + 1, 0);
+    r->field_windows = wins;
+    r->has_fields = keep;
+    r->field_offsets.assign(n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        std::vector<uint32_t> path, field;
+        uint32_t cost = kMax;
+        MRC_TRY(plain_one(ctx, &board, nets[i], wins[i], &cost, &path, keep ? &field : nullptr));
+        if (cost == kMax && (flags & MRC_FLAG_RETRY_FULL) && !is_full(wins[i], g.w, g.h)) {
+            r->field_windows[i] = full_window(g.w, g.h);
+            r->retried++;
+            MRC_TRY(plain_one(ctx, &board, nets[i], r->field_windows[i], &cost, &path, keep ? &field : nullptr));
+        }
+        r->costs[i] = cost;
+        r->offsets[i + 1] = r->offsets[i] + path.size();
+        r->cells.insert(r->cells.end(), path.begin(), path.end());
+        if (keep) {
+            r->field_offsets[i + 1] = r->field_offsets[i] + field.size();
+            r->fields.insert(r->fields.end(), field.begin(), field.end());
+        }
+    }
+    *out = r.release();
+    return MRC_OK;
+}

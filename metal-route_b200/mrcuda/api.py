@@ -1,0 +1,476 @@
+"""ctypes binding of libmr_cuda.so (include/mr_cuda.h).
+
+This module mirrors the reference's provider seam so that callers read like
+metalroute's own code:
+
+* ``CudaIsolatedProvider.route_isolated_batch(request)`` — the
+  ``IsolatedRouteProvider`` trait (crates/mr-cpu/src/negotiated.rs:554-560):
+  aligned ``Optional[List[CellIdx]]`` per net, all-or-error.
+* ``Engine.route_isolated_batch`` — ``metal_route_isolated_batch`` plus the
+  adapter's full-board retry (crates/mr-metal/src/lib.rs:414-558,
+  crates/mr-cli/src/lib.rs:549-607), returning paths and search costs.
+* ``Engine.route_lee`` / ``Engine.distance_fields`` — the ``Router`` contract
+  of LeeRouter/MetalRouter and the batched complete fields.
+
+There is no CPU fallback anywhere in here: if the CUDA library or device is
+unavailable every call raises ``BackendUnavailable`` and the caller decides.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .types import (
+    COST_MAX,
+    Grid,
+    IsolatedRouteRequest,
+    IsolatedRouteWindow,
+    NetEndpoints,
+)
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmr_cuda.so")
+
+MRC_OK = 0
+MRC_FLAG_RETRY_FULL = 0x1
+MRC_FLAG_KEEP_FIELDS = 0x2
+MRC_FLAG_NO_WAIT = 0x4
+MRC_FLAG_TIME_KERNELS = 0x8
+NO_PATH = 0xFFFFFFFF
+
+
+class RouterError(Exception):
+    """Base of the errors a routing call may raise (core/src/lib.rs:698-708)."""
+
+    status = -1
+
+
+class InvalidArgument(RouterError):
+    status = 1
+
+
+class MalformedGrid(RouterError):
+    status = 2
+
+
+class InvalidEndpoint(RouterError):
+    status = 3
+
+
+class BackendUnavailable(RouterError):
+    status = 4
+
+
+class Busy(BackendUnavailable):
+    status = 5
+
+
+class IterationLimit(BackendUnavailable):
+    status = 6
+
+
+class OutOfMemory(BackendUnavailable):
+    status = 7
+
+
+class LimitExceeded(BackendUnavailable):
+    status = 8
+
+
+_ERRORS = {c.status: c for c in (InvalidArgument, MalformedGrid, InvalidEndpoint, BackendUnavailable, Busy,
+                                 IterationLimit, OutOfMemory, LimitExceeded)}
+
+
+class _Grid(C.Structure):
+    _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("layers", C.c_uint32), ("cost", C.c_void_p),
+                ("board_constraint", C.c_void_p), ("via_forbidden", C.c_void_p)]
+
+
+class _Net(C.Structure):
+    _fields_ = [("src", C.c_uint32), ("dst", C.c_uint32), ("passable_pads", C.c_void_p),
+                ("n_passable_pads", C.c_uint32), ("via_passable_pads", C.c_void_p),
+                ("n_via_passable_pads", C.c_uint32)]
+
+
+class _Window(C.Structure):
+    _fields_ = [("x0", C.c_uint32), ("y0", C.c_uint32), ("x1", C.c_uint32), ("y1", C.c_uint32)]
+
+
+class _Edges(C.Structure):
+    _fields_ = [("x_edge_costs", C.c_void_p), ("n_x_edge_costs", C.c_uint32), ("y_edge_costs", C.c_void_p),
+                ("n_y_edge_costs", C.c_uint32), ("via_edge_costs", C.c_void_p), ("via_allowed", C.c_void_p),
+                ("n_via_edge_costs", C.c_uint32), ("directed_in_costs", C.c_void_p)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("grid", C.POINTER(_Grid)), ("nets", C.c_void_p), ("n_nets", C.c_uint32),
+                ("windows", C.c_void_p), ("edges", _Edges)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load_library(path: str = _LIB_PATH) -> C.CDLL:
+    """Load libmr_cuda.so; raises BackendUnavailable when it is missing."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise BackendUnavailable(f"CUDA engine library not built: {path}")
+        L = C.CDLL(path)
+        vp, u32, u64p, u32p = C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)
+        sig = {
+            "mrc_abi_version": (u32, []),
+            "mrc_last_error": (C.c_char_p, [vp]),
+            "mrc_context_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+            "mrc_context_destroy": (None, [vp]),
+            "mrc_route_isolated_batch": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(vp)]),
+            "mrc_route_isolated_plain": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(vp)]),
+            "mrc_route_lee": (C.c_int, [vp, C.POINTER(_Grid), vp, u32, C.POINTER(vp)]),
+            "mrc_distance_fields": (C.c_int, [vp, C.POINTER(_Grid), vp, u32, vp]),
+            "mrc_result_count": (u32, [vp]),
+            "mrc_result_path_offsets": (u64p, [vp]),
+            "mrc_result_path_cells": (u32p, [vp]),
+            "mrc_result_search_costs": (u32p, [vp]),
+            "mrc_result_field_offsets": (u64p, [vp]),
+            "mrc_result_fields": (u32p, [vp]),
+            "mrc_result_field_windows": (C.POINTER(_Window), [vp]),
+            "mrc_result_retried": (u32, [vp]),
+            "mrc_result_free": (None, [vp]),
+            "mrc_board_create": (C.c_int, [vp, C.POINTER(_Grid), C.POINTER(_Edges), C.POINTER(vp)]),
+            "mrc_board_destroy": (None, [vp]),
+            "mrc_batch_create": (C.c_int, [vp, vp, vp, u32, vp, u32, C.POINTER(vp)]),
+            "mrc_batch_launch": (C.c_int, [vp, vp, vp]),
+            "mrc_batch_finish": (C.c_int, [vp, vp, C.POINTER(vp)]),
+            "mrc_batch_kernel_launches": (u32, [vp]),
+            "mrc_batch_window_cells": (C.c_uint64, [vp]),
+            "mrc_batch_relax_ms": (C.c_float, [vp]),
+            "mrc_batch_destroy": (None, [vp]),
+            "mrc_net_windows": (C.c_int, [u32, u32, u32, vp, u32, vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+        return L
+
+
+def exported_symbols() -> List[str]:
+    """Names declared in include/mr_cuda.h that the binding resolves."""
+    L = load_library()
+    return [n for n in dir(L) if n.startswith("mrc_")]
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1))
+
+
+class _Marshal:
+    """Keeps every numpy buffer alive for the duration of one C call."""
+
+    def __init__(self):
+        self.keep = []
+
+    def arr(self, a: Optional[np.ndarray]):
+        if a is None:
+            return None
+        self.keep.append(a)
+        return a.ctypes.data
+
+    def grid(self, g: Grid) -> _Grid:
+        s = _Grid(g.dims.w, g.dims.h, g.dims.layers, self.arr(g.cost), self.arr(g.board_constraint),
+                  self.arr(g.via_forbidden))
+        self.keep.append(s)
+        return s
+
+    def nets(self, nets: Sequence[NetEndpoints]):
+        arr = (_Net * max(len(nets), 1))()
+        for i, n in enumerate(nets):
+            pads = _u32(n.passable_pads) if len(n.passable_pads) else None
+            vpads = _u32(n.via_passable_pads) if len(n.via_passable_pads) else None
+            arr[i] = _Net(n.src, n.dst, self.arr(pads), len(n.passable_pads), self.arr(vpads),
+                          len(n.via_passable_pads))
+        self.keep.append(arr)
+        return C.cast(arr, C.c_void_p)
+
+    def windows(self, wins: Optional[Sequence[IsolatedRouteWindow]]):
+        if wins is None:
+            return None
+        arr = (_Window * max(len(wins), 1))()
+        for i, w in enumerate(wins):
+            arr[i] = _Window(w.x0, w.y0, w.x1, w.y1)
+        self.keep.append(arr)
+        return C.cast(arr, C.c_void_p)
+
+    def edges(self, x, y, vias, directed=None) -> _Edges:
+        xe, ye = _u32(x), _u32(y)
+        ve = np.array([0 if v is None else int(v) for v in vias], dtype=np.uint32)
+        va = np.array([0 if v is None else 1 for v in vias], dtype=np.uint8)
+        d = None if directed is None else _u32(directed)
+        e = _Edges(self.arr(xe) if xe.size else None, xe.size, self.arr(ye) if ye.size else None, ye.size,
+                   self.arr(ve) if ve.size else None, self.arr(va) if va.size else None, ve.size, self.arr(d))
+        self.keep.append(e)
+        return e
+
+
+@dataclass
+class IsolatedBatchResult:
+    """Per-net outputs, aligned with the request's nets."""
+
+    paths: List[Optional[List[int]]]
+    search_costs: List[int]
+    fields: Optional[List[np.ndarray]] = None
+    field_windows: Optional[List[IsolatedRouteWindow]] = None
+    retried: int = 0
+
+
+def _take_result(L, res, n: int, fields: bool, layers: int = 1) -> IsolatedBatchResult:
+    try:
+        cnt = L.mrc_result_count(res)
+        assert cnt == n, (cnt, n)
+        off = np.ctypeslib.as_array(L.mrc_result_path_offsets(res), shape=(n + 1,)).copy()
+        total = int(off[-1])
+        cells = (np.ctypeslib.as_array(L.mrc_result_path_cells(res), shape=(total,)).copy()
+                 if total else np.zeros(0, np.uint32))
+        costs = (np.ctypeslib.as_array(L.mrc_result_search_costs(res), shape=(n,)).copy()
+                 if n else np.zeros(0, np.uint32))
+        paths = [cells[off[i]:off[i + 1]].tolist() if off[i + 1] > off[i] else None for i in range(n)]
+        out = IsolatedBatchResult(paths, [int(c) for c in costs], retried=int(L.mrc_result_retried(res)))
+        wp = L.mrc_result_field_windows(res)
+        if n and wp:
+            out.field_windows = [IsolatedRouteWindow(wp[i].x0, wp[i].y0, wp[i].x1, wp[i].y1) for i in range(n)]
+        if fields:
+            fo = np.ctypeslib.as_array(L.mrc_result_field_offsets(res), shape=(n + 1,)).copy()
+            ft = int(fo[-1])
+            fa = (np.ctypeslib.as_array(L.mrc_result_fields(res), shape=(ft,)).copy() if ft
+                  else np.zeros(0, np.uint32))
+            out.fields = [fa[fo[i]:fo[i + 1]] for i in range(n)]
+        return out
+    finally:
+        L.mrc_result_free(res)
+
+
+class Board:
+    """A board resident in HBM (cost, masks, edge prices)."""
+
+    def __init__(self, engine: "Engine", grid: Grid, x, y, vias, directed=None):
+        self.engine = engine
+        self.grid = grid
+        m = _Marshal()
+        h = C.c_void_p()
+        engine._check(engine.lib.mrc_board_create(engine.ctx, C.byref(m.grid(grid)),
+                                                  C.byref(m.edges(x, y, vias, directed)), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self.engine.lib.mrc_board_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """A validated batch of nets staged against a resident Board."""
+
+    def __init__(self, board: Board, nets: Sequence[NetEndpoints],
+                 windows: Optional[Sequence[IsolatedRouteWindow]] = None, retry_full: bool = True,
+                 keep_fields: bool = False, time_kernels: bool = False):
+        self.board = board
+        self.engine = board.engine
+        self.n = len(nets)
+        self.keep_fields = keep_fields
+        flags = ((MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
+                 | (MRC_FLAG_TIME_KERNELS if time_kernels else 0))
+        m = _Marshal()
+        h = C.c_void_p()
+        e = self.engine
+        e._check(e.lib.mrc_batch_create(e.ctx, board.handle, m.nets(nets), len(nets), m.windows(windows), flags,
+                                        C.byref(h)))
+        self.handle = h
+
+    def launch(self, stream: int = 0) -> None:
+        """Enqueue the solve on a cudaStream_t (an integer handle, 0 = the engine's stream)."""
+        e = self.engine
+        e._check(e.lib.mrc_batch_launch(e.ctx, self.handle, C.c_void_p(stream) if stream else None))
+
+    def finish(self) -> IsolatedBatchResult:
+        e = self.engine
+        res = C.c_void_p()
+        e._check(e.lib.mrc_batch_finish(e.ctx, self.handle, C.byref(res)))
+        return _take_result(e.lib, res, self.n, self.keep_fields)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.engine.lib.mrc_batch_kernel_launches(self.handle))
+
+    def relax_ms(self) -> float:
+        """Device time of the relax kernel in the last launch (needs time_kernels)."""
+        return float(self.engine.lib.mrc_batch_relax_ms(self.handle))
+
+    @property
+    def window_cells(self) -> int:
+        return int(self.engine.lib.mrc_batch_window_cells(self.handle))
+
+    def close(self):
+        if self.handle:
+            self.engine.lib.mrc_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """One CUDA context of the engine (one per process per device)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        ctx = C.c_void_p()
+        self.ctx = None
+        self._check(self.lib.mrc_context_create(int(device), C.byref(ctx)))
+        self.ctx = ctx
+
+    def close(self):
+        if self.ctx:
+            self.lib.mrc_context_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status: int) -> None:
+        if status != MRC_OK:
+            msg = self.lib.mrc_last_error(self.ctx)
+            msg = msg.decode() if msg else ""
+            raise _ERRORS.get(status, RouterError)(msg)
+
+    # -- the provider seam ---------------------------------------------------
+    def _request(self, m: _Marshal, req: IsolatedRouteRequest) -> _Request:
+        if len(req.windows) != len(req.nets):
+            raise BackendUnavailable("isolated request windows are not net-aligned")
+        r = _Request(C.pointer(m.grid(req.grid)), m.nets(req.nets), len(req.nets), m.windows(req.windows),
+                     m.edges(req.x_edge_costs, req.y_edge_costs, req.via_edge_costs, req.directed_in_costs))
+        m.keep.append(r)
+        return r
+
+    def route_isolated_batch(self, req: IsolatedRouteRequest, retry_full: bool = True, keep_fields: bool = False,
+                             no_wait: bool = False) -> IsolatedBatchResult:
+        m = _Marshal()
+        r = self._request(m, req)
+        flags = ((MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
+                 | (MRC_FLAG_NO_WAIT if no_wait else 0))
+        res = C.c_void_p()
+        self._check(self.lib.mrc_route_isolated_batch(self.ctx, C.byref(r), flags, C.byref(res)))
+        return _take_result(self.lib, res, len(req.nets), keep_fields)
+
+    def route_isolated_plain(self, req: IsolatedRouteRequest, retry_full: bool = True,
+                             keep_fields: bool = False) -> IsolatedBatchResult:
+        m = _Marshal()
+        r = self._request(m, req)
+        flags = (MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
+        res = C.c_void_p()
+        self._check(self.lib.mrc_route_isolated_plain(self.ctx, C.byref(r), flags, C.byref(res)))
+        return _take_result(self.lib, res, len(req.nets), keep_fields)
+
+    # -- Router contract and fields -------------------------------------------
+    def route_lee(self, grid: Grid, nets: Sequence[NetEndpoints]) -> "BoardRoute":
+        m = _Marshal()
+        res = C.c_void_p()
+        self._check(self.lib.mrc_route_lee(self.ctx, C.byref(m.grid(grid)), m.nets(nets), len(nets),
+                                           C.byref(res)))
+        out = _take_result(self.lib, res, len(nets), False)
+        return BoardRoute.from_paths(grid, nets, out.paths, out.search_costs)
+
+    def distance_fields(self, grid: Grid, sources: Sequence[int]) -> np.ndarray:
+        m = _Marshal()
+        src = _u32(sources)
+        out = np.zeros((len(sources), len(grid.dims)), dtype=np.uint32)
+        if len(sources):
+            self._check(self.lib.mrc_distance_fields(self.ctx, C.byref(m.grid(grid)), m.arr(src), len(sources),
+                                                     m.arr(out)))
+        return out
+
+    def board(self, grid: Grid, x, y, vias, directed=None) -> Board:
+        return Board(self, grid, x, y, vias, directed)
+
+
+def net_windows(dims, nets: Sequence[NetEndpoints]) -> List[IsolatedRouteWindow]:
+    """net_window (negotiated.rs:568-594), computed by the library."""
+    L = load_library()
+    m = _Marshal()
+    out = (_Window * max(len(nets), 1))()
+    st = L.mrc_net_windows(dims.w, dims.h, dims.layers, m.nets(nets), len(nets), C.cast(out, C.c_void_p))
+    if st != MRC_OK:
+        raise _ERRORS.get(st, RouterError)("net_windows failed")
+    return [IsolatedRouteWindow(out[i].x0, out[i].y0, out[i].x1, out[i].y1) for i in range(len(nets))]
+
+
+@dataclass
+class RouteResult:
+    net: str
+    path: List[int]
+    cost: int
+
+
+@dataclass
+class BoardRoute:
+    """mr_core::BoardRoute (core/src/lib.rs:552-594)."""
+
+    results: List[RouteResult]
+    unrouted: List[str]
+    congestion: np.ndarray
+
+    @staticmethod
+    def from_paths(grid: Grid, nets, paths, costs) -> "BoardRoute":
+        results, unrouted = [], []
+        cong = np.zeros(len(grid.dims), dtype=np.uint32)
+        for n, p, c in zip(nets, paths, costs):
+            if p is None:
+                unrouted.append(n.net)
+                continue
+            results.append(RouteResult(n.net, p, c))
+            cong[np.unique(np.asarray(p, dtype=np.int64))] += 1
+        return BoardRoute(results, unrouted, cong)
+
+
+class CudaIsolatedProvider:
+    """IsolatedRouteProvider backed by the CUDA engine (negotiated.rs:554-560).
+
+    Mirrors MetalIsolatedProvider (crates/mr-cli/src/lib.rs:612-625): a busy
+    engine fails immediately (the router then takes its CPU path) instead of
+    queueing behind another board's batch."""
+
+    def __init__(self, engine: Optional[Engine] = None, device: int = 0):
+        self.engine = engine or Engine(device)
+
+    def route_isolated_batch(self, request: IsolatedRouteRequest) -> List[Optional[List[int]]]:
+        out = self.engine.route_isolated_batch(request, retry_full=True, no_wait=True)
+        if len(out.paths) != len(request.nets):
+            raise BackendUnavailable("CUDA isolated result is not net-aligned")
+        return out.paths
+
+
+__all__ = [
+    "Engine", "Board", "Batch", "CudaIsolatedProvider", "IsolatedBatchResult", "BoardRoute", "RouteResult",
+    "RouterError", "InvalidArgument", "MalformedGrid", "InvalidEndpoint", "BackendUnavailable", "Busy",
+    "IterationLimit", "OutOfMemory", "LimitExceeded", "net_windows", "load_library", "exported_symbols",
+    "COST_MAX", "NO_PATH",
+]
