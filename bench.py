@@ -55,12 +55,14 @@ def _traffic_per_launch(kernel_profile: str):
     return None
 
 
-def _workload(name: str, rank: int):
+def _workload(name: str, rank: int, nets: int = 0):
     from mrcuda import workloads as W
 
     if name == "plain":
-        return W.plain_board(seed=1 + 1000 * rank)
-    return W.congestion_board(seed=2, net_seed=None if rank == 0 else 2 + 1000 * rank)
+        wl = W.plain_board(seed=1 + 1000 * rank)
+    else:
+        wl = W.congestion_board(seed=2, net_seed=None if rank == 0 else 2 + 1000 * rank)
+    return W.scaled(wl, nets) if nets else wl
 
 
 class ClockSampler:
@@ -131,7 +133,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    wl = _workload(args.workload, 0)
+    wl = _workload(args.workload, 0, args.nets)
     cores = os.cpu_count() or 1
     n_sample = min(args.cpu_sample, len(wl.nets))
     for _ in range(args.warmup):
@@ -176,7 +178,7 @@ def run_engine(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    wl = _workload(args.workload, rank)
+    wl = _workload(args.workload, rank, args.nets)
     eng = mrcuda.Engine(local)
     board = eng.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
     batch = mrcuda.Batch(board, wl.nets, wl.windows, retry_full=True, time_kernels=True)
@@ -214,6 +216,7 @@ def run_engine(args):
     if dist:
         dist.barrier()
     clk = clocks.stop()
+    work = batch.stats()
     ms = statistics.fmean(step_ms)
     ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -247,7 +250,7 @@ def run_engine(args):
     alg_bytes = wl.window_cells() * wl.bytes_per_cell() + 4 * path_cells
     relax_avg = statistics.fmean(relax_ms) if relax_ms and min(relax_ms) > 0 else ms
     achieved = alg_bytes / (relax_avg / 1000.0) / 1e9
-    traffic = _traffic_per_launch(f"relax_tiles_{args.workload}.md")
+    traffic = _traffic_per_launch(f"relax_rounds_{args.workload}.md")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -259,9 +262,10 @@ def run_engine(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": batch.kernel_launches * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "relax_tiles_kernel",
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "relax_rounds_kernel",
                      "kernel_ms": relax_avg, "algorithmic_bytes_per_launch": int(alg_bytes),
-                     "bytes_per_cell": wl.bytes_per_cell()},
+                     "bytes_per_cell": wl.bytes_per_cell(), "tile_activations": work["activations"],
+                     "in_tile_sweeps": work["sweeps"], "rounds": work["rounds"], "tiles": work["tiles"]},
         "clocks": clk,
     }
 
@@ -299,6 +303,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", choices=["congestion", "plain"], default="congestion")
+    ap.add_argument("--nets", type=int, default=0, help="route only the first N nets (0 = all)")
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--plain-sample", type=int, default=8)
     ap.add_argument("--no-plain", action="store_true")

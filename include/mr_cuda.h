@@ -191,6 +191,11 @@ uint32_t mrc_batch_kernel_launches(const mrc_batch *batch);
  * recorded on the launching stream (batch created with MRC_FLAG_TIME_KERNELS;
  * call after the stream has been synchronised).  Negative when unavailable. */
 float mrc_batch_relax_ms(const mrc_batch *batch);
+/* Work counters of the last launch (after the stream has been synchronised):
+ * out[0] = tile activations, out[1] = in-tile sweeps, out[2] = rounds,
+ * out[3] = tiles in the batch.  Returns MRC_ERR_BACKEND_UNAVAILABLE if the
+ * counters cannot be read. */
+mrc_status mrc_batch_stats(const mrc_batch *batch, uint64_t out[4]);
 /* Cells in all windows of the batch (the per-launch work unit). */
 uint64_t mrc_batch_window_cells(const mrc_batch *batch);
 void mrc_batch_destroy(mrc_batch *batch);

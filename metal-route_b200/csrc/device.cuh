@@ -53,11 +53,22 @@ struct DevBoard {
 struct DevField {
     uint32_t src, dst;          // global CellIdx
     uint32_t x0, y0, ww, wh;    // window origin and extent
-    uint64_t lab_off;           // first cell of this field in the label arrays
+    uint64_t lab_off;           // first cell of this field in the label arena
     uint32_t pad_off, n_pads;   // sorted own pads in the pad arena
     uint32_t vpad_off, n_vpads; // sorted via exemptions in the pad arena
     uint32_t out;               // output slot (the net's request index)
-    uint32_t pad_;
+    uint32_t tile_off;          // first tile of this field in the tile-state arrays
+};
+
+// Control block of one batch launch (device memory, zeroed before launch).
+struct Ctl {
+    uint32_t count[3];          // items in the three rotating tile lists
+    uint32_t head[3];           // consumption cursors
+    uint32_t bar_count, bar_gen;
+    uint32_t status;
+    uint32_t rounds;
+    unsigned long long activations;
+    unsigned long long sweeps;
 };
 
 __device__ __forceinline__ uint32_t capmul(uint32_t e, uint32_t w) {

@@ -252,10 +252,6 @@ struct mrc_board {
     DevBoard dev{};
 };
 
-namespace mrc {
-cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, uint64_t n, cudaStream_t st);
-}
-
 namespace {
 
 mrc_status upload(mrc_context *ctx, DBuf &buf, const void *src, size_t bytes, const char *what) {
@@ -352,11 +348,11 @@ struct mrc_batch {
     uint32_t flags = 0;
     std::vector<NetCopy> nets;
     std::vector<mrc_window> windows;
-    std::vector<DevField> fields;  // processing order
+    std::vector<DevField> fields;  // ascending lab_off (largest windows first)
     uint64_t total_cells = 0;
-    uint32_t max_tiles = 0, tile_h = 32, grid = 1;
+    uint32_t total_tiles = 0, max_tiles = 0, tile_h = 32, grid = 1;
     size_t smem = 0;
-    DBuf d_fields, d_pads, d_dist, d_hops, d_scratch, d_costs, d_lens, d_offsets, d_cells, d_ctl;
+    DBuf d_fields, d_pads, d_lab, d_tstamp, d_tvisit, d_lists, d_costs, d_lens, d_offsets, d_cells, d_ctl, d_out;
     uint32_t launches = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -368,7 +364,6 @@ struct mrc_batch {
 
 namespace {
 
-constexpr uint32_t kActivationFactor = 256;
 
 mrc_status choose_tile(mrc_context *ctx, uint32_t layers, bool directed, uint32_t *tile_h, size_t *smem) {
     const size_t budget_fast = 110u << 10;  // two CTAs per SM
@@ -406,7 +401,7 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cells_of(a) > cells_of(b); });
     std::vector<uint32_t> pads;
     bt->fields.resize(n);
-    uint64_t off = 0;
+    uint64_t off = 0, toff = 0;
     uint32_t max_tiles = 1;
     for (uint32_t k = 0; k < n; ++k) {
         const uint32_t i = order[k];
@@ -428,30 +423,34 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
         f.n_vpads = (uint32_t)nc.vpads.size();
         pads.insert(pads.end(), nc.vpads.begin(), nc.vpads.end());
         f.out = i;
-        f.pad_ = 0;
         const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + bt->tile_h - 1) / bt->tile_h);
-        if (tiles > (1u << 24)) return fail(MRC_ERR_LIMIT, "window has more than 2^24 tiles");
+        f.tile_off = (uint32_t)toff;
+        toff += tiles;
+        if (toff > 0x7FFFFFFFull) return fail(MRC_ERR_LIMIT, "batch has more than 2^31 tiles");
         max_tiles = std::max<uint32_t>(max_tiles, (uint32_t)tiles);
         if (pads.size() > 0xFFFFFFF0u) return fail(MRC_ERR_LIMIT, "pad lists exceed 2^32 entries");
     }
     bt->total_cells = off;
+    bt->total_tiles = (uint32_t)std::max<uint64_t>(toff, 1);
     bt->max_tiles = max_tiles;
     int per_sm = 1;
     MRC_CUDA(relax_configure(board->directed, bt->smem), "configure relax kernel");
     MRC_CUDA(relax_occupancy(board->directed, bt->smem, &per_sm), "relax occupancy");
-    per_sm = std::max(per_sm, 1);
-    bt->grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n, (uint64_t)ctx->sms * per_sm));
-    const uint32_t stride = max_tiles + (max_tiles + 31) / 32;
+    if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
+    // cooperative launch: every CTA must be co-resident
+    bt->grid = (uint32_t)ctx->sms * (uint32_t)per_sm;
     MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
     MRC_TRY(upload(ctx, bt->d_pads, pads.data(), pads.size() * 4, "upload pads"));
-    MRC_TRY(bt->d_dist.get(ctx, std::max<uint64_t>(off, 1) * 4, "dist labels"));
-    MRC_TRY(bt->d_hops.get(ctx, std::max<uint64_t>(off, 1) * 4, "hop labels"));
-    MRC_TRY(bt->d_scratch.get(ctx, (size_t)bt->grid * stride * 4, "tile queues"));
+    MRC_TRY(bt->d_lab.get(ctx, std::max<uint64_t>(off, 1) * 8, "labels"));
+    MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
+    MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
+    MRC_TRY(bt->d_lists.get(ctx, (size_t)bt->total_tiles * 3 * 8, "tile lists"));
     MRC_TRY(bt->d_costs.get(ctx, std::max<size_t>(n, 1) * 4, "costs"));
     MRC_TRY(bt->d_lens.get(ctx, std::max<size_t>(n, 1) * 4, "lengths"));
     MRC_TRY(bt->d_offsets.get(ctx, ((size_t)n + 1) * 8, "offsets"));
     MRC_TRY(bt->d_cells.get(ctx, std::max<uint64_t>(off, 1) * 4, "path cells"));
-    MRC_TRY(bt->d_ctl.get(ctx, 64, "control words"));
+    MRC_TRY(bt->d_ctl.get(ctx, sizeof(Ctl), "control block"));
+    if (flags & MRC_FLAG_KEEP_FIELDS) MRC_TRY(bt->d_out.get(ctx, std::max<uint64_t>(off, 1) * 4, "fields"));
     if (flags & MRC_FLAG_TIME_KERNELS) {
         MRC_CUDA(cudaEventCreate(&bt->ev0), "create event");
         MRC_CUDA(cudaEventCreate(&bt->ev1), "create event");
@@ -459,52 +458,64 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
     return MRC_OK;
 }
 
+PathArgs path_args(const mrc_batch *bt) {
+    PathArgs pa;
+    pa.board = bt->board->dev;
+    pa.fields = bt->d_fields.as<DevField>();
+    pa.n_fields = (uint32_t)bt->fields.size();
+    pa.pads = bt->d_pads.as<uint32_t>();
+    pa.lab = bt->d_lab.as<u64>();
+    pa.tvisit = bt->d_tvisit.as<uint32_t>();
+    pa.tile_h = bt->tile_h;
+    pa.costs = bt->d_costs.as<uint32_t>();
+    pa.lens = bt->d_lens.as<uint32_t>();
+    pa.offsets = bt->d_offsets.as<unsigned long long>();
+    pa.cells = bt->d_cells.as<uint32_t>();
+    pa.status = &bt->d_ctl.as<Ctl>()->status;
+    return pa;
+}
+
 mrc_status batch_launch(mrc_batch *bt, cudaStream_t st) {
     const uint32_t n = (uint32_t)bt->fields.size();
-    uint32_t *ctl = bt->d_ctl.as<uint32_t>();  // [0] work counter, [1] status
     bt->stream = st;
     bt->launches = 0;
-    MRC_CUDA(cudaMemsetAsync(ctl, 0, 64, st), "reset control words");
+    MRC_CUDA(cudaMemsetAsync(bt->d_ctl.p, 0, sizeof(Ctl), st), "reset control block");
+    MRC_CUDA(cudaMemsetAsync(bt->d_tstamp.p, 0, (size_t)bt->total_tiles * 4, st), "reset tile stamps");
+    MRC_CUDA(cudaMemsetAsync(bt->d_tvisit.p, 0, (size_t)bt->total_tiles * 4, st), "reset tile flags");
     RelaxArgs ra;
     ra.board = bt->board->dev;
     ra.fields = bt->d_fields.as<DevField>();
     ra.n_fields = n;
     ra.pads = bt->d_pads.as<uint32_t>();
-    ra.dist = bt->d_dist.as<uint32_t>();
-    ra.hops = bt->d_hops.as<uint32_t>();
-    ra.work_counter = ctl;
-    ra.tile_scratch = bt->d_scratch.as<uint32_t>();
-    ra.scratch_stride = bt->max_tiles + (bt->max_tiles + 31) / 32;
-    ra.max_tiles = bt->max_tiles;
+    ra.lab = bt->d_lab.as<u64>();
+    ra.tstamp = bt->d_tstamp.as<uint32_t>();
+    ra.tvisit = bt->d_tvisit.as<uint32_t>();
+    ra.lists = bt->d_lists.as<u64>();
+    ra.list_cap = bt->total_tiles;
+    ra.ctl = bt->d_ctl.as<Ctl>();
     ra.tile_h = bt->tile_h;
-    ra.activation_factor = kActivationFactor;
-    ra.status = ctl + 1;
+    ra.round_limit = 64u * bt->max_tiles + 4096u;
     if (n) {
         if (bt->ev0) MRC_CUDA(cudaEventRecord(bt->ev0, st), "record event");
         MRC_CUDA(relax_launch(ra, bt->grid, bt->smem, st), "launch relax kernel");
         if (bt->ev1) MRC_CUDA(cudaEventRecord(bt->ev1, st), "record event");
         bt->launches++;
     }
-    PathArgs pa;
-    pa.board = bt->board->dev;
-    pa.fields = ra.fields;
-    pa.n_fields = n;
-    pa.pads = ra.pads;
-    pa.dist = ra.dist;
-    pa.hops = ra.hops;
-    pa.costs = bt->d_costs.as<uint32_t>();
-    pa.lens = bt->d_lens.as<uint32_t>();
-    pa.offsets = bt->d_offsets.as<unsigned long long>();
-    pa.cells = bt->d_cells.as<uint32_t>();
-    pa.status = ctl + 1;
+    const PathArgs pa = path_args(bt);
     MRC_CUDA(path_launch(pa, st), "launch path kernels");
     bt->launches += n ? 2 : 1;
+    if (bt->d_out.p && n) {
+        MRC_CUDA(fields_launch(pa, bt->d_out.as<uint32_t>(), bt->total_cells, st), "launch field emit");
+        bt->launches++;
+    }
     return MRC_OK;
 }
 
 mrc_status status_error(uint32_t status) {
-    if (status & 3u) return fail(MRC_ERR_ITERATION_LIMIT, "a field hit its relaxation bound");
-    if (status & 4u) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "canonical path reconstruction failed");
+    if (status & (kStatusActivationLimit | kStatusRoundLimit))
+        return fail(MRC_ERR_ITERATION_LIMIT, "a field hit its relaxation bound");
+    if (status & kStatusBarrier) return fail(MRC_ERR_ITERATION_LIMIT, "grid barrier wait exceeded its bound");
+    if (status & kStatusPathBroken) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "canonical path reconstruction failed");
     return fail(MRC_ERR_BACKEND_UNAVAILABLE, "tile queue overflow");
 }
 
@@ -514,7 +525,7 @@ mrc_status batch_collect(mrc_batch *bt, bool keep_fields, std::vector<uint32_t> 
     cudaStream_t st = bt->stream;
     const uint32_t n = (uint32_t)bt->fields.size();
     uint32_t status = 0;
-    MRC_CUDA(cudaMemcpyAsync(&status, bt->d_ctl.as<uint32_t>() + 1, 4, cudaMemcpyDeviceToHost, st), "read status");
+    MRC_CUDA(cudaMemcpyAsync(&status, &bt->d_ctl.as<Ctl>()->status, 4, cudaMemcpyDeviceToHost, st), "read status");
     std::vector<uint64_t> off(n + 1);
     costs->assign(n, kMax);
     if (n) MRC_CUDA(cudaMemcpyAsync(costs->data(), bt->d_costs.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "read costs");
@@ -528,8 +539,8 @@ mrc_status batch_collect(mrc_batch *bt, bool keep_fields, std::vector<uint32_t> 
     if (keep_fields) {
         fields->assign(n, {});
         std::vector<uint32_t> all(bt->total_cells);
-        if (bt->total_cells)
-            MRC_CUDA(cudaMemcpy(all.data(), bt->d_dist.p, bt->total_cells * 4, cudaMemcpyDeviceToHost), "read fields");
+        if (bt->total_cells && bt->d_out.p)
+            MRC_CUDA(cudaMemcpy(all.data(), bt->d_out.p, bt->total_cells * 4, cudaMemcpyDeviceToHost), "read fields");
         for (const DevField &f : bt->fields) {
             const uint64_t c = (uint64_t)f.ww * f.wh * bt->board->view.layers;
             (*fields)[f.out].assign(all.begin() + f.lab_off, all.begin() + f.lab_off + c);
@@ -865,6 +876,18 @@ mrc_status mrc_batch_finish(mrc_context *ctx, mrc_batch *batch, mrc_result **out
 uint32_t mrc_batch_kernel_launches(const mrc_batch *batch) { return batch ? batch->launches : 0; }
 uint64_t mrc_batch_window_cells(const mrc_batch *batch) { return batch ? batch->total_cells : 0; }
 
+mrc_status mrc_batch_stats(const mrc_batch *batch, uint64_t out[4]) {
+    if (!batch || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    if (batch->d_ctl.p) MRC_CUDA(cudaMemcpy(&c, batch->d_ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost), "read counters");
+    out[0] = c.activations;
+    out[1] = c.sweeps;
+    out[2] = c.rounds;
+    out[3] = batch->total_tiles;
+    return MRC_OK;
+}
+
 float mrc_batch_relax_ms(const mrc_batch *batch) {
     if (!batch || !batch->ev0 || !batch->ev1) return -1.0f;
     float ms = -1.0f;
@@ -898,6 +921,7 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
                      uint32_t *cost, std::vector<uint32_t> *path, std::vector<uint32_t> *field) {
     const GridView &g = board->view;
     cudaStream_t st = ctx->stream;
+    constexpr uint32_t kPlainTileH = 32;
     DevField f{};
     f.src = net.src;
     f.dst = net.dst;
@@ -911,50 +935,47 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     f.vpad_off = f.n_pads;
     f.n_vpads = (uint32_t)net.vpads.size();
     f.out = 0;
+    f.tile_off = 0;
     const uint64_t wc = (uint64_t)f.ww * f.wh * g.layers;
+    const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + kPlainTileH - 1) / kPlainTileH);
     std::vector<uint32_t> pads(net.pads);
     pads.insert(pads.end(), net.vpads.begin(), net.vpads.end());
-    DBuf d_pads, d_a, d_ha, d_b, d_hb, d_ctl, d_field, d_costs, d_lens, d_off, d_cells;
+    DBuf d_pads, d_a, d_b, d_ctl, d_field, d_costs, d_lens, d_off, d_cells, d_vis, d_out;
     MRC_TRY(upload(ctx, d_pads, pads.data(), pads.size() * 4, "plain pads"));
     MRC_TRY(upload(ctx, d_field, &f, sizeof(f), "plain field"));
-    MRC_TRY(d_a.get(ctx, wc * 4, "plain labels"));
-    MRC_TRY(d_ha.get(ctx, wc * 4, "plain labels"));
-    MRC_TRY(d_b.get(ctx, wc * 4, "plain labels"));
-    MRC_TRY(d_hb.get(ctx, wc * 4, "plain labels"));
+    MRC_TRY(d_a.get(ctx, wc * 8, "plain labels"));
+    MRC_TRY(d_b.get(ctx, wc * 8, "plain labels"));
     MRC_TRY(d_ctl.get(ctx, 64, "plain flags"));
-    MRC_CUDA(cudaMemsetAsync(d_a.p, 0xFF, wc * 4, st), "plain init");
-    MRC_CUDA(cudaMemsetAsync(d_ha.p, 0xFF, wc * 4, st), "plain init");
+    MRC_TRY(d_vis.get(ctx, tiles * 4, "plain tile flags"));
+    MRC_CUDA(cudaMemsetAsync(d_a.p, 0xFF, wc * 8, st), "plain init");
     MRC_CUDA(cudaMemsetAsync(d_ctl.p, 0, 64, st), "plain init");
+    MRC_CUDA(cudaMemsetAsync(d_vis.p, 0x01, tiles * 4, st), "plain init");  // every tile holds labels
     const uint32_t plane = g.w * g.h;
     const uint32_t sx = (net.src % plane) % g.w, sy = (net.src % plane) / g.w, sl = net.src / plane;
-    const bool src_ok = sx >= win.x0 && sx <= win.x1 && sy >= win.y0 && sy <= win.y1;
-    static const uint32_t zero = 0;
+    const bool src_ok = sx >= win.x0 && sx <= win.x1 && sy >= win.y0 && sy <= win.y1 &&
+                        !g.board_forbidden(net.src) && (!g.obstacle(net.src) || sorted_contains(net.pads, net.src));
+    static const u64 zero = 0;
     if (src_ok) {
         const uint64_t lc = ((uint64_t)sl * f.wh + (sy - f.y0)) * f.ww + (sx - f.x0);
-        MRC_CUDA(cudaMemcpyAsync(d_a.as<uint32_t>() + lc, &zero, 4, cudaMemcpyHostToDevice, st), "plain seed");
-        MRC_CUDA(cudaMemcpyAsync(d_ha.as<uint32_t>() + lc, &zero, 4, cudaMemcpyHostToDevice, st), "plain seed");
+        MRC_CUDA(cudaMemcpyAsync(d_a.as<u64>() + lc, &zero, 8, cudaMemcpyHostToDevice, st), "plain seed");
     }
     PlainArgs pa;
     pa.board = board->dev;
     pa.field = f;
     pa.pads = d_pads.as<uint32_t>();
     pa.changed = d_ctl.as<uint32_t>();
-    uint32_t *in_d = d_a.as<uint32_t>(), *in_h = d_ha.as<uint32_t>();
-    uint32_t *out_d = d_b.as<uint32_t>(), *out_h = d_hb.as<uint32_t>();
+    u64 *in = d_a.as<u64>(), *out = d_b.as<u64>();
     const uint64_t round_limit = wc + 2;
     for (uint64_t round = 0; src_ok; ++round) {
         if (round > round_limit) return fail(MRC_ERR_ITERATION_LIMIT, "plain relaxation did not converge");
         uint32_t changed = 0;
         MRC_CUDA(cudaMemsetAsync(pa.changed, 0, 4, st), "plain round");
-        pa.in_dist = in_d;
-        pa.in_hops = in_h;
-        pa.out_dist = out_d;
-        pa.out_hops = out_h;
+        pa.in = in;
+        pa.out = out;
         MRC_CUDA(plain_round_launch(pa, wc, st), "plain round");
         MRC_CUDA(cudaMemcpyAsync(&changed, pa.changed, 4, cudaMemcpyDeviceToHost, st), "plain flag");
         MRC_CUDA(cudaStreamSynchronize(st), "plain round");
-        std::swap(in_d, out_d);
-        std::swap(in_h, out_h);
+        std::swap(in, out);
         if (!changed) break;
     }
     MRC_TRY(d_costs.get(ctx, 4, "plain cost"));
@@ -966,14 +987,19 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     pt.fields = d_field.as<DevField>();
     pt.n_fields = 1;
     pt.pads = d_pads.as<uint32_t>();
-    pt.dist = in_d;
-    pt.hops = in_h;
+    pt.lab = in;
+    pt.tvisit = d_vis.as<uint32_t>();
+    pt.tile_h = kPlainTileH;
     pt.costs = d_costs.as<uint32_t>();
     pt.lens = d_lens.as<uint32_t>();
     pt.offsets = d_off.as<unsigned long long>();
     pt.cells = d_cells.as<uint32_t>();
     pt.status = d_ctl.as<uint32_t>() + 1;
     MRC_CUDA(path_launch(pt, st), "plain path");
+    if (field) {
+        MRC_TRY(d_out.get(ctx, wc * 4, "plain field"));
+        MRC_CUDA(fields_launch(pt, d_out.as<uint32_t>(), wc, st), "plain field");
+    }
     uint32_t status = 0;
     uint64_t off[2];
     MRC_CUDA(cudaMemcpyAsync(&status, pt.status, 4, cudaMemcpyDeviceToHost, st), "plain status");
@@ -985,7 +1011,7 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     if (off[1]) MRC_CUDA(cudaMemcpy(path->data(), pt.cells, off[1] * 4, cudaMemcpyDeviceToHost), "plain path");
     if (field) {
         field->resize(wc);
-        MRC_CUDA(cudaMemcpy(field->data(), in_d, wc * 4, cudaMemcpyDeviceToHost), "plain field");
+        MRC_CUDA(cudaMemcpy(field->data(), d_out.p, wc * 4, cudaMemcpyDeviceToHost), "plain field");
     }
     return MRC_OK;
 }

@@ -12,19 +12,26 @@ namespace mrc {
 
 constexpr int kRelaxThreads = 256;
 
+// Status bits reported through Ctl::status / PathArgs::status.
+constexpr uint32_t kStatusActivationLimit = 1u << 0;
+constexpr uint32_t kStatusRoundLimit = 1u << 1;
+constexpr uint32_t kStatusPathBroken = 1u << 2;
+constexpr uint32_t kStatusQueueOverflow = 1u << 3;
+constexpr uint32_t kStatusBarrier = 1u << 4;
+
 struct RelaxArgs {
     DevBoard board;
-    const DevField *fields;     // in processing order (largest windows first)
+    const DevField *fields;     // ascending lab_off
     uint32_t n_fields;
     const uint32_t *pads;       // sorted pad lists, indexed by DevField offsets
-    uint32_t *dist, *hops;      // label arenas
-    uint32_t *work_counter;     // zeroed before launch
-    uint32_t *tile_scratch;     // per CTA: queue[max_tiles] + in-queue bitmap
-    uint32_t scratch_stride;
-    uint32_t max_tiles;
+    u64 *lab;                   // label arena (dist << 32 | hops)
+    uint32_t *tstamp;           // per tile: last round it was queued for, + 1 (zeroed)
+    uint32_t *tvisit;           // per tile: labels valid (zeroed)
+    u64 *lists;                 // 3 rotating lists of (field << 32 | tile)
+    uint32_t list_cap;          // total tiles of the batch
+    Ctl *ctl;                   // zeroed before launch
     uint32_t tile_h;            // 32, 16 or 8
-    uint32_t activation_factor; // tile activations allowed per tile (guard)
-    uint32_t *status;           // error bits (0 = fine)
+    uint32_t round_limit;       // guard on the number of rounds
 };
 
 struct PathArgs {
@@ -32,7 +39,9 @@ struct PathArgs {
     const DevField *fields;
     uint32_t n_fields;
     const uint32_t *pads;
-    const uint32_t *dist, *hops;
+    const u64 *lab;
+    const uint32_t *tvisit;
+    uint32_t tile_h;
     uint32_t *costs;                 // [n] by output slot
     uint32_t *lens;                  // [n] by output slot
     unsigned long long *offsets;     // [n+1] by output slot
@@ -44,8 +53,8 @@ struct PlainArgs {
     DevBoard board;
     DevField field;
     const uint32_t *pads;
-    const uint32_t *in_dist, *in_hops;
-    uint32_t *out_dist, *out_hops;
+    const u64 *in;
+    u64 *out;
     uint32_t *changed;
 };
 
@@ -54,6 +63,8 @@ cudaError_t relax_configure(bool directed, size_t smem);
 cudaError_t relax_occupancy(bool directed, size_t smem, int *blocks_per_sm);
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, size_t smem, cudaStream_t st);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
+cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);
+cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, uint64_t n, cudaStream_t st);
 
 }  // namespace mrc

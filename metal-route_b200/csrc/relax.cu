@@ -1,14 +1,23 @@
 // relax.cu — the batched field + canonical path kernels.
 //
-// relax_tiles_kernel: a persistent CTA takes one field (net x window) at a
-// time from a device work counter.  The field's labels live in HBM (u32 dist,
-// u32 hops, window-packed like the reference's ragged layout,
-// metal/src/lib.rs:833-871).  The window is cut into tiles of 32 x TH cells
-// over every layer; an active tile is staged in shared memory with a one-cell
-// halo ring, relaxed to local convergence by directional sweeps (rows, columns,
-// layer stacks — the edge-aware sweep of gpu.rs:259-430 run on-chip instead of
-// one dispatch per round), written back, and any neighbour whose halo it can
-// now improve is queued.  The field is final when the tile queue drains.
+// relax_rounds_kernel: one cooperative persistent launch solves every field
+// (net x window) of a batch.  Each field's labels live in HBM as u64
+// (dist << 32 | hops), window-packed like the reference's ragged layout
+// (metal/src/lib.rs:833-871).  Windows are cut into tiles of 32 x TH cells over
+// every layer.  Work proceeds in bulk-synchronous rounds over a shared list of
+// active (field, tile) items: a CTA stages a tile plus a one-cell halo ring in
+// shared memory, relaxes it to local convergence with directional sweeps (the
+// edge-aware row / column / layer-stack sweeps of gpu.rs:259-430, run on-chip
+// instead of one dispatch per round), writes it back and queues each neighbour
+// whose halo it now improves for the next round.  A field is final when no
+// tile of it is queued; the launch ends when the whole list drains.
+//
+// Tiles of one field run concurrently in different CTAs.  That is safe because
+// labels only decrease, every label is one aligned 64-bit word (a halo read is
+// an old or a new label, never a torn mix), labels are read through L2
+// (ld.global.cg) so no SM sees a stale L1 line, and a tile is processed by at
+// most one CTA per round.  A neighbour read before it improves is re-queued by
+// that neighbour's own push check, so no improvement is lost.
 //
 // path kernels: the path length is hops[dst] + 1 (every canonical predecessor
 // has exactly one fewer hop), so offsets come from one device scan and one warp
@@ -23,13 +32,9 @@
 
 namespace mrc {
 
-// Status bits reported through the kernels' status word.
-constexpr uint32_t kStatusActivationLimit = 1u << 0;
-constexpr uint32_t kStatusRoundLimit = 1u << 1;
-constexpr uint32_t kStatusPathBroken = 1u << 2;
-constexpr uint32_t kStatusQueueOverflow = 1u << 3;
-
 constexpr uint32_t kTW = 32;  // tile width (one warp across a row)
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
 struct TileSmem {
     u64 *lab;
@@ -51,8 +56,39 @@ __device__ __forceinline__ uint32_t planar_step(const TileSmem &s, uint32_t p, u
     return capmul(base, e);
 }
 
+// Grid-wide barrier for a cooperative launch.  The wait is bounded: after
+// kBarrierSpinLimit polls it records kStatusBarrier and returns, and every CTA
+// leaves the round loop once the status word is non-zero.
+__device__ void grid_barrier(Ctl *c, uint32_t nblocks) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        volatile uint32_t *gen_p = &c->bar_gen;
+        const uint32_t gen = *gen_p;
+        const uint32_t arrived = atomicAdd(&c->bar_count, 1u) + 1u;
+        if (arrived == nblocks) {
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (*gen_p == gen) {
+                if (++spins > kBarrierSpinLimit) {
+                    atomicOr(&c->status, kStatusBarrier);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t ld_status(const Ctl *c) { return *(volatile const uint32_t *)&c->status; }
+
 template <bool DIRECTED>
-__global__ void __launch_bounds__(kRelaxThreads) relax_tiles_kernel(RelaxArgs a) {
+__global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const DevBoard b = a.board;
     const uint32_t L = b.layers;
@@ -71,98 +107,100 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_tiles_kernel(RelaxArgs a)
     }
     __shared__ uint32_t xe_s[kTW + 2];
     __shared__ uint32_t ye_s[34];
-    __shared__ uint32_t s_field, s_tile, s_qhead, s_qtail, s_act, s_abort;
+    __shared__ u64 s_item;
     __shared__ uint32_t s_push[4];
+    __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
+    __shared__ uint32_t s_sweeps;
 
+    Ctl *ctl = a.ctl;
     const uint32_t tid = threadIdx.x;
-    uint32_t *queue = a.tile_scratch + (size_t)blockIdx.x * a.scratch_stride;
-    uint32_t *inq = queue + a.max_tiles;
+    const uint32_t cap = a.list_cap;
 
-    for (;;) {
-        if (tid == 0) s_field = atomicAdd(a.work_counter, 1u);
-        __syncthreads();
-        const uint32_t fi = s_field;
-        if (fi >= a.n_fields) break;
+    // ---- round 0: every field's source tile ---------------------------------
+    for (uint32_t fi = blockIdx.x * blockDim.x + tid; fi < a.n_fields; fi += gridDim.x * blockDim.x) {
         const DevField f = a.fields[fi];
-        const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
-        const uint32_t ntiles = ntx * nty;
-        const uint64_t wcells = (uint64_t)f.ww * f.wh * L;
-        uint32_t *dist = a.dist + f.lab_off;
-        uint32_t *hops = a.hops + f.lab_off;
-
-        for (uint64_t i = tid; i < wcells; i += blockDim.x) {
-            dist[i] = kMax;
-            hops[i] = kMax;
+        const uint32_t plane = b.w * b.h;
+        const uint32_t sr = f.src % plane, sx = sr % b.w, sy = sr / b.w;
+        const uint8_t sfl = b.flags ? b.flags[f.src] : 0;
+        if (sx >= f.x0 && sx < f.x0 + f.ww && sy >= f.y0 && sy < f.y0 + f.wh &&
+            cell_enter(b, f, a.pads, f.src, sfl) != kMax) {
+            const uint32_t ntx = (f.ww + kTW - 1) / kTW;
+            const uint32_t t = ((sy - f.y0) / TH) * ntx + (sx - f.x0) / kTW;
+            a.tstamp[f.tile_off + t] = 1u;
+            const uint32_t idx = atomicAdd(&ctl->count[0], 1u);
+            a.lists[idx] = ((u64)fi << 32) | t;
         }
-        for (uint32_t i = tid; i < (ntiles + 31) / 32; i += blockDim.x) inq[i] = 0;
-        __syncthreads();
-        if (tid == 0) {
-            s_qhead = 0;
-            s_qtail = 0;
-            s_act = 0;
-            s_abort = 0;
-            const uint32_t plane = b.w * b.h;
-            const uint32_t sl = f.src / plane, sr = f.src % plane;
-            const uint32_t sx = sr % b.w, sy = sr / b.w;
-            const uint8_t sfl = b.flags ? b.flags[f.src] : 0;
-            if (sx >= f.x0 && sx < f.x0 + f.ww && sy >= f.y0 && sy < f.y0 + f.wh &&
-                cell_enter(b, f, a.pads, f.src, sfl) != kMax) {
-                const uint64_t lc = ((uint64_t)sl * f.wh + (sy - f.y0)) * f.ww + (sx - f.x0);
-                dist[lc] = 0;
-                hops[lc] = 0;
-                const uint32_t t = ((sy - f.y0) / TH) * ntx + (sx - f.x0) / kTW;
-                queue[0] = t;
-                s_qtail = 1;
-                inq[t >> 5] |= 1u << (t & 31);
-            }
-        }
-        __syncthreads();
-        const uint32_t act_limit = a.activation_factor * ntiles + 65536u;
+    }
+    grid_barrier(ctl, gridDim.x);
 
+    for (uint32_t round = 0;; ++round) {
+        const uint32_t cur = round % 3, nxt = (round + 1) % 3, old = (round + 2) % 3;
+        const uint32_t n = *(volatile uint32_t *)&ctl->count[cur];
+        if (n == 0 || ld_status(ctl)) break;
+        if (round >= a.round_limit) {
+            if (blockIdx.x == 0 && tid == 0) atomicOr(&ctl->status, kStatusRoundLimit);
+            break;
+        }
+        if (blockIdx.x == 0 && tid == 0) {
+            ctl->count[old] = 0;
+            ctl->head[old] = 0;
+            ctl->rounds = round + 1;
+        }
         for (;;) {
             if (tid == 0) {
-                if (s_qhead == s_qtail || s_abort) {
-                    s_tile = kMax;
-                } else {
-                    const uint32_t t = queue[s_qhead % a.max_tiles];
-                    s_qhead++;
-                    inq[t >> 5] &= ~(1u << (t & 31));
-                    s_tile = t;
-                    if (++s_act > act_limit) {
-                        atomicOr(a.status, kStatusActivationLimit);
-                        s_abort = 1;
-                        s_tile = kMax;
-                    }
-                }
+                const uint32_t idx = atomicAdd(&ctl->head[cur], 1u);
+                s_item = idx < n ? __ldcg(a.lists + (size_t)cur * cap + idx) : kInf;
                 s_push[0] = s_push[1] = s_push[2] = s_push[3] = 0;
+                s_sweeps = 0;
             }
             __syncthreads();
-            const uint32_t t = s_tile;
-            if (t == kMax) break;
+            const u64 item = s_item;
+            if (item == kInf) break;
+            const uint32_t fi = (uint32_t)(item >> 32), t = (uint32_t)item;
+            const DevField f = a.fields[fi];
+            const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
             const uint32_t txi = t % ntx, tyi = t / ntx;
             const int tx0 = (int)(f.x0 + txi * kTW), ty0 = (int)(f.y0 + tyi * TH);
             const uint32_t tw = min(kTW, f.ww - txi * kTW), th = min(TH, f.wh - tyi * TH);
             const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
+            const u64 *lab = a.lab + f.lab_off;
+            if (tid < 5) {
+                uint32_t u = kNone;
+                if (tid == 0) u = t;
+                else if (tid == 1 && txi > 0) u = t - 1;
+                else if (tid == 2 && txi + 1 < ntx) u = t + 1;
+                else if (tid == 3 && tyi > 0) u = t - ntx;
+                else if (tid == 4 && tyi + 1 < nty) u = t + ntx;
+                s_vis[tid] = u == kNone ? 0u : __ldcg(a.tvisit + f.tile_off + u);
+            }
+            __syncthreads();
 
-            // ---- stage the tile and its halo ring ---------------------------
+            // ---- stage the tile and its halo ring (labels through L2) -------
             for (uint32_t i = tid; i < nsm; i += blockDim.x) {
                 const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
                 const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
-                u64 lab = kInf;
+                u64 lv = kInf;
                 uint32_t ent = kMax;
                 uint8_t fl = 0;
                 if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1) {
+                    const bool hx = sx == 0 || sx == tw + 1, hy = sy == 0 || sy == th + 1;
+                    uint32_t owner;  // which tile's label this smem cell holds
+                    if (hx && hy) owner = 5;  // corner: never read
+                    else if (sx == 0) owner = 1;
+                    else if (sx == tw + 1) owner = 2;
+                    else if (sy == 0) owner = 3;
+                    else if (sy == th + 1) owner = 4;
+                    else owner = 0;
                     const uint32_t gcell = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
                     const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0);
-                    const uint32_t d = dist[lc];
-                    lab = d == kMax ? kInf : (((u64)d << 32) | hops[lc]);
+                    if (owner < 5 && s_vis[owner]) lv = __ldcg(lab + lc);
+                    else if (owner == 0 && gcell == f.src) lv = 0;  // first visit of the source tile
                     const uint8_t gf = b.flags ? __ldg(b.flags + gcell) : 0;
                     ent = cell_enter(b, f, a.pads, gcell, gf);
                     fl = cell_tile_flags(f, a.pads, gcell, gf);
-                    if (DIRECTED && sx >= 1 && sx <= kTW && sy >= 1 && sy <= TH)
-                        s.din[(l * TH + sy - 1) * kTW + sx - 1] = __ldg(b.directed + gcell);
+                    if (DIRECTED && owner == 0) s.din[(l * TH + sy - 1) * kTW + sx - 1] = __ldg(b.directed + gcell);
                 }
-                s.lab[i] = lab;
+                s.lab[i] = lv;
                 s.ent[i] = ent;
                 s.fl[i] = fl;
             }
@@ -178,8 +216,8 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_tiles_kernel(RelaxArgs a)
             __syncthreads();
 
             // ---- relax to local convergence ---------------------------------
-            const uint32_t round_limit = L * kTW * TH + 4;
-            uint32_t round = 0;
+            const uint32_t sweep_limit = L * kTW * TH + 4;
+            uint32_t sweep = 0;
             for (;;) {
                 bool ch = false;
                 // rows: one thread per (layer, row)
@@ -285,25 +323,23 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_tiles_kernel(RelaxArgs a)
                         }
                     }
                 }
+                ++sweep;
                 const int any = __syncthreads_or(ch ? 1 : 0);
                 if (!any) break;
-                if (++round > round_limit) {
-                    if (tid == 0) {
-                        atomicOr(a.status, kStatusRoundLimit);
-                        s_abort = 1;
-                    }
+                if (sweep > sweep_limit) {
+                    if (tid == 0) atomicOr(&ctl->status, kStatusRoundLimit);
                     break;
                 }
             }
 
             // ---- write back and find neighbours this tile can improve -------
+            u64 *labw = a.lab + f.lab_off;
             for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
                 const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
                 const uint32_t c = (l * SH + ty + 1) * SW + tx + 1;
-                const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-                const u64 v = s.lab[c];
-                dist[lc] = (uint32_t)(v >> 32);
-                hops[lc] = v == kInf ? kMax : (uint32_t)v;
+                const uint64_t lc =
+                    ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
+                labw[lc] = s.lab[c];
             }
             // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
             const uint32_t nb = 2 * L * th + 2 * L * tw;
@@ -365,7 +401,8 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_tiles_kernel(RelaxArgs a)
                 if (DIRECTED) {
                     // the neighbour's in-price is not staged; read it from HBM
                     const uint32_t nsx = nc % SW, nsy = (nc / SW) % SH;
-                    const uint32_t gcell = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
+                    const uint32_t gcell =
+                        (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
                     const uint4 d4 = __ldg(b.directed + gcell);
                     base = dir == 0 ? d4.x : dir == 1 ? d4.y : dir == 2 ? d4.z : d4.w;
                 }
@@ -374,25 +411,38 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_tiles_kernel(RelaxArgs a)
             }
             __syncthreads();
             if (tid == 0) {
+                __threadfence();  // labels before the visited flag and the queue entries
+                if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
                 const uint32_t nbr[4] = {t - 1, t + 1, t - ntx, t + ntx};
-                for (int sdx = 0; sdx < 4; ++sdx) {
-                    if (!s_push[sdx]) continue;
-                    const uint32_t u = nbr[sdx];
-                    if (inq[u >> 5] & (1u << (u & 31))) continue;
-                    if (s_qtail - s_qhead >= a.max_tiles) {
-                        atomicOr(a.status, kStatusQueueOverflow);
-                        s_abort = 1;
-                        break;
+                const uint32_t want = round + 2;  // stamp s = queued for round s-1
+                for (int sd = 0; sd < 4; ++sd) {
+                    if (!s_push[sd]) continue;
+                    const uint32_t g = f.tile_off + nbr[sd];
+                    if (atomicMax(a.tstamp + g, want) < want) {
+                        const uint32_t idx = atomicAdd(&ctl->count[nxt], 1u);
+                        if (idx < cap) {
+                            a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | nbr[sd];
+                        } else {
+                            atomicOr(&ctl->status, kStatusQueueOverflow);
+                        }
                     }
-                    queue[s_qtail % a.max_tiles] = u;
-                    s_qtail++;
-                    inq[u >> 5] |= 1u << (u & 31);
                 }
+                atomicAdd(&ctl->activations, 1ull);
+                atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
             }
             __syncthreads();
         }
-        __syncthreads();
+        grid_barrier(ctl, gridDim.x);
     }
+}
+
+// Label of a window cell after the relax launch (unvisited tiles are unreached).
+__device__ __forceinline__ u64 field_label(const PathArgs &a, const DevField &f, uint32_t lx, uint32_t ly,
+                                           uint32_t l) {
+    const uint32_t ntx = (f.ww + kTW - 1) / kTW;
+    const uint32_t t = (ly / a.tile_h) * ntx + lx / kTW;
+    if (!a.tvisit[f.tile_off + t]) return kInf;
+    return a.lab[f.lab_off + ((uint64_t)l * f.wh + ly) * f.ww + lx];
 }
 
 // Per field: search cost and path length (hops[dst] + 1), then an exclusive
@@ -408,9 +458,9 @@ __global__ void __launch_bounds__(1024) path_offsets_kernel(PathArgs a) {
         const uint32_t dx = dr % a.board.w, dy = dr / a.board.w;
         uint32_t cost = kMax, len = 0;
         if (dx >= f.x0 && dx < f.x0 + f.ww && dy >= f.y0 && dy < f.y0 + f.wh) {
-            const uint64_t lc = f.lab_off + ((uint64_t)dl * f.wh + (dy - f.y0)) * f.ww + (dx - f.x0);
-            cost = a.dist[lc];
-            if (cost != kMax) len = a.hops[lc] + 1u;
+            const u64 v = field_label(a, f, dx - f.x0, dy - f.y0, dl);
+            cost = (uint32_t)(v >> 32);
+            if (cost != kMax) len = (uint32_t)v + 1u;
             // a simple path never has more cells than its window
             if ((uint64_t)len > (uint64_t)f.ww * f.wh * a.board.layers) {
                 atomicOr(a.status, kStatusPathBroken);
@@ -452,11 +502,10 @@ __global__ void __launch_bounds__(1024) path_offsets_kernel(PathArgs a) {
     if (threadIdx.x == 0) a.offsets[a.n_fields] = carry;
 }
 
-// Shared by the path walk: is p a canonical predecessor candidate of cur?
-// Returns the step price p->cur, kMax when the move is not allowed.
+// Step price of the move p -> cur for the walk and the plain form.
+// kind: 0 = p is cur's lower layer, 1 = -y, 2 = -x, 3 = +x, 4 = +y, 5 = upper layer.
 __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevField &f, const uint32_t *pads,
                                                 uint32_t p, uint32_t cur, int kind) {
-    // kind: 0 = p is cur's lower layer, 1 = -y, 2 = -x, 3 = +x, 4 = +y, 5 = upper layer
     const uint8_t fc = b.flags ? b.flags[cur] : 0, fp = b.flags ? b.flags[p] : 0;
     const uint32_t ec = cell_enter(b, f, pads, cur, fc);
     if (ec == kMax) return kMax;
@@ -472,16 +521,20 @@ __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevFiel
     uint8_t out_bit, in_bit;
     uint32_t base;
     if (kind == 1) {  // p at -y: p moves +y
-        out_bit = kEdgePosY; in_bit = kEdgeNegY;
+        out_bit = kEdgePosY;
+        in_bit = kEdgeNegY;
         base = b.directed ? __ldg(b.directed + cur).x : __ldg(b.y_edge + y - 1);
     } else if (kind == 2) {  // p at -x: p moves +x
-        out_bit = kEdgePosX; in_bit = kEdgeNegX;
+        out_bit = kEdgePosX;
+        in_bit = kEdgeNegX;
         base = b.directed ? __ldg(b.directed + cur).y : __ldg(b.x_edge + x - 1);
     } else if (kind == 3) {  // p at +x: p moves -x
-        out_bit = kEdgeNegX; in_bit = kEdgePosX;
+        out_bit = kEdgeNegX;
+        in_bit = kEdgePosX;
         base = b.directed ? __ldg(b.directed + cur).z : __ldg(b.x_edge + x);
     } else {  // p at +y: p moves -y
-        out_bit = kEdgeNegY; in_bit = kEdgePosY;
+        out_bit = kEdgeNegY;
+        in_bit = kEdgePosY;
         base = b.directed ? __ldg(b.directed + cur).w : __ldg(b.y_edge + y);
     }
     if ((fp & out_bit) | (fc & in_bit)) return kMax;
@@ -509,8 +562,7 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
             break;
         }
         const uint32_t r = cur % plane, x = r % b.w, y = r / b.w, l = cur / plane;
-        const uint64_t lcur = f.lab_off + ((uint64_t)l * f.wh + (y - f.y0)) * f.ww + (x - f.x0);
-        const uint32_t need_d = a.dist[lcur], need_h = a.hops[lcur];
+        const u64 need = field_label(a, f, x - f.x0, y - f.y0, l);
         bool ok = false;
         uint32_t p = 0;
         if (lane < 6) {
@@ -524,14 +576,10 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
             if (pl >= 0 && pl < (int)b.layers && px >= (int)f.x0 && px < (int)(f.x0 + f.ww) && py >= (int)f.y0 &&
                 py < (int)(f.y0 + f.wh)) {
                 p = ((uint32_t)pl * b.h + (uint32_t)py) * b.w + (uint32_t)px;
-                const uint64_t lp = f.lab_off + ((uint64_t)pl * f.wh + ((uint32_t)py - f.y0)) * f.ww + ((uint32_t)px - f.x0);
-                const uint32_t dp = a.dist[lp], hp = a.hops[lp];
-                if (dp != kMax && hp + 1u == need_h) {
+                const u64 lp = field_label(a, f, (uint32_t)px - f.x0, (uint32_t)py - f.y0, (uint32_t)pl);
+                if (lp != kInf) {
                     const uint32_t st = global_step(b, f, a.pads, p, cur, (int)lane);
-                    if (st != kMax) {
-                        const uint32_t s = dp + st;
-                        ok = s >= dp && s == need_d;
-                    }
+                    ok = extend(lp, st) == need;
                 }
             }
         }
@@ -542,6 +590,26 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
         }
         const uint32_t win = __ffs(m) - 1;
         cur = __shfl_sync(0xFFFFFFFFu, p, win);
+    }
+}
+
+// Complete u32 distance field of every field (MRC_FLAG_KEEP_FIELDS).
+// `fields_by_offset` lists the fields in ascending lab_off order.
+__global__ void emit_fields_kernel(PathArgs a, uint32_t *out, uint64_t total) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = a.n_fields;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (a.fields[mid].lab_off <= i) lo = mid;
+            else hi = mid;
+        }
+        const DevField f = a.fields[lo];
+        const uint64_t li = i - f.lab_off;
+        const uint32_t lx = (uint32_t)(li % f.ww);
+        const uint64_t rr = li / f.ww;
+        const uint32_t ly = (uint32_t)(rr % f.wh), l = (uint32_t)(rr / f.wh);
+        out[i] = (uint32_t)(field_label(a, f, lx, ly, l) >> 32);
     }
 }
 
@@ -557,9 +625,8 @@ __global__ void plain_round_kernel(PlainArgs a) {
     const uint32_t ly = (uint32_t)(r % f.wh), l = (uint32_t)(r / f.wh);
     const uint32_t x = f.x0 + lx, y = f.y0 + ly;
     const uint32_t cur = (l * b.h + y) * b.w + x;
-    const uint32_t *din = a.in_dist, *hin = a.in_hops;
-    const uint32_t d0 = din[i];
-    u64 best = d0 == kMax ? kInf : (((u64)d0 << 32) | hin[i]);
+    const u64 old = a.in[i];
+    u64 best = old;
     if (!(cur == f.src && best == 0)) {
         const int64_t plane_l = (int64_t)f.ww * f.wh;
         const int64_t off[6] = {-plane_l, -(int64_t)f.ww, -1, 1, (int64_t)f.ww, plane_l};
@@ -568,17 +635,15 @@ __global__ void plain_round_kernel(PlainArgs a) {
         for (int k = 0; k < 6; ++k) {
             if (!has[k]) continue;
             const uint64_t j = (uint64_t)((int64_t)i + off[k]);
-            const uint32_t dp = din[j];
-            if (dp == kMax) continue;
+            const u64 lp = a.in[j];
+            if (lp == kInf) continue;
             const uint32_t p = (uint32_t)((int64_t)cur + goff[k]);
-            const uint32_t st = global_step(b, f, a.pads, p, cur, k);
-            const u64 cand = extend(((u64)dp << 32) | hin[j], st);
+            const u64 cand = extend(lp, global_step(b, f, a.pads, p, cur, k));
             if (cand < best) best = cand;
         }
     }
-    a.out_dist[i] = (uint32_t)(best >> 32);
-    a.out_hops[i] = best == kInf ? kMax : (uint32_t)best;
-    if (best != (d0 == kMax ? kInf : (((u64)d0 << 32) | hin[i]))) *a.changed = 1u;
+    a.out[i] = best;
+    if (best != old) *a.changed = 1u;
 }
 
 // OR Grid::via_forbidden into the flag byte as kStaticVia.
@@ -608,22 +673,24 @@ size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
 
 cudaError_t relax_configure(bool directed, size_t smem) {
     if (directed)
-        return cudaFuncSetAttribute(relax_tiles_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return cudaFuncSetAttribute(relax_tiles_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return cudaFuncSetAttribute(relax_rounds_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaFuncSetAttribute(relax_rounds_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t relax_occupancy(bool directed, size_t smem, int *blocks_per_sm) {
     if (directed)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_tiles_kernel<true>, kRelaxThreads, smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_tiles_kernel<false>, kRelaxThreads, smem);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_rounds_kernel<true>, kRelaxThreads,
+                                                             smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_rounds_kernel<false>, kRelaxThreads,
+                                                         smem);
 }
 
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, size_t smem, cudaStream_t st) {
-    if (a.board.directed)
-        relax_tiles_kernel<true><<<grid, kRelaxThreads, smem, st>>>(a);
-    else
-        relax_tiles_kernel<false><<<grid, kRelaxThreads, smem, st>>>(a);
-    return cudaGetLastError();
+    RelaxArgs copy = a;
+    void *args[] = {&copy};
+    const void *fn =
+        a.board.directed ? (const void *)relax_rounds_kernel<true> : (const void *)relax_rounds_kernel<false>;
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kRelaxThreads), args, smem, st);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {
@@ -634,6 +701,13 @@ cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {
         const uint32_t warps_per_block = 8;
         path_walk_kernel<<<(a.n_fields + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(a);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st) {
+    if (total == 0 || a.n_fields == 0) return cudaSuccess;
+    const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 8192);
+    emit_fields_kernel<<<(uint32_t)blocks, 256, 0, st>>>(a, out, total);
     return cudaGetLastError();
 }
 

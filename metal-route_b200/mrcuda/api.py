@@ -151,6 +151,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_batch_kernel_launches": (u32, [vp]),
             "mrc_batch_window_cells": (C.c_uint64, [vp]),
             "mrc_batch_relax_ms": (C.c_float, [vp]),
+            "mrc_batch_stats": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
             "mrc_batch_destroy": (None, [vp]),
             "mrc_net_windows": (C.c_int, [u32, u32, u32, vp, u32, vp]),
         }
@@ -314,6 +315,13 @@ class Batch:
     @property
     def kernel_launches(self) -> int:
         return int(self.engine.lib.mrc_batch_kernel_launches(self.handle))
+
+    def stats(self) -> dict:
+        """Work counters of the last launch: tile activations, in-tile sweeps,
+        rounds and the batch's tile count."""
+        out = (C.c_uint64 * 4)()
+        self.engine._check(self.engine.lib.mrc_batch_stats(self.handle, out))
+        return {"activations": int(out[0]), "sweeps": int(out[1]), "rounds": int(out[2]), "tiles": int(out[3])}
 
     def relax_ms(self) -> float:
         """Device time of the relax kernel in the last launch (needs time_kernels)."""
