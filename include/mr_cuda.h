@@ -211,6 +211,46 @@ void mrc_batch_destroy(mrc_batch *batch);
 mrc_status mrc_route_isolated_plain(mrc_context *ctx, const mrc_isolated_request *req, uint32_t flags,
                                     mrc_result **out);
 
+/* ---- no device allocation --------------------------------------------------- */
+
+/* Bytes of the one file-scope device array that backs every scratch buffer of
+ * mrc_route_isolated_batch_noalloc.  Each GPU that loads the library holds this
+ * much device memory until the process exits. */
+#define MRC_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Window solve of an isolated batch (the semantics of mrc_route_isolated_batch
+ * without MRC_FLAG_RETRY_FULL) that never allocates device memory.  This entry
+ * point has no counterpart in the reference.
+ *
+ * Who needs it: a caller that cannot call cudaMalloc — a long-running router
+ * process that hands nearly all of HBM to its own allocator at start-up (a
+ * PyTorch caching allocator, an arena shared by several engines) and has
+ * nothing left for cudaMalloc, or a caller on a latency-critical path where
+ * cudaMalloc/cudaFree, which can synchronise the whole device, are not allowed.
+ * The caller passes the request and the host output buffers; all device
+ * scratch (board copy, descriptors, labels, tile lists, outputs before their
+ * download) is carved from MRC_NOALLOC_SCRATCH_BYTES of static device memory.
+ *
+ * - Runs on the calling thread's current device, on `stream` (a cudaStream_t;
+ *   NULL = the legacy default stream), and returns after the results are on the
+ *   host.
+ * - The first call on a device looks the scratch array up (once per device);
+ *   make that first call before any stream capture.
+ * - A request whose scratch would exceed MRC_NOALLOC_SCRATCH_BYTES (8 B per
+ *   window cell for labels plus 4 B per window cell for paths, the board copy,
+ *   and per-tile state) fails with MRC_ERR_LIMIT and does no device work.
+ * - All calls share the one array and find the previous call's contents in it;
+ *   the entry point clears what must start at zero.  Calls serialise on a
+ *   process-wide lock and each returns only after its device work finished;
+ *   device work that overlaps a call from elsewhere on the same GPU (e.g. a
+ *   second process of this library sharing the context) would race.
+ * - path_offsets[n+1] and search_costs[n] are always written on success; when
+ *   the paths need more than path_cells_capacity cells the call returns
+ *   MRC_ERR_LIMIT with the offsets filled so the caller can size the buffer. */
+mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_request *req, void *stream, uint32_t *search_costs,
+                                            uint64_t *path_offsets, uint32_t *path_cells,
+                                            uint64_t path_cells_capacity);
+
 /* net_window (negotiated.rs:568-594) for a batch of nets. */
 mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
                            mrc_window *out);

@@ -1063,3 +1063,242 @@ extern "C" mrc_status mrc_route_isolated_plain(mrc_context *ctx, const mrc_isola
     *out = r.release();
     return MRC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// No device allocation: every scratch buffer of one window solve is carved
+// from a file-scope device array.  Callers that cannot call cudaMalloc (their
+// allocator owns the HBM, or the call sits on a path where cudaMalloc/cudaFree
+// may not synchronise the device) use mrc_route_isolated_batch_noalloc.
+
+namespace {
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[MRC_NOALLOC_SCRATCH_BYTES];
+
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
+    int sms = 0;
+    size_t smem_optin = 0;
+};
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoallocDevice g_noalloc_dev[kNoallocMaxDevices];
+
+// Once per device, with that device current: look up the array's device address.
+mrc_status noalloc_setup(int device, NoallocDevice **out) {
+    if (device < 0 || device >= kNoallocMaxDevices) return fail(MRC_ERR_LIMIT, "device ordinal beyond 63");
+    NoallocDevice &d = g_noalloc_dev[device];
+    if (!d.ready) {
+        void *p = nullptr;
+        MRC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "look up the no-allocation scratch array");
+        cudaDeviceProp prop;
+        MRC_CUDA(cudaGetDeviceProperties(&prop, device), "device properties");
+        if (prop.major < 10) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "device is not sm_100 class");
+        d.scratch = static_cast<unsigned char *>(p);
+        d.sms = prop.multiProcessorCount;
+        d.smem_optin = prop.sharedMemPerBlockOptin;
+        d.ready = true;
+    }
+    *out = &d;
+    return MRC_OK;
+}
+
+// Bump allocator over the scratch array (offsets only, 256-byte aligned).
+struct Carve {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        const size_t o = off;
+        off = (off + std::max<size_t>(bytes, 4) + 255) & ~(size_t)255;
+        return o;
+    }
+};
+
+}  // namespace
+
+extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_request *req, void *stream,
+                                                       uint32_t *search_costs, uint64_t *path_offsets,
+                                                       uint32_t *path_cells, uint64_t path_cells_capacity) {
+    if (!req || !path_offsets || (req->n_nets && !search_costs) || (path_cells_capacity && !path_cells))
+        return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    int device = 0;
+    MRC_CUDA(cudaGetDevice(&device), "current device");
+    NoallocDevice *dev = nullptr;
+    MRC_TRY(noalloc_setup(device, &dev));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    GridView g;
+    MRC_TRY(view_grid(req->grid, &g));
+    const mrc_edges &e = req->edges;
+    const uint32_t ex = g.w ? g.w - 1 : 0, ey = g.h ? g.h - 1 : 0, ev = g.layers - 1;
+    if (e.n_x_edge_costs != ex || e.n_y_edge_costs != ey || e.n_via_edge_costs != ev)
+        return fail(MRC_ERR_INVALID_ARGUMENT, "isolated batch shape does not match grid/nets");
+    if ((ex && !e.x_edge_costs) || (ey && !e.y_edge_costs) || (ev && (!e.via_edge_costs || !e.via_allowed)))
+        return fail(MRC_ERR_INVALID_ARGUMENT, "edge price pointer is NULL");
+    if (req->n_nets && !req->windows) return fail(MRC_ERR_INVALID_ARGUMENT, "windows is NULL");
+    std::vector<NetCopy> nets;
+    MRC_TRY(validate_nets(g, req->nets, req->n_nets, &nets));
+    std::vector<mrc_window> wins;
+    MRC_TRY(collect_windows(g, nets, req->windows, &wins));
+    const uint32_t n = (uint32_t)nets.size();
+    path_offsets[0] = 0;
+    if (n == 0) return MRC_OK;
+
+    // tile height: the largest whose shared tile fits the per-CTA budget
+    const bool directed = e.directed_in_costs != nullptr;
+    uint32_t tile_h = 0;
+    size_t smem = 0;
+    const size_t budget = std::min<size_t>(dev->smem_optin ? dev->smem_optin : (227u << 10), 227u << 10) - 1024;
+    for (size_t b : {(size_t)(110u << 10), budget}) {
+        for (uint32_t th : {32u, 16u, 8u}) {
+            if (!tile_h && relax_smem_bytes(g.layers, th, directed) <= b) {
+                tile_h = th;
+                smem = relax_smem_bytes(g.layers, th, directed);
+            }
+        }
+    }
+    if (!tile_h) return fail(MRC_ERR_LIMIT, "too many layers for one shared-memory tile");
+
+    // field descriptors, largest windows first, and the pad arena
+    std::vector<uint32_t> order(n);
+    std::iota(order.begin(), order.end(), 0u);
+    auto cells_of = [&](uint32_t i) {
+        return (uint64_t)(wins[i].x1 - wins[i].x0 + 1) * (wins[i].y1 - wins[i].y0 + 1) * g.layers;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cells_of(a) > cells_of(b); });
+    std::vector<DevField> fields(n);
+    std::vector<uint32_t> pads;
+    uint64_t cells = 0, tiles = 0;
+    uint32_t max_tiles = 1;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t i = order[k];
+        DevField &f = fields[k];
+        f.src = nets[i].src;
+        f.dst = nets[i].dst;
+        f.x0 = wins[i].x0;
+        f.y0 = wins[i].y0;
+        f.ww = wins[i].x1 - wins[i].x0 + 1;
+        f.wh = wins[i].y1 - wins[i].y0 + 1;
+        f.lab_off = cells;
+        cells += cells_of(i);
+        f.pad_off = (uint32_t)pads.size();
+        f.n_pads = (uint32_t)nets[i].pads.size();
+        pads.insert(pads.end(), nets[i].pads.begin(), nets[i].pads.end());
+        f.vpad_off = (uint32_t)pads.size();
+        f.n_vpads = (uint32_t)nets[i].vpads.size();
+        pads.insert(pads.end(), nets[i].vpads.begin(), nets[i].vpads.end());
+        f.out = i;
+        const uint64_t t = (uint64_t)((f.ww + 31) / 32) * ((f.wh + tile_h - 1) / tile_h);
+        f.tile_off = (uint32_t)std::min<uint64_t>(tiles, 0xFFFFFFFFull);
+        tiles += t;
+        max_tiles = (uint32_t)std::max<uint64_t>(max_tiles, t);
+    }
+
+    // carve the scratch array; reject before any device work when it does not fit
+    const bool has_flags = g.board || g.via_forbidden;
+    Carve c;
+    const size_t o_ctl = c.take(sizeof(Ctl)), o_fields = c.take(n * sizeof(DevField)), o_pads = c.take(pads.size() * 4);
+    const size_t o_cost = c.take(g.n * 4), o_flags = has_flags ? c.take(g.n) : 0;
+    const size_t o_vf = g.via_forbidden ? c.take(g.n) : 0, o_dir = directed ? c.take(g.n * 16) : 0;
+    const size_t o_x = c.take((size_t)ex * 4), o_y = c.take((size_t)ey * 4), o_via = c.take((size_t)std::max(ev, 1u) * 4);
+    const size_t o_tstamp = c.take(tiles * 4), o_tvisit = c.take(tiles * 4), o_lists = c.take(tiles * 24);
+    const size_t o_lab = c.take(cells * 8), o_costs = c.take((size_t)n * 4), o_lens = c.take((size_t)n * 4);
+    const size_t o_offsets = c.take(((size_t)n + 1) * 8), o_cells = c.take(cells * 4);
+    if (c.off > (size_t)MRC_NOALLOC_SCRATCH_BYTES || tiles > 0x7FFFFFFFull)
+        return fail(MRC_ERR_LIMIT, "request needs " + std::to_string(c.off) + " bytes of scratch; the no-allocation "
+                                   "entry point has MRC_NOALLOC_SCRATCH_BYTES = " +
+                                       std::to_string((size_t)MRC_NOALLOC_SCRATCH_BYTES) + " bytes");
+    unsigned char *s = dev->scratch;
+
+    // inputs into the scratch array
+    MRC_CUDA(cudaMemcpyAsync(s + o_fields, fields.data(), n * sizeof(DevField), cudaMemcpyHostToDevice, st), "upload fields");
+    if (!pads.empty())
+        MRC_CUDA(cudaMemcpyAsync(s + o_pads, pads.data(), pads.size() * 4, cudaMemcpyHostToDevice, st), "upload pads");
+    MRC_CUDA(cudaMemcpyAsync(s + o_cost, g.cost, g.n * 4, cudaMemcpyHostToDevice, st), "upload cost");
+    if (has_flags) {
+        if (g.board) MRC_CUDA(cudaMemcpyAsync(s + o_flags, g.board, g.n, cudaMemcpyHostToDevice, st), "upload board mask");
+        else MRC_CUDA(cudaMemsetAsync(s + o_flags, 0, g.n, st), "clear flags");
+        if (g.via_forbidden) {
+            MRC_CUDA(cudaMemcpyAsync(s + o_vf, g.via_forbidden, g.n, cudaMemcpyHostToDevice, st), "upload via mask");
+            MRC_CUDA(combine_flags_launch(s + o_flags, s + o_vf, g.n, st), "combine masks");
+        }
+    }
+    if (directed)
+        MRC_CUDA(cudaMemcpyAsync(s + o_dir, e.directed_in_costs, g.n * 16, cudaMemcpyHostToDevice, st), "upload prices");
+    uint32_t via_mask = 0;
+    std::vector<uint32_t> vias(std::max(ev, 1u), 0);
+    for (uint32_t k = 0; k < ev; ++k) {
+        vias[k] = e.via_edge_costs[k];
+        if (e.via_allowed[k]) via_mask |= 1u << k;
+    }
+    if (ex) MRC_CUDA(cudaMemcpyAsync(s + o_x, e.x_edge_costs, (size_t)ex * 4, cudaMemcpyHostToDevice, st), "upload x");
+    if (ey) MRC_CUDA(cudaMemcpyAsync(s + o_y, e.y_edge_costs, (size_t)ey * 4, cudaMemcpyHostToDevice, st), "upload y");
+    MRC_CUDA(cudaMemcpyAsync(s + o_via, vias.data(), vias.size() * 4, cudaMemcpyHostToDevice, st), "upload vias");
+    // state that must start at zero (the array keeps the previous call's contents)
+    MRC_CUDA(cudaMemsetAsync(s + o_ctl, 0, sizeof(Ctl), st), "clear control block");
+    MRC_CUDA(cudaMemsetAsync(s + o_tstamp, 0, tiles * 4, st), "clear tile stamps");
+    MRC_CUDA(cudaMemsetAsync(s + o_tvisit, 0, tiles * 4, st), "clear tile flags");
+
+    DevBoard b;
+    b.w = g.w;
+    b.h = g.h;
+    b.layers = g.layers;
+    b.via_mask = via_mask;
+    b.cost = reinterpret_cast<const uint32_t *>(s + o_cost);
+    b.flags = has_flags ? s + o_flags : nullptr;
+    b.x_edge = reinterpret_cast<const uint32_t *>(s + o_x);
+    b.y_edge = reinterpret_cast<const uint32_t *>(s + o_y);
+    b.via_edge = reinterpret_cast<const uint32_t *>(s + o_via);
+    b.directed = directed ? reinterpret_cast<const uint4 *>(s + o_dir) : nullptr;
+
+    int per_sm = 0;
+    MRC_CUDA(relax_configure(directed, smem), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(directed, smem, &per_sm), "relax occupancy");
+    if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
+    RelaxArgs ra;
+    ra.board = b;
+    ra.fields = reinterpret_cast<const DevField *>(s + o_fields);
+    ra.n_fields = n;
+    ra.pads = reinterpret_cast<const uint32_t *>(s + o_pads);
+    ra.lab = reinterpret_cast<u64 *>(s + o_lab);
+    ra.tstamp = reinterpret_cast<uint32_t *>(s + o_tstamp);
+    ra.tvisit = reinterpret_cast<uint32_t *>(s + o_tvisit);
+    ra.lists = reinterpret_cast<u64 *>(s + o_lists);
+    ra.list_cap = (uint32_t)tiles;
+    ra.ctl = reinterpret_cast<Ctl *>(s + o_ctl);
+    ra.tile_h = tile_h;
+    ra.round_limit = 64u * max_tiles + 4096u;
+    MRC_CUDA(relax_launch(ra, (uint32_t)dev->sms * (uint32_t)per_sm, smem, st), "launch relax kernel");
+    PathArgs pa;
+    pa.board = b;
+    pa.fields = ra.fields;
+    pa.n_fields = n;
+    pa.pads = ra.pads;
+    pa.lab = ra.lab;
+    pa.tvisit = ra.tvisit;
+    pa.tile_h = tile_h;
+    pa.costs = reinterpret_cast<uint32_t *>(s + o_costs);
+    pa.lens = reinterpret_cast<uint32_t *>(s + o_lens);
+    pa.offsets = reinterpret_cast<unsigned long long *>(s + o_offsets);
+    pa.cells = reinterpret_cast<uint32_t *>(s + o_cells);
+    pa.status = &ra.ctl->status;
+    MRC_CUDA(path_launch(pa, st), "launch path kernels");
+
+    uint32_t status = 0;
+    MRC_CUDA(cudaMemcpyAsync(&status, pa.status, 4, cudaMemcpyDeviceToHost, st), "read status");
+    MRC_CUDA(cudaMemcpyAsync(search_costs, pa.costs, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "read costs");
+    MRC_CUDA(cudaMemcpyAsync(path_offsets, pa.offsets, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost, st),
+             "read offsets");
+    MRC_CUDA(cudaStreamSynchronize(st), "no-allocation batch");
+    if (status) return status_error(status);
+    const uint64_t total = path_offsets[n];
+    if (total > path_cells_capacity)
+        return fail(MRC_ERR_LIMIT, "paths need " + std::to_string(total) + " cells; path_cells_capacity is " +
+                                       std::to_string(path_cells_capacity));
+    if (total) {
+        MRC_CUDA(cudaMemcpyAsync(path_cells, pa.cells, total * 4, cudaMemcpyDeviceToHost, st), "read paths");
+        MRC_CUDA(cudaStreamSynchronize(st), "read paths");
+    }
+    return MRC_OK;
+}
