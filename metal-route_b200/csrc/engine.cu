@@ -365,11 +365,14 @@ struct mrc_batch {
 namespace {
 
 
+// Tile height: every row and column pass keeps 4*L*TH lanes busy, so prefer
+// L*TH = 64 (all 256 threads), then the tallest tile that still fits three CTAs
+// (75 KB) or two (110 KB) on an SM.
 mrc_status choose_tile(mrc_context *ctx, uint32_t layers, bool directed, uint32_t *tile_h, size_t *smem) {
-    const size_t budget_fast = 110u << 10;  // two CTAs per SM
-    const size_t budget_max = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
-    for (size_t budget : {budget_fast, budget_max}) {
-        for (uint32_t th : {32u, 16u, 8u}) {
+    const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
+    for (size_t budget : {(size_t)(75u << 10), (size_t)(110u << 10), hard}) {
+        for (uint32_t th : {64u, 32u, 16u, 8u}) {
+            if (layers * th > 64 && th > 8) continue;
             const size_t s = relax_smem_bytes(layers, th, directed);
             if (s <= budget) {
                 *tile_h = th;
@@ -434,8 +437,8 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
     bt->total_tiles = (uint32_t)std::max<uint64_t>(toff, 1);
     bt->max_tiles = max_tiles;
     int per_sm = 1;
-    MRC_CUDA(relax_configure(board->directed, bt->smem), "configure relax kernel");
-    MRC_CUDA(relax_occupancy(board->directed, bt->smem, &per_sm), "relax occupancy");
+    MRC_CUDA(relax_configure(bt->tile_h, bt->smem), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(bt->tile_h, bt->smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
     bt->grid = (uint32_t)ctx->sms * (uint32_t)per_sm;
@@ -1253,8 +1256,8 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     b.directed = directed ? reinterpret_cast<const uint4 *>(s + o_dir) : nullptr;
 
     int per_sm = 0;
-    MRC_CUDA(relax_configure(directed, smem), "configure relax kernel");
-    MRC_CUDA(relax_occupancy(directed, smem, &per_sm), "relax occupancy");
+    MRC_CUDA(relax_configure(tile_h, smem), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(tile_h, smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     RelaxArgs ra;
     ra.board = b;

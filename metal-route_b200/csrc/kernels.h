@@ -58,9 +58,10 @@ struct PlainArgs {
     uint32_t *changed;
 };
 
+// Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);
-cudaError_t relax_configure(bool directed, size_t smem);
-cudaError_t relax_occupancy(bool directed, size_t smem, int *blocks_per_sm);
+cudaError_t relax_configure(uint32_t tile_h, size_t smem);
+cudaError_t relax_occupancy(uint32_t tile_h, size_t smem, int *blocks_per_sm);
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, size_t smem, cudaStream_t st);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);

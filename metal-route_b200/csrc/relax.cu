@@ -36,24 +36,118 @@ constexpr uint32_t kTW = 32;  // tile width (one warp across a row)
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
-struct TileSmem {
-    u64 *lab;
-    uint32_t *ent;
-    uint8_t *fl;
-    uint4 *din;
+// Label extended by a run of `h` steps whose prices sum to `d` (kMax = blocked or
+// saturated); a dist reaching 0xFFFFFFFF is unreachable.
+__device__ __forceinline__ u64 ext2(u64 t, uint32_t d, uint32_t h) {
+    const uint32_t td = (uint32_t)(t >> 32);
+    const uint32_t nd = td + d;
+    const bool bad = (td == kMax) | (d == kMax) | (nd < td) | (nd == kMax);
+    return bad ? kInf : (((u64)nd << 32) | (uint32_t)((uint32_t)t + h));
+}
+
+// Saturating sum of step prices; kMax absorbs.
+__device__ __forceinline__ uint32_t dsum(uint32_t a, uint32_t b) {
+    const uint32_t s = a + b;
+    return (a == kMax) | (b == kMax) | (s < a) ? kMax : s;
+}
+
+__device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
+
+// Step-price planes of a staged tile: the move into cell c from its neighbour
+// at -x, +x, -y, +y, the layer below and the layer above.
+enum { kFromNegX = 0, kFromPosX = 1, kFromNegY = 2, kFromPosY = 3, kFromBelow = 4, kFromAbove = 5 };
+
+struct Tile {
+    u64 *lab;        // [L][TH+2][34] labels with a one-cell halo ring
+    uint32_t *st;    // [6][L][TH][32] step prices into interior cells
+    uint32_t L, TH;
+    __device__ __forceinline__ uint32_t li(uint32_t l, uint32_t sy, uint32_t sx) const {
+        return (l * (TH + 2) + sy) * 34u + sx;
+    }
+    __device__ __forceinline__ uint32_t si(uint32_t plane, uint32_t l, uint32_t y, uint32_t x) const {
+        return ((plane * L + l) * TH + y) * 32u + x;
+    }
 };
 
-// Price of the planar move p -> c between staged cells; kMax = not allowed.
-// A kMax base price blocks only in the directed form: the reference's axis gap
-// price may itself saturate and still yields the capped step.
-template <bool DIRECTED>
-__device__ __forceinline__ uint32_t planar_step(const TileSmem &s, uint32_t p, uint32_t c, uint32_t base,
-                                                uint8_t out_bit, uint8_t in_bit) {
-    uint32_t e = s.ent[c];
-    if (e == kMax) return kMax;
-    if ((s.fl[p] & out_bit) | (s.fl[c] & in_bit)) return kMax;
-    if (DIRECTED && base == kMax) return kMax;
-    return capmul(base, e);
+// One directional pass over lines of K*S cells, S consecutive lanes per line
+// (K cells each).  Each lane runs its segment's local chain, the S lanes combine
+// their transfer functions f(t) = min(A, t (+) (D, H)) with a Kogge-Stone scan,
+// and every cell takes min(local, incoming (+) prefix).  `cell(line, pos, &lab,
+// &step)` maps the pos-th cell of a line in traversal order; `halo(line)` is the
+// label index before the first cell, or kNone.  Returns whether any label fell.
+template <int K, int S, class CellFn, class HaloFn>
+__device__ __forceinline__ bool seg_pass(const Tile &t, uint32_t nlines, CellFn cell, HaloFn halo) {
+    bool changed = false;
+    const uint32_t lanes_total = nlines * S;  // a multiple of 32: whole warps are active or idle
+    for (uint32_t base = 0; base < lanes_total; base += blockDim.x) {
+        const uint32_t tl = base + threadIdx.x;
+        if (base + (threadIdx.x & ~31u) >= lanes_total) break;
+        const uint32_t line = tl / S, seg = tl % S;
+        u64 v[K], u[K];
+        uint32_t sp[K], P[K], li[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            uint32_t sidx;
+            cell(line, seg * K + i, &li[i], &sidx);
+            v[i] = t.lab[li[i]];
+            sp[i] = t.st[sidx];
+        }
+        u[0] = v[0];
+        P[0] = sp[0];
+#pragma unroll
+        for (int i = 1; i < K; ++i) {
+            u[i] = umin64(v[i], ext2(u[i - 1], sp[i], 1));
+            P[i] = dsum(P[i - 1], sp[i]);
+        }
+        u64 A = u[K - 1];
+        uint32_t D = P[K - 1], H = K;
+#pragma unroll
+        for (int o = 1; o < S; o <<= 1) {
+            const u64 Ap = __shfl_up_sync(0xFFFFFFFFu, A, o, S);
+            const uint32_t Dp = __shfl_up_sync(0xFFFFFFFFu, D, o, S);
+            const uint32_t Hp = __shfl_up_sync(0xFFFFFFFFu, H, o, S);
+            if (seg >= (uint32_t)o) {
+                A = umin64(A, ext2(Ap, D, H));
+                D = dsum(Dp, D);
+                H = Hp + H;
+            }
+        }
+        const uint32_t hi = halo(line);
+        const u64 hl = hi == kNone ? kInf : t.lab[hi];
+        u64 C = hl;
+        if (S > 1) {
+            const u64 Fa = __shfl_up_sync(0xFFFFFFFFu, A, 1, S);
+            const uint32_t Fd = __shfl_up_sync(0xFFFFFFFFu, D, 1, S);
+            const uint32_t Fh = __shfl_up_sync(0xFFFFFFFFu, H, 1, S);
+            if (seg > 0) C = umin64(Fa, ext2(hl, Fd, Fh));
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const u64 w = umin64(u[i], ext2(C, P[i], (uint32_t)i + 1u));
+            if (w < v[i]) {
+                t.lab[li[i]] = w;
+                changed = true;
+            }
+        }
+    }
+    return changed;
+}
+
+// Step price of the planar move p -> c read from HBM (staging and push checks).
+// out_bit / in_bit are the Grid::BOARD_EDGE_* bits of the move; dir is the
+// directed in-price slot of c (0 = from -y, 1 = -x, 2 = +x, 3 = +y).
+__device__ __forceinline__ uint32_t planar_step_g(const DevBoard &b, uint32_t ec, uint8_t fp, uint8_t fc,
+                                                  uint8_t out_bit, uint8_t in_bit, uint32_t gcell_c, uint32_t dir,
+                                                  uint32_t gap) {
+    if (ec == kMax) return kMax;
+    if ((fp & out_bit) | (fc & in_bit)) return kMax;
+    uint32_t base = gap;
+    if (b.directed) {
+        const uint4 d4 = __ldg(b.directed + gcell_c);
+        base = dir == 0 ? d4.x : dir == 1 ? d4.y : dir == 2 ? d4.z : d4.w;
+        if (base == kMax) return kMax;
+    }
+    return capmul(base, ec);
 }
 
 // Grid-wide barrier for a cooperative launch.  The wait is bounded: after
@@ -87,7 +181,88 @@ __device__ void grid_barrier(Ctl *c, uint32_t nblocks) {
 
 __device__ __forceinline__ uint32_t ld_status(const Ctl *c) { return *(volatile const uint32_t *)&c->status; }
 
-template <bool DIRECTED>
+// Flags of a window cell as a via endpoint: blocked by the board via node bit or
+// by the static via mask unless the net lists the cell as a via pad.
+__device__ __forceinline__ bool via_blocked(const DevField &f, const uint32_t *pads, uint32_t gcell, uint8_t gf) {
+    return (cell_tile_flags(f, pads, gcell, gf) & kViaBlocked) != 0;
+}
+
+template <int SC>
+__device__ __forceinline__ bool relax_tile(const Tile &t, uint32_t via_mask) {
+    const uint32_t L = t.L, TH = t.TH;
+    bool ch = false;
+    // rows: 4 lanes x 8 cells per 32-cell row; forward (-x to +x) then backward
+    ch |= seg_pass<8, 4>(
+        t, L * TH,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
+            const uint32_t l = line / TH, y = line % TH;
+            *li = t.li(l, y + 1, pos + 1);
+            *si = t.si(kFromNegX, l, y, pos);
+        },
+        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 0); });
+    __syncwarp();
+    ch |= seg_pass<8, 4>(
+        t, L * TH,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
+            const uint32_t l = line / TH, y = line % TH, x = 31 - pos;
+            *li = t.li(l, y + 1, x + 1);
+            *si = t.si(kFromPosX, l, y, x);
+        },
+        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 33); });
+    __syncthreads();
+    // columns: TH/8 lanes x 8 cells per column; down then up
+    ch |= seg_pass<8, SC>(
+        t, L * 32,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
+            const uint32_t l = line / 32, x = line % 32;
+            *li = t.li(l, pos + 1, x + 1);
+            *si = t.si(kFromNegY, l, pos, x);
+        },
+        [&](uint32_t line) { return t.li(line / 32, 0, line % 32 + 1); });
+    __syncwarp();
+    ch |= seg_pass<8, SC>(
+        t, L * 32,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
+            const uint32_t l = line / 32, x = line % 32, y = TH - 1 - pos;
+            *li = t.li(l, y + 1, x + 1);
+            *si = t.si(kFromPosY, l, y, x);
+        },
+        [&](uint32_t line) { return t.li(line / 32, TH + 1, line % 32 + 1); });
+    if (L > 1) {
+        __syncthreads();
+        // layer stacks: one thread per (x, y), up then down
+        for (uint32_t r = threadIdx.x; r < TH * 32; r += blockDim.x) {
+            const uint32_t y = r / 32, x = r % 32;
+            u64 prev = kInf;
+            for (uint32_t l = 0; l < L; ++l) {
+                const uint32_t c = t.li(l, y + 1, x + 1);
+                const u64 cur = t.lab[c];
+                const u64 w = umin64(cur, ext2(prev, l ? t.st[t.si(kFromBelow, l, y, x)] : kMax, 1));
+                if (w < cur) {
+                    t.lab[c] = w;
+                    ch = true;
+                }
+                prev = w;
+            }
+            prev = kInf;
+            for (int l = (int)L - 1; l >= 0; --l) {
+                const uint32_t c = t.li((uint32_t)l, y + 1, x + 1);
+                const u64 cur = t.lab[c];
+                const u64 w =
+                    umin64(cur, ext2(prev, (uint32_t)l + 1 < L ? t.st[t.si(kFromAbove, (uint32_t)l, y, x)] : kMax, 1));
+                if (w < cur) {
+                    t.lab[c] = w;
+                    ch = true;
+                }
+                prev = w;
+            }
+        }
+    }
+    (void)via_mask;
+    return ch;
+}
+
+template <int SC>
 __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const DevBoard b = a.board;
@@ -95,22 +270,14 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
     const uint32_t TH = a.tile_h;
     const uint32_t SW = kTW + 2, SH = TH + 2;
     const uint32_t nsm = L * SH * SW;
-    TileSmem s;
-    s.lab = reinterpret_cast<u64 *>(smem_raw);
-    s.ent = reinterpret_cast<uint32_t *>(s.lab + nsm);
-    s.fl = reinterpret_cast<uint8_t *>(s.ent + nsm);
-    s.din = nullptr;
-    if (DIRECTED) {
-        size_t off = (size_t)nsm * 13;
-        off = (off + 15) & ~(size_t)15;
-        s.din = reinterpret_cast<uint4 *>(smem_raw + off);
-    }
-    __shared__ uint32_t xe_s[kTW + 2];
-    __shared__ uint32_t ye_s[34];
+    Tile tile;
+    tile.lab = reinterpret_cast<u64 *>(smem_raw);
+    tile.st = reinterpret_cast<uint32_t *>(tile.lab + nsm);
+    tile.L = L;
+    tile.TH = TH;
     __shared__ u64 s_item;
     __shared__ uint32_t s_push[4];
     __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
-    __shared__ uint32_t s_sweeps;
 
     Ctl *ctl = a.ctl;
     const uint32_t tid = threadIdx.x;
@@ -151,7 +318,6 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
                 const uint32_t idx = atomicAdd(&ctl->head[cur], 1u);
                 s_item = idx < n ? __ldcg(a.lists + (size_t)cur * cap + idx) : kInf;
                 s_push[0] = s_push[1] = s_push[2] = s_push[3] = 0;
-                s_sweeps = 0;
             }
             __syncthreads();
             const u64 item = s_item;
@@ -175,43 +341,75 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
             }
             __syncthreads();
 
-            // ---- stage the tile and its halo ring (labels through L2) -------
+            // ---- stage labels (tile + halo ring, through L2) ------------------
             for (uint32_t i = tid; i < nsm; i += blockDim.x) {
                 const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
                 const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
                 u64 lv = kInf;
-                uint32_t ent = kMax;
-                uint8_t fl = 0;
                 if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1) {
-                    const bool hx = sx == 0 || sx == tw + 1, hy = sy == 0 || sy == th + 1;
+                    const bool hx = sx == 0 || sx == SW - 1, hy = sy == 0 || sy == SH - 1;
                     uint32_t owner;  // which tile's label this smem cell holds
                     if (hx && hy) owner = 5;  // corner: never read
                     else if (sx == 0) owner = 1;
-                    else if (sx == tw + 1) owner = 2;
+                    else if (sx == SW - 1) owner = 2;
                     else if (sy == 0) owner = 3;
-                    else if (sy == th + 1) owner = 4;
+                    else if (sy == SH - 1) owner = 4;
                     else owner = 0;
                     const uint32_t gcell = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
                     const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0);
                     if (owner < 5 && s_vis[owner]) lv = __ldcg(lab + lc);
                     else if (owner == 0 && gcell == f.src) lv = 0;  // first visit of the source tile
-                    const uint8_t gf = b.flags ? __ldg(b.flags + gcell) : 0;
-                    ent = cell_enter(b, f, a.pads, gcell, gf);
-                    fl = cell_tile_flags(f, a.pads, gcell, gf);
-                    if (DIRECTED && owner == 0) s.din[(l * TH + sy - 1) * kTW + sx - 1] = __ldg(b.directed + gcell);
                 }
-                s.lab[i] = lv;
-                s.ent[i] = ent;
-                s.fl[i] = fl;
+                tile.lab[i] = lv;
             }
-            // xe_s[sx] prices the gap between shared columns sx-1 and sx.
-            for (uint32_t i = tid; i < SW; i += blockDim.x) {
-                const int g = tx0 + (int)i - 2;
-                xe_s[i] = (g >= 0 && g + 1 < (int)b.w) ? __ldg(b.x_edge + g) : kMax;
-            }
-            for (uint32_t i = tid; i < SH; i += blockDim.x) {
-                const int g = ty0 + (int)i - 2;
-                ye_s[i] = (g >= 0 && g + 1 < (int)b.h) ? __ldg(b.y_edge + g) : kMax;
+            // ---- step prices into every interior cell -------------------------
+            for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
+                const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+                const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+                uint32_t s0 = kMax, s1 = kMax, s2 = kMax, s3 = kMax, s4 = kMax, s5 = kMax;
+                if (gx < wx1 && gy < wy1) {
+                    const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                    const uint8_t fc = b.flags ? __ldg(b.flags + gc) : 0;
+                    const uint32_t ec = cell_enter(b, f, a.pads, gc, fc);
+                    if (ec != kMax) {
+                        if (gx > wx0) {
+                            const uint8_t fp = b.flags ? __ldg(b.flags + gc - 1) : 0;
+                            s0 = planar_step_g(b, ec, fp, fc, kEdgePosX, kEdgeNegX, gc, 1, __ldg(b.x_edge + gx - 1));
+                        }
+                        if (gx + 1 < wx1) {
+                            const uint8_t fp = b.flags ? __ldg(b.flags + gc + 1) : 0;
+                            s1 = planar_step_g(b, ec, fp, fc, kEdgeNegX, kEdgePosX, gc, 2, __ldg(b.x_edge + gx));
+                        }
+                        if (gy > wy0) {
+                            const uint8_t fp = b.flags ? __ldg(b.flags + gc - b.w) : 0;
+                            s2 = planar_step_g(b, ec, fp, fc, kEdgePosY, kEdgeNegY, gc, 0, __ldg(b.y_edge + gy - 1));
+                        }
+                        if (gy + 1 < wy1) {
+                            const uint8_t fp = b.flags ? __ldg(b.flags + gc + b.w) : 0;
+                            s3 = planar_step_g(b, ec, fp, fc, kEdgeNegY, kEdgePosY, gc, 3, __ldg(b.y_edge + gy));
+                        }
+                        if (L > 1) {
+                            const bool vc = via_blocked(f, a.pads, gc, fc);
+                            const uint32_t plane = b.w * b.h;
+                            if (l > 0 && ((b.via_mask >> (l - 1)) & 1u) && !vc) {
+                                const uint32_t gp = gc - plane;
+                                if (!via_blocked(f, a.pads, gp, b.flags ? __ldg(b.flags + gp) : 0))
+                                    s4 = capmul(__ldg(b.via_edge + l - 1), ec);
+                            }
+                            if (l + 1 < L && ((b.via_mask >> l) & 1u) && !vc) {
+                                const uint32_t gp = gc + plane;
+                                if (!via_blocked(f, a.pads, gp, b.flags ? __ldg(b.flags + gp) : 0))
+                                    s5 = capmul(__ldg(b.via_edge + l), ec);
+                            }
+                        }
+                    }
+                }
+                tile.st[tile.si(kFromNegX, l, y, x)] = s0;
+                tile.st[tile.si(kFromPosX, l, y, x)] = s1;
+                tile.st[tile.si(kFromNegY, l, y, x)] = s2;
+                tile.st[tile.si(kFromPosY, l, y, x)] = s3;
+                tile.st[tile.si(kFromBelow, l, y, x)] = s4;
+                tile.st[tile.si(kFromAbove, l, y, x)] = s5;
             }
             __syncthreads();
 
@@ -219,110 +417,7 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
             const uint32_t sweep_limit = L * kTW * TH + 4;
             uint32_t sweep = 0;
             for (;;) {
-                bool ch = false;
-                // rows: one thread per (layer, row)
-                for (uint32_t r = tid; r < L * th; r += blockDim.x) {
-                    const uint32_t l = r / th, ty = r % th;
-                    const uint32_t base = (l * SH + ty + 1) * SW;
-                    u64 prev = s.lab[base];
-                    for (uint32_t sx = 1; sx <= tw; ++sx) {
-                        const uint32_t c = base + sx;
-                        u64 cur = s.lab[c];
-                        const uint32_t bp = DIRECTED ? s.din[(l * TH + ty) * kTW + sx - 1].y : xe_s[sx];
-                        const u64 cand = extend(prev, planar_step<DIRECTED>(s, c - 1, c, bp, kEdgePosX, kEdgeNegX));
-                        if (cand < cur) {
-                            cur = cand;
-                            s.lab[c] = cur;
-                            ch = true;
-                        }
-                        prev = cur;
-                    }
-                    prev = s.lab[base + tw + 1];
-                    for (uint32_t sx = tw; sx >= 1; --sx) {
-                        const uint32_t c = base + sx;
-                        u64 cur = s.lab[c];
-                        const uint32_t bp = DIRECTED ? s.din[(l * TH + ty) * kTW + sx - 1].z : xe_s[sx + 1];
-                        const u64 cand = extend(prev, planar_step<DIRECTED>(s, c + 1, c, bp, kEdgeNegX, kEdgePosX));
-                        if (cand < cur) {
-                            cur = cand;
-                            s.lab[c] = cur;
-                            ch = true;
-                        }
-                        prev = cur;
-                    }
-                }
-                __syncthreads();
-                // columns: one thread per (layer, column)
-                for (uint32_t r = tid; r < L * tw; r += blockDim.x) {
-                    const uint32_t l = r / tw, tx = r % tw;
-                    const uint32_t base = l * SH * SW + tx + 1;
-                    u64 prev = s.lab[base];
-                    for (uint32_t sy = 1; sy <= th; ++sy) {
-                        const uint32_t c = base + sy * SW;
-                        u64 cur = s.lab[c];
-                        const uint32_t bp = DIRECTED ? s.din[(l * TH + sy - 1) * kTW + tx].x : ye_s[sy];
-                        const u64 cand = extend(prev, planar_step<DIRECTED>(s, c - SW, c, bp, kEdgePosY, kEdgeNegY));
-                        if (cand < cur) {
-                            cur = cand;
-                            s.lab[c] = cur;
-                            ch = true;
-                        }
-                        prev = cur;
-                    }
-                    prev = s.lab[base + (th + 1) * SW];
-                    for (uint32_t sy = th; sy >= 1; --sy) {
-                        const uint32_t c = base + sy * SW;
-                        u64 cur = s.lab[c];
-                        const uint32_t bp = DIRECTED ? s.din[(l * TH + sy - 1) * kTW + tx].w : ye_s[sy + 1];
-                        const u64 cand = extend(prev, planar_step<DIRECTED>(s, c + SW, c, bp, kEdgeNegY, kEdgePosY));
-                        if (cand < cur) {
-                            cur = cand;
-                            s.lab[c] = cur;
-                            ch = true;
-                        }
-                        prev = cur;
-                    }
-                }
-                if (L > 1) {
-                    __syncthreads();
-                    // layer stacks: one thread per (x, y), up then down
-                    for (uint32_t r = tid; r < th * tw; r += blockDim.x) {
-                        const uint32_t ty = r / tw, tx = r % tw;
-                        const uint32_t base = (ty + 1) * SW + tx + 1;
-                        const uint32_t lstride = SH * SW;
-                        u64 prev = s.lab[base];
-                        for (uint32_t l = 1; l < L; ++l) {
-                            const uint32_t c = base + l * lstride, p = c - lstride;
-                            u64 cur = s.lab[c];
-                            uint32_t st = kMax;
-                            if (((b.via_mask >> (l - 1)) & 1u) && !((s.fl[p] | s.fl[c]) & kViaBlocked) &&
-                                s.ent[c] != kMax)
-                                st = capmul(__ldg(b.via_edge + l - 1), s.ent[c]);
-                            const u64 cand = extend(prev, st);
-                            if (cand < cur) {
-                                cur = cand;
-                                s.lab[c] = cur;
-                                ch = true;
-                            }
-                            prev = cur;
-                        }
-                        for (int l = (int)L - 2; l >= 0; --l) {
-                            const uint32_t c = base + (uint32_t)l * lstride, p = c + lstride;
-                            u64 cur = s.lab[c];
-                            uint32_t st = kMax;
-                            if (((b.via_mask >> l) & 1u) && !((s.fl[p] | s.fl[c]) & kViaBlocked) &&
-                                s.ent[c] != kMax)
-                                st = capmul(__ldg(b.via_edge + l), s.ent[c]);
-                            const u64 cand = extend(prev, st);
-                            if (cand < cur) {
-                                cur = cand;
-                                s.lab[c] = cur;
-                                ch = true;
-                            }
-                            prev = cur;
-                        }
-                    }
-                }
+                const bool ch = relax_tile<SC>(tile, b.via_mask);
                 ++sweep;
                 const int any = __syncthreads_or(ch ? 1 : 0);
                 if (!any) break;
@@ -336,10 +431,9 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
             u64 *labw = a.lab + f.lab_off;
             for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
                 const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
-                const uint32_t c = (l * SH + ty + 1) * SW + tx + 1;
                 const uint64_t lc =
                     ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-                labw[lc] = s.lab[c];
+                labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
             }
             // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
             const uint32_t nb = 2 * L * th + 2 * L * tw;
@@ -358,56 +452,41 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
                     k = r % tw;
                 }
                 bool exists;
-                uint32_t bc, nc, dir;
+                uint32_t bsx, bsy, nsx, nsy, dir;
                 uint8_t out_bit, in_bit;
-                uint32_t gap;
                 if (side == 0) {
                     exists = txi > 0;
-                    bc = (l * SH + k + 1) * SW + 1;
-                    nc = bc - 1;
-                    dir = 2;
-                    out_bit = kEdgeNegX;
-                    in_bit = kEdgePosX;
-                    gap = xe_s[1];
+                    bsx = 1; bsy = k + 1; nsx = 0; nsy = bsy;
+                    dir = 2; out_bit = kEdgeNegX; in_bit = kEdgePosX;
                 } else if (side == 1) {
                     exists = txi + 1 < ntx;
-                    bc = (l * SH + k + 1) * SW + tw;
-                    nc = bc + 1;
-                    dir = 1;
-                    out_bit = kEdgePosX;
-                    in_bit = kEdgeNegX;
-                    gap = xe_s[tw + 1];
+                    bsx = tw; bsy = k + 1; nsx = tw + 1; nsy = bsy;
+                    dir = 1; out_bit = kEdgePosX; in_bit = kEdgeNegX;
                 } else if (side == 2) {
                     exists = tyi > 0;
-                    bc = (l * SH + 1) * SW + k + 1;
-                    nc = bc - SW;
-                    dir = 3;
-                    out_bit = kEdgeNegY;
-                    in_bit = kEdgePosY;
-                    gap = ye_s[1];
+                    bsx = k + 1; bsy = 1; nsx = bsx; nsy = 0;
+                    dir = 3; out_bit = kEdgeNegY; in_bit = kEdgePosY;
                 } else {
                     exists = tyi + 1 < nty;
-                    bc = (l * SH + th) * SW + k + 1;
-                    nc = bc + SW;
-                    dir = 0;
-                    out_bit = kEdgePosY;
-                    in_bit = kEdgeNegY;
-                    gap = ye_s[th + 1];
+                    bsx = k + 1; bsy = th; nsx = bsx; nsy = th + 1;
+                    dir = 0; out_bit = kEdgePosY; in_bit = kEdgeNegY;
                 }
                 if (!exists || s_push[side]) continue;
-                const u64 lb = s.lab[bc];
-                if (lb == kInf || s.ent[nc] == kMax) continue;
-                uint32_t base = gap;
-                if (DIRECTED) {
-                    // the neighbour's in-price is not staged; read it from HBM
-                    const uint32_t nsx = nc % SW, nsy = (nc / SW) % SH;
-                    const uint32_t gcell =
-                        (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
-                    const uint4 d4 = __ldg(b.directed + gcell);
-                    base = dir == 0 ? d4.x : dir == 1 ? d4.y : dir == 2 ? d4.z : d4.w;
-                }
-                const u64 cand = extend(lb, planar_step<DIRECTED>(s, bc, nc, base, out_bit, in_bit));
-                if (cand < s.lab[nc]) s_push[side] = 1;
+                const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
+                if (lb == kInf) continue;
+                const uint32_t gb = (l * b.h + (uint32_t)(ty0 + (int)bsy - 1)) * b.w + (uint32_t)(tx0 + (int)bsx - 1);
+                const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
+                const uint8_t fb = b.flags ? __ldg(b.flags + gb) : 0, fn = b.flags ? __ldg(b.flags + gn) : 0;
+                const uint32_t en = cell_enter(b, f, a.pads, gn, fn);
+                if (en == kMax) continue;
+                const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
+                uint32_t gap;
+                if (side == 0) gap = __ldg(b.x_edge + gx_n);
+                else if (side == 1) gap = __ldg(b.x_edge + gx_n - 1);
+                else if (side == 2) gap = __ldg(b.y_edge + gy_n);
+                else gap = __ldg(b.y_edge + gy_n - 1);
+                const u64 cand = ext2(lb, planar_step_g(b, en, fb, fn, out_bit, in_bit, gn, dir, gap), 1);
+                if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
             }
             __syncthreads();
             if (tid == 0) {
@@ -662,35 +741,33 @@ cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, u
 }
 
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
-    const size_t nsm = (size_t)layers * (tile_h + 2) * (kTW + 2);
-    size_t bytes = nsm * 13;
-    if (directed) {
-        bytes = (bytes + 15) & ~(size_t)15;
-        bytes += (size_t)layers * tile_h * kTW * 16;
+    (void)directed;  // directed prices are folded into the step planes
+    return (size_t)layers * (tile_h + 2) * (kTW + 2) * 8 + (size_t)6 * layers * tile_h * kTW * 4;
+}
+
+namespace {
+const void *relax_fn(uint32_t tile_h) {
+    switch (tile_h) {
+        case 8: return (const void *)relax_rounds_kernel<1>;
+        case 16: return (const void *)relax_rounds_kernel<2>;
+        case 32: return (const void *)relax_rounds_kernel<4>;
+        default: return (const void *)relax_rounds_kernel<8>;
     }
-    return bytes;
+}
+}  // namespace
+
+cudaError_t relax_configure(uint32_t tile_h, size_t smem) {
+    return cudaFuncSetAttribute(relax_fn(tile_h), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-cudaError_t relax_configure(bool directed, size_t smem) {
-    if (directed)
-        return cudaFuncSetAttribute(relax_rounds_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return cudaFuncSetAttribute(relax_rounds_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
-
-cudaError_t relax_occupancy(bool directed, size_t smem, int *blocks_per_sm) {
-    if (directed)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_rounds_kernel<true>, kRelaxThreads,
-                                                             smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_rounds_kernel<false>, kRelaxThreads,
-                                                         smem);
+cudaError_t relax_occupancy(uint32_t tile_h, size_t smem, int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h), kRelaxThreads, smem);
 }
 
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, size_t smem, cudaStream_t st) {
     RelaxArgs copy = a;
     void *args[] = {&copy};
-    const void *fn =
-        a.board.directed ? (const void *)relax_rounds_kernel<true> : (const void *)relax_rounds_kernel<false>;
-    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kRelaxThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel(relax_fn(a.tile_h), dim3(grid), dim3(kRelaxThreads), args, smem, st);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {
