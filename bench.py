@@ -182,6 +182,7 @@ def run_engine(args):
     eng = mrcuda.Engine(local)
     board = eng.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
     batch = mrcuda.Batch(board, wl.nets, wl.windows, retry_full=True, time_kernels=True)
+    tuned = batch.autotune() if not args.no_autotune else None  # setup, outside the timed region
     stream = torch.cuda.Stream()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
@@ -258,7 +259,7 @@ def run_engine(args):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl.meta["workload"], "nets_per_rank": len(wl.nets), "window_cells": wl.window_cells(),
                    "routed": routed, "retried": first.retried, "l2": "flushed between steps (512 MiB write)",
-                   "windows": wl.meta.get("windows")},
+                   "windows": wl.meta.get("windows"), "autotuned": tuned},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": batch.kernel_launches * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -308,6 +309,7 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=8)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -185,6 +185,15 @@ mrc_status mrc_batch_create(mrc_context *ctx, const mrc_board *board, const mrc_
 mrc_status mrc_batch_launch(mrc_context *ctx, mrc_batch *batch, void *stream);
 /* Wait for the batch, run the full-board retry if flagged, copy results out. */
 mrc_status mrc_batch_finish(mrc_context *ctx, mrc_batch *batch, mrc_result **out);
+/* Autotuner: time every relax configuration (tile height 8/16/32/64 cells,
+ * 128 or 256 threads per CTA, and with them the CTAs per SM) on this batch,
+ * keep the fastest for the batch, and cache it in the context for later batches
+ * with the same layer count and price form.  Outputs may be NULL. */
+mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile_h, uint32_t *threads,
+                              float *best_ms);
+/* Force a relax configuration on a batch: tile height in {8, 16, 32, 64} cells
+ * and 128 or 256 threads per CTA.  MRC_ERR_LIMIT when the tile does not fit. */
+mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t tile_h, uint32_t threads);
 /* Kernels launched by the last mrc_batch_launch (for launch accounting). */
 uint32_t mrc_batch_kernel_launches(const mrc_batch *batch);
 /* Device milliseconds of the relax kernel of the last launch, from CUDA events

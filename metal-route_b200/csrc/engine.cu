@@ -100,6 +100,8 @@ struct mrc_context {
     Pool pool;
     int sms = 148;
     size_t smem_optin = 0;
+    // autotuned relax configuration per (layers, directed): tile height, CTA width
+    std::map<uint32_t, std::pair<uint32_t, uint32_t>> tuned;
 };
 
 namespace {
@@ -350,7 +352,7 @@ struct mrc_batch {
     std::vector<mrc_window> windows;
     std::vector<DevField> fields;  // ascending lab_off (largest windows first)
     uint64_t total_cells = 0;
-    uint32_t total_tiles = 0, max_tiles = 0, tile_h = 32, grid = 1;
+    uint32_t total_tiles = 0, max_tiles = 0, tile_h = 32, threads = kRelaxThreads, grid = 1;
     size_t smem = 0;
     DBuf d_fields, d_pads, d_lab, d_tstamp, d_tvisit, d_lists, d_costs, d_lens, d_offsets, d_cells, d_ctl, d_out;
     uint32_t launches = 0;
@@ -384,6 +386,40 @@ mrc_status choose_tile(mrc_context *ctx, uint32_t layers, bool directed, uint32_
     return fail(MRC_ERR_LIMIT, "too many layers for one shared-memory tile");
 }
 
+uint32_t tune_key(uint32_t layers, bool directed) { return layers * 2u + (directed ? 1u : 0u); }
+
+// Tile-dependent layout of a staged batch: tile offsets, the CTA grid and the
+// per-tile buffers.  Re-run by the autotuner for every candidate.
+mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
+    mrc_context *ctx = bt->ctx;
+    const mrc_board *board = bt->board;
+    bt->tile_h = tile_h;
+    bt->threads = threads;
+    bt->smem = relax_smem_bytes(board->view.layers, tile_h, board->directed);
+    uint64_t toff = 0;
+    uint32_t max_tiles = 1;
+    for (DevField &f : bt->fields) {
+        const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + tile_h - 1) / tile_h);
+        f.tile_off = (uint32_t)std::min<uint64_t>(toff, 0xFFFFFFFFull);
+        toff += tiles;
+        max_tiles = (uint32_t)std::max<uint64_t>(max_tiles, tiles);
+    }
+    if (toff > 0x7FFFFFFFull) return fail(MRC_ERR_LIMIT, "batch has more than 2^31 tiles");
+    bt->total_tiles = (uint32_t)std::max<uint64_t>(toff, 1);
+    bt->max_tiles = max_tiles;
+    int per_sm = 1;
+    MRC_CUDA(relax_configure(tile_h, threads, bt->smem), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm), "relax occupancy");
+    if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
+    // cooperative launch: every CTA must be co-resident
+    bt->grid = (uint32_t)ctx->sms * (uint32_t)per_sm;
+    MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
+    MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
+    MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
+    MRC_TRY(bt->d_lists.get(ctx, (size_t)bt->total_tiles * 3 * 8, "tile lists"));
+    return MRC_OK;
+}
+
 mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> nets,
                        std::vector<mrc_window> windows, uint32_t flags, mrc_batch *bt) {
     const GridView &g = board->view;
@@ -393,7 +429,15 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
     bt->nets = std::move(nets);
     bt->windows = std::move(windows);
     const uint32_t n = (uint32_t)bt->nets.size();
-    MRC_TRY(choose_tile(ctx, g.layers, board->directed, &bt->tile_h, &bt->smem));
+    uint32_t tile_h = 0, threads = kRelaxThreads;
+    size_t smem = 0;
+    auto tuned = ctx->tuned.find(tune_key(g.layers, board->directed));
+    if (tuned != ctx->tuned.end()) {
+        tile_h = tuned->second.first;
+        threads = tuned->second.second;
+    } else {
+        MRC_TRY(choose_tile(ctx, g.layers, board->directed, &tile_h, &smem));
+    }
     // largest windows first: the persistent CTAs then finish together
     std::vector<uint32_t> order(n);
     std::iota(order.begin(), order.end(), 0u);
@@ -404,8 +448,7 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cells_of(a) > cells_of(b); });
     std::vector<uint32_t> pads;
     bt->fields.resize(n);
-    uint64_t off = 0, toff = 0;
-    uint32_t max_tiles = 1;
+    uint64_t off = 0;
     for (uint32_t k = 0; k < n; ++k) {
         const uint32_t i = order[k];
         const NetCopy &nc = bt->nets[i];
@@ -426,28 +469,13 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
         f.n_vpads = (uint32_t)nc.vpads.size();
         pads.insert(pads.end(), nc.vpads.begin(), nc.vpads.end());
         f.out = i;
-        const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + bt->tile_h - 1) / bt->tile_h);
-        f.tile_off = (uint32_t)toff;
-        toff += tiles;
-        if (toff > 0x7FFFFFFFull) return fail(MRC_ERR_LIMIT, "batch has more than 2^31 tiles");
-        max_tiles = std::max<uint32_t>(max_tiles, (uint32_t)tiles);
+        f.tile_off = 0;
         if (pads.size() > 0xFFFFFFF0u) return fail(MRC_ERR_LIMIT, "pad lists exceed 2^32 entries");
     }
     bt->total_cells = off;
-    bt->total_tiles = (uint32_t)std::max<uint64_t>(toff, 1);
-    bt->max_tiles = max_tiles;
-    int per_sm = 1;
-    MRC_CUDA(relax_configure(bt->tile_h, bt->smem), "configure relax kernel");
-    MRC_CUDA(relax_occupancy(bt->tile_h, bt->smem, &per_sm), "relax occupancy");
-    if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
-    // cooperative launch: every CTA must be co-resident
-    bt->grid = (uint32_t)ctx->sms * (uint32_t)per_sm;
-    MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
+    MRC_TRY(batch_layout(bt, tile_h, threads));
     MRC_TRY(upload(ctx, bt->d_pads, pads.data(), pads.size() * 4, "upload pads"));
     MRC_TRY(bt->d_lab.get(ctx, std::max<uint64_t>(off, 1) * 8, "labels"));
-    MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
-    MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
-    MRC_TRY(bt->d_lists.get(ctx, (size_t)bt->total_tiles * 3 * 8, "tile lists"));
     MRC_TRY(bt->d_costs.get(ctx, std::max<size_t>(n, 1) * 4, "costs"));
     MRC_TRY(bt->d_lens.get(ctx, std::max<size_t>(n, 1) * 4, "lengths"));
     MRC_TRY(bt->d_offsets.get(ctx, ((size_t)n + 1) * 8, "offsets"));
@@ -500,7 +528,7 @@ mrc_status batch_launch(mrc_batch *bt, cudaStream_t st) {
     ra.round_limit = 64u * bt->max_tiles + 4096u;
     if (n) {
         if (bt->ev0) MRC_CUDA(cudaEventRecord(bt->ev0, st), "record event");
-        MRC_CUDA(relax_launch(ra, bt->grid, bt->smem, st), "launch relax kernel");
+        MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st), "launch relax kernel");
         if (bt->ev1) MRC_CUDA(cudaEventRecord(bt->ev1, st), "record event");
         bt->launches++;
     }
@@ -874,6 +902,66 @@ mrc_status mrc_batch_finish(mrc_context *ctx, mrc_batch *batch, mrc_result **out
     MRC_TRY(set_device(ctx));
     if (!batch->stream) return fail(MRC_ERR_INVALID_ARGUMENT, "batch was never launched");
     return solve(ctx, batch->board, {}, {}, batch->flags, out, batch);
+}
+
+mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile_h, uint32_t *threads,
+                              float *best_ms) {
+    if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    const uint32_t layers = batch->board->view.layers;
+    const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MRC_CUDA(cudaEventCreate(&e0), "create event");
+    MRC_CUDA(cudaEventCreate(&e1), "create event");
+    float best = -1.0f;
+    uint32_t best_th = batch->tile_h, best_nt = batch->threads;
+    mrc_status rc = MRC_OK;
+    for (uint32_t th : {8u, 16u, 32u, 64u}) {
+        if (relax_smem_bytes(layers, th, batch->board->directed) > hard) continue;
+        for (uint32_t nt : {128u, 256u}) {
+            if (4u * layers * th < nt / 2) continue;  // most lanes would idle in the line passes
+            rc = batch_layout(batch, th, nt);
+            if (rc != MRC_OK) break;
+            float ms = 0.0f, sum = 0.0f;
+            for (int rep = 0; rep < 2 && rc == MRC_OK; ++rep) {
+                cudaEventRecord(e0, ctx->stream);
+                rc = batch_launch(batch, ctx->stream);
+                cudaEventRecord(e1, ctx->stream);
+                if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(MRC_ERR_BACKEND_UNAVAILABLE, "autotune");
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep) sum += ms;  // the first launch warms the configuration
+            }
+            if (rc != MRC_OK) break;
+            if (best < 0.0f || sum < best) {
+                best = sum;
+                best_th = th;
+                best_nt = nt;
+            }
+        }
+        if (rc != MRC_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != MRC_OK) return rc;
+    MRC_TRY(batch_layout(batch, best_th, best_nt));
+    ctx->tuned[tune_key(layers, batch->board->directed)] = {best_th, best_nt};
+    if (tile_h) *tile_h = best_th;
+    if (threads) *threads = best_nt;
+    if (best_ms) *best_ms = best;
+    return MRC_OK;
+}
+
+mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t tile_h, uint32_t threads) {
+    if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if ((tile_h != 8 && tile_h != 16 && tile_h != 32 && tile_h != 64) || (threads != 128 && threads != 256))
+        return fail(MRC_ERR_INVALID_ARGUMENT, "tile height must be 8/16/32/64 and threads 128/256");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
+    if (relax_smem_bytes(batch->board->view.layers, tile_h, batch->board->directed) > hard)
+        return fail(MRC_ERR_LIMIT, "tile does not fit in shared memory");
+    return batch_layout(batch, tile_h, threads);
 }
 
 uint32_t mrc_batch_kernel_launches(const mrc_batch *batch) { return batch ? batch->launches : 0; }
@@ -1256,8 +1344,8 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     b.directed = directed ? reinterpret_cast<const uint4 *>(s + o_dir) : nullptr;
 
     int per_sm = 0;
-    MRC_CUDA(relax_configure(tile_h, smem), "configure relax kernel");
-    MRC_CUDA(relax_occupancy(tile_h, smem, &per_sm), "relax occupancy");
+    MRC_CUDA(relax_configure(tile_h, kRelaxThreads, smem), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(tile_h, kRelaxThreads, smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     RelaxArgs ra;
     ra.board = b;
@@ -1272,7 +1360,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     ra.ctl = reinterpret_cast<Ctl *>(s + o_ctl);
     ra.tile_h = tile_h;
     ra.round_limit = 64u * max_tiles + 4096u;
-    MRC_CUDA(relax_launch(ra, (uint32_t)dev->sms * (uint32_t)per_sm, smem, st), "launch relax kernel");
+    MRC_CUDA(relax_launch(ra, (uint32_t)dev->sms * (uint32_t)per_sm, kRelaxThreads, smem, st), "launch relax kernel");
     PathArgs pa;
     pa.board = b;
     pa.fields = ra.fields;

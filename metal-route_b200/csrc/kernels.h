@@ -10,7 +10,7 @@
 
 namespace mrc {
 
-constexpr int kRelaxThreads = 256;
+constexpr int kRelaxThreads = 256;  // default CTA width of the relax kernel
 
 // Status bits reported through Ctl::status / PathArgs::status.
 constexpr uint32_t kStatusActivationLimit = 1u << 0;
@@ -60,9 +60,10 @@ struct PlainArgs {
 
 // Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);
-cudaError_t relax_configure(uint32_t tile_h, size_t smem);
-cudaError_t relax_occupancy(uint32_t tile_h, size_t smem, int *blocks_per_sm);
-cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, size_t smem, cudaStream_t st);
+// The relax kernel is instantiated for threads in {128, 256} per CTA.
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem);
+cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm);
+cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);

@@ -57,40 +57,64 @@ __device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
 // at -x, +x, -y, +y, the layer below and the layer above.
 enum { kFromNegX = 0, kFromPosX = 1, kFromNegY = 2, kFromPosY = 3, kFromBelow = 4, kFromAbove = 5 };
 
+template <int TH>
 struct Tile {
     u64 *lab;        // [L][TH+2][34] labels with a one-cell halo ring
     uint32_t *st;    // [6][L][TH][32] step prices into interior cells
-    uint32_t L, TH;
+    uint8_t *rowd;   // [L][TH] row needs a sweep
+    uint8_t *cold;   // [L][32] column needs a sweep
+    uint8_t *stackd; // [TH][32] layer stack needs a sweep
+    uint32_t L;
     __device__ __forceinline__ uint32_t li(uint32_t l, uint32_t sy, uint32_t sx) const {
         return (l * (TH + 2) + sy) * 34u + sx;
     }
     __device__ __forceinline__ uint32_t si(uint32_t plane, uint32_t l, uint32_t y, uint32_t x) const {
         return ((plane * L + l) * TH + y) * 32u + x;
     }
+    // a label of interior cell (l, y, x) fell: every other line through it must be swept again
+    __device__ __forceinline__ void touched_by_row(uint32_t l, uint32_t y, uint32_t x) const {
+        cold[l * 32 + x] = 1;
+        stackd[y * 32 + x] = 1;
+    }
+    __device__ __forceinline__ void touched_by_col(uint32_t l, uint32_t y, uint32_t x) const {
+        rowd[l * TH + y] = 1;
+        stackd[y * 32 + x] = 1;
+    }
+    __device__ __forceinline__ void touched_by_stack(uint32_t l, uint32_t y, uint32_t x) const {
+        rowd[l * TH + y] = 1;
+        cold[l * 32 + x] = 1;
+    }
 };
 
 // One directional pass over lines of K*S cells, S consecutive lanes per line
-// (K cells each).  Each lane runs its segment's local chain, the S lanes combine
-// their transfer functions f(t) = min(A, t (+) (D, H)) with a Kogge-Stone scan,
-// and every cell takes min(local, incoming (+) prefix).  `cell(line, pos, &lab,
-// &step)` maps the pos-th cell of a line in traversal order; `halo(line)` is the
-// label index before the first cell, or kNone.  Returns whether any label fell.
-template <int K, int S, class CellFn, class HaloFn>
-__device__ __forceinline__ bool seg_pass(const Tile &t, uint32_t nlines, CellFn cell, HaloFn halo) {
+// (K cells each), skipping lines whose dirty flag is clear.  Each lane runs its
+// segment's local chain, the S lanes combine their transfer functions
+// f(t) = min(A, t (+) (D, H)) with a Kogge-Stone scan, and every cell takes
+// min(local, incoming (+) prefix).  `cell(line, pos, &lab, &step)` maps the
+// pos-th cell of a line in traversal order; `halo(line)` is the label index
+// before the first cell; `touch(line, pos)` marks the crossing lines of a cell
+// whose label fell; `clear` resets the line's dirty flag (last pass of a pair).
+template <int K, int S, class CellFn, class HaloFn, class TouchFn>
+__device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *dirty, uint32_t nlines, bool clear,
+                                         CellFn cell, HaloFn halo, TouchFn touch) {
     bool changed = false;
     const uint32_t lanes_total = nlines * S;  // a multiple of 32: whole warps are active or idle
     for (uint32_t base = 0; base < lanes_total; base += blockDim.x) {
-        const uint32_t tl = base + threadIdx.x;
         if (base + (threadIdx.x & ~31u) >= lanes_total) break;
+        const uint32_t tl = base + threadIdx.x;
         const uint32_t line = tl / S, seg = tl % S;
+        const bool mine = dirty[line] != 0;
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, mine);
+        if (!mine) continue;  // whole S-lane groups drop out together
+        if (clear && seg == 0) dirty[line] = 0;
         u64 v[K], u[K];
         uint32_t sp[K], P[K], li[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             uint32_t sidx;
             cell(line, seg * K + i, &li[i], &sidx);
-            v[i] = t.lab[li[i]];
-            sp[i] = t.st[sidx];
+            v[i] = lab[li[i]];
+            sp[i] = st[sidx];
         }
         u[0] = v[0];
         P[0] = sp[0];
@@ -103,29 +127,32 @@ __device__ __forceinline__ bool seg_pass(const Tile &t, uint32_t nlines, CellFn 
         uint32_t D = P[K - 1], H = K;
 #pragma unroll
         for (int o = 1; o < S; o <<= 1) {
-            const u64 Ap = __shfl_up_sync(0xFFFFFFFFu, A, o, S);
-            const uint32_t Dp = __shfl_up_sync(0xFFFFFFFFu, D, o, S);
-            const uint32_t Hp = __shfl_up_sync(0xFFFFFFFFu, H, o, S);
+            const u64 Ap = __shfl_up_sync(mask, A, o, S);
+            const uint32_t Dp = __shfl_up_sync(mask, D, o, S);
+            const uint32_t Hp = __shfl_up_sync(mask, H, o, S);
             if (seg >= (uint32_t)o) {
                 A = umin64(A, ext2(Ap, D, H));
                 D = dsum(Dp, D);
                 H = Hp + H;
             }
         }
-        const uint32_t hi = halo(line);
-        const u64 hl = hi == kNone ? kInf : t.lab[hi];
+        const u64 hl = lab[halo(line)];
         u64 C = hl;
         if (S > 1) {
-            const u64 Fa = __shfl_up_sync(0xFFFFFFFFu, A, 1, S);
-            const uint32_t Fd = __shfl_up_sync(0xFFFFFFFFu, D, 1, S);
-            const uint32_t Fh = __shfl_up_sync(0xFFFFFFFFu, H, 1, S);
+            const u64 Fa = __shfl_up_sync(mask, A, 1, S);
+            const uint32_t Fd = __shfl_up_sync(mask, D, 1, S);
+            const uint32_t Fh = __shfl_up_sync(mask, H, 1, S);
             if (seg > 0) C = umin64(Fa, ext2(hl, Fd, Fh));
+        }
+        if (C != kInf) {
+#pragma unroll
+            for (int i = 0; i < K; ++i) u[i] = umin64(u[i], ext2(C, P[i], (uint32_t)i + 1u));
         }
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            const u64 w = umin64(u[i], ext2(C, P[i], (uint32_t)i + 1u));
-            if (w < v[i]) {
-                t.lab[li[i]] = w;
+            if (u[i] < v[i]) {
+                lab[li[i]] = u[i];
+                touch(line, seg * K + i);
                 changed = true;
             }
         }
@@ -187,51 +214,58 @@ __device__ __forceinline__ bool via_blocked(const DevField &f, const uint32_t *p
     return (cell_tile_flags(f, pads, gcell, gf) & kViaBlocked) != 0;
 }
 
-template <int SC>
-__device__ __forceinline__ bool relax_tile(const Tile &t, uint32_t via_mask) {
-    const uint32_t L = t.L, TH = t.TH;
+// One sweep of a staged tile: rows (4 lanes x 8 cells), columns (TH/8 lanes x
+// 8 cells), layer stacks (one thread each), each forward then backward, only
+// over lines whose dirty flag is set.
+template <int TH>
+__device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
+    constexpr int SC = TH / 8;
+    const uint32_t L = t.L;
     bool ch = false;
-    // rows: 4 lanes x 8 cells per 32-cell row; forward (-x to +x) then backward
     ch |= seg_pass<8, 4>(
-        t, L * TH,
+        t.lab, t.st, t.rowd, L * TH, false,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / TH, y = line % TH;
             *li = t.li(l, y + 1, pos + 1);
             *si = t.si(kFromNegX, l, y, pos);
         },
-        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 0); });
+        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 0); },
+        [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, pos); });
     __syncwarp();
     ch |= seg_pass<8, 4>(
-        t, L * TH,
+        t.lab, t.st, t.rowd, L * TH, true,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / TH, y = line % TH, x = 31 - pos;
             *li = t.li(l, y + 1, x + 1);
             *si = t.si(kFromPosX, l, y, x);
         },
-        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 33); });
+        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 33); },
+        [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, 31 - pos); });
     __syncthreads();
-    // columns: TH/8 lanes x 8 cells per column; down then up
     ch |= seg_pass<8, SC>(
-        t, L * 32,
+        t.lab, t.st, t.cold, L * 32, false,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / 32, x = line % 32;
             *li = t.li(l, pos + 1, x + 1);
             *si = t.si(kFromNegY, l, pos, x);
         },
-        [&](uint32_t line) { return t.li(line / 32, 0, line % 32 + 1); });
+        [&](uint32_t line) { return t.li(line / 32, 0, line % 32 + 1); },
+        [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, pos, line % 32); });
     __syncwarp();
     ch |= seg_pass<8, SC>(
-        t, L * 32,
+        t.lab, t.st, t.cold, L * 32, true,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / 32, x = line % 32, y = TH - 1 - pos;
             *li = t.li(l, y + 1, x + 1);
             *si = t.si(kFromPosY, l, y, x);
         },
-        [&](uint32_t line) { return t.li(line / 32, TH + 1, line % 32 + 1); });
+        [&](uint32_t line) { return t.li(line / 32, TH + 1, line % 32 + 1); },
+        [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, TH - 1 - pos, line % 32); });
     if (L > 1) {
         __syncthreads();
-        // layer stacks: one thread per (x, y), up then down
         for (uint32_t r = threadIdx.x; r < TH * 32; r += blockDim.x) {
+            if (!t.stackd[r]) continue;
+            t.stackd[r] = 0;
             const uint32_t y = r / 32, x = r % 32;
             u64 prev = kInf;
             for (uint32_t l = 0; l < L; ++l) {
@@ -240,6 +274,7 @@ __device__ __forceinline__ bool relax_tile(const Tile &t, uint32_t via_mask) {
                 const u64 w = umin64(cur, ext2(prev, l ? t.st[t.si(kFromBelow, l, y, x)] : kMax, 1));
                 if (w < cur) {
                     t.lab[c] = w;
+                    t.touched_by_stack(l, y, x);
                     ch = true;
                 }
                 prev = w;
@@ -252,29 +287,30 @@ __device__ __forceinline__ bool relax_tile(const Tile &t, uint32_t via_mask) {
                     umin64(cur, ext2(prev, (uint32_t)l + 1 < L ? t.st[t.si(kFromAbove, (uint32_t)l, y, x)] : kMax, 1));
                 if (w < cur) {
                     t.lab[c] = w;
+                    t.touched_by_stack((uint32_t)l, y, x);
                     ch = true;
                 }
                 prev = w;
             }
         }
     }
-    (void)via_mask;
     return ch;
 }
 
-template <int SC>
-__global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a) {
+template <int TH, int NT>
+__global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const DevBoard b = a.board;
     const uint32_t L = b.layers;
-    const uint32_t TH = a.tile_h;
     const uint32_t SW = kTW + 2, SH = TH + 2;
     const uint32_t nsm = L * SH * SW;
-    Tile tile;
+    Tile<TH> tile;
     tile.lab = reinterpret_cast<u64 *>(smem_raw);
     tile.st = reinterpret_cast<uint32_t *>(tile.lab + nsm);
+    tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kTW);
+    tile.cold = tile.rowd + L * TH;
+    tile.stackd = tile.cold + L * kTW;
     tile.L = L;
-    tile.TH = TH;
     __shared__ u64 s_item;
     __shared__ uint32_t s_push[4];
     __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
@@ -411,13 +447,14 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
                 tile.st[tile.si(kFromBelow, l, y, x)] = s4;
                 tile.st[tile.si(kFromAbove, l, y, x)] = s5;
             }
+            for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 1;
             __syncthreads();
 
             // ---- relax to local convergence ---------------------------------
             const uint32_t sweep_limit = L * kTW * TH + 4;
             uint32_t sweep = 0;
             for (;;) {
-                const bool ch = relax_tile<SC>(tile, b.via_mask);
+                const bool ch = relax_tile<TH>(tile);
                 ++sweep;
                 const int any = __syncthreads_or(ch ? 1 : 0);
                 if (!any) break;
@@ -489,25 +526,24 @@ __global__ void __launch_bounds__(kRelaxThreads) relax_rounds_kernel(RelaxArgs a
                 if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
             }
             __syncthreads();
-            if (tid == 0) {
+            if (tid < 5) {
                 __threadfence();  // labels before the visited flag and the queue entries
-                if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
-                const uint32_t nbr[4] = {t - 1, t + 1, t - ntx, t + ntx};
-                const uint32_t want = round + 2;  // stamp s = queued for round s-1
-                for (int sd = 0; sd < 4; ++sd) {
-                    if (!s_push[sd]) continue;
-                    const uint32_t g = f.tile_off + nbr[sd];
-                    if (atomicMax(a.tstamp + g, want) < want) {
+                if (tid == 4) {
+                    if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
+                    atomicAdd(&ctl->activations, 1ull);
+                    atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
+                } else if (s_push[tid]) {
+                    const uint32_t u = tid == 0 ? t - 1 : tid == 1 ? t + 1 : tid == 2 ? t - ntx : t + ntx;
+                    const uint32_t want = round + 2;  // stamp s = queued for round s-1
+                    if (atomicMax(a.tstamp + f.tile_off + u, want) < want) {
                         const uint32_t idx = atomicAdd(&ctl->count[nxt], 1u);
                         if (idx < cap) {
-                            a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | nbr[sd];
+                            a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | u;
                         } else {
                             atomicOr(&ctl->status, kStatusQueueOverflow);
                         }
                     }
                 }
-                atomicAdd(&ctl->activations, 1ull);
-                atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
             }
             __syncthreads();
         }
@@ -622,7 +658,9 @@ __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevFiel
 }
 
 // One warp per field: lanes 0..5 test the six neighbours (ascending CellIdx)
-// and the lowest qualifying one is the canonical predecessor.
+// and the lowest qualifying one is the canonical predecessor.  Each step issues
+// all of its loads at once (the candidate's label and tile flag, and the step
+// inputs) and carries the winner's label forward as the next target.
 __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
@@ -632,8 +670,14 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
     if (len == 0) return;
     const DevBoard b = a.board;
     const uint32_t plane = b.w * b.h;
+    const uint32_t ntx = (f.ww + kTW - 1) / kTW;
     uint32_t *out = a.cells + a.offsets[f.out];
     uint32_t cur = f.dst;
+    u64 need;
+    {
+        const uint32_t r = cur % plane;
+        need = field_label(a, f, r % b.w - f.x0, r / b.w - f.y0, cur / plane);
+    }
     for (uint32_t pos = len - 1;; --pos) {
         if (lane == 0) out[pos] = cur;
         if (pos == 0) {
@@ -641,9 +685,9 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
             break;
         }
         const uint32_t r = cur % plane, x = r % b.w, y = r / b.w, l = cur / plane;
-        const u64 need = field_label(a, f, x - f.x0, y - f.y0, l);
         bool ok = false;
         uint32_t p = 0;
+        u64 lp = kInf;
         if (lane < 6) {
             int px = (int)x, py = (int)y, pl = (int)l;
             if (lane == 0) pl -= 1;
@@ -655,11 +699,12 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
             if (pl >= 0 && pl < (int)b.layers && px >= (int)f.x0 && px < (int)(f.x0 + f.ww) && py >= (int)f.y0 &&
                 py < (int)(f.y0 + f.wh)) {
                 p = ((uint32_t)pl * b.h + (uint32_t)py) * b.w + (uint32_t)px;
-                const u64 lp = field_label(a, f, (uint32_t)px - f.x0, (uint32_t)py - f.y0, (uint32_t)pl);
-                if (lp != kInf) {
-                    const uint32_t st = global_step(b, f, a.pads, p, cur, (int)lane);
-                    ok = extend(lp, st) == need;
-                }
+                const uint32_t lx = (uint32_t)px - f.x0, ly = (uint32_t)py - f.y0;
+                const uint32_t vis = a.tvisit[f.tile_off + (ly / a.tile_h) * ntx + lx / kTW];
+                const u64 raw = a.lab[f.lab_off + ((uint64_t)pl * f.wh + ly) * f.ww + lx];
+                const uint32_t st = global_step(b, f, a.pads, p, cur, (int)lane);
+                lp = vis ? raw : kInf;
+                ok = lp != kInf && extend(lp, st) == need;
             }
         }
         const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
@@ -669,6 +714,7 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
         }
         const uint32_t win = __ffs(m) - 1;
         cur = __shfl_sync(0xFFFFFFFFu, p, win);
+        need = __shfl_sync(0xFFFFFFFFu, lp, win);
     }
 }
 
@@ -742,32 +788,34 @@ cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, u
 
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
     (void)directed;  // directed prices are folded into the step planes
-    return (size_t)layers * (tile_h + 2) * (kTW + 2) * 8 + (size_t)6 * layers * tile_h * kTW * 4;
+    return (size_t)layers * (tile_h + 2) * (kTW + 2) * 8 + (size_t)6 * layers * tile_h * kTW * 4 +
+           (size_t)layers * tile_h + (size_t)layers * kTW + (size_t)tile_h * kTW;
 }
 
 namespace {
-const void *relax_fn(uint32_t tile_h) {
+const void *relax_fn(uint32_t tile_h, uint32_t threads) {
+    const bool wide = threads >= 256;
     switch (tile_h) {
-        case 8: return (const void *)relax_rounds_kernel<1>;
-        case 16: return (const void *)relax_rounds_kernel<2>;
-        case 32: return (const void *)relax_rounds_kernel<4>;
-        default: return (const void *)relax_rounds_kernel<8>;
+        case 8: return wide ? (const void *)relax_rounds_kernel<8, 256> : (const void *)relax_rounds_kernel<8, 128>;
+        case 16: return wide ? (const void *)relax_rounds_kernel<16, 256> : (const void *)relax_rounds_kernel<16, 128>;
+        case 32: return wide ? (const void *)relax_rounds_kernel<32, 256> : (const void *)relax_rounds_kernel<32, 128>;
+        default: return wide ? (const void *)relax_rounds_kernel<64, 256> : (const void *)relax_rounds_kernel<64, 128>;
     }
 }
 }  // namespace
 
-cudaError_t relax_configure(uint32_t tile_h, size_t smem) {
-    return cudaFuncSetAttribute(relax_fn(tile_h), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem) {
+    return cudaFuncSetAttribute(relax_fn(tile_h, threads), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-cudaError_t relax_occupancy(uint32_t tile_h, size_t smem, int *blocks_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h), kRelaxThreads, smem);
+cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h, threads), (int)threads, smem);
 }
 
-cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, size_t smem, cudaStream_t st) {
+cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st) {
     RelaxArgs copy = a;
     void *args[] = {&copy};
-    return cudaLaunchCooperativeKernel(relax_fn(a.tile_h), dim3(grid), dim3(kRelaxThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel(relax_fn(a.tile_h, threads), dim3(grid), dim3(threads), args, smem, st);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {

@@ -152,6 +152,9 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_batch_window_cells": (C.c_uint64, [vp]),
             "mrc_batch_relax_ms": (C.c_float, [vp]),
             "mrc_batch_stats": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+            "mrc_batch_set_config": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32]),
+            "mrc_batch_autotune": (C.c_int, [vp, vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_float)]),
             "mrc_batch_destroy": (None, [vp]),
             "mrc_net_windows": (C.c_int, [u32, u32, u32, vp, u32, vp]),
         }
@@ -315,6 +318,18 @@ class Batch:
     @property
     def kernel_launches(self) -> int:
         return int(self.engine.lib.mrc_batch_kernel_launches(self.handle))
+
+    def set_config(self, tile_h: int, threads: int) -> None:
+        """Force the relax kernel's tile height and CTA width for this batch."""
+        e = self.engine
+        e._check(e.lib.mrc_batch_set_config(e.ctx, self.handle, int(tile_h), int(threads)))
+
+    def autotune(self) -> dict:
+        """Time every relax configuration on this batch and keep the fastest."""
+        th, nt, ms = C.c_uint32(), C.c_uint32(), C.c_float()
+        e = self.engine
+        e._check(e.lib.mrc_batch_autotune(e.ctx, self.handle, C.byref(th), C.byref(nt), C.byref(ms)))
+        return {"tile_h": int(th.value), "threads": int(nt.value), "ms": float(ms.value)}
 
     def stats(self) -> dict:
         """Work counters of the last launch: tile activations, in-tile sweeps,

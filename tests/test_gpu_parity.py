@@ -224,6 +224,12 @@ def test_deterministic_across_calls_and_batches(engine):
         c = batch.finish()
         assert c.paths == a.paths and c.search_costs == a.search_costs
     assert batch.kernel_launches == 3
+    # every tile height / CTA width the autotuner tries computes the same answer
+    tuned = batch.autotune()
+    assert tuned["tile_h"] in (8, 16, 32, 64) and tuned["threads"] in (128, 256)
+    batch.launch()
+    c = batch.finish()
+    assert c.paths == a.paths and c.search_costs == a.search_costs
 
 
 def test_edge_cases_and_errors(engine):
@@ -261,3 +267,23 @@ def test_edge_cases_and_errors(engine):
     prov = mrcuda.CudaIsolatedProvider(engine)
     paths = prov.route_isolated_batch(IsolatedRouteRequest(grid, nets, wins, x, y, []))
     assert paths[0] == [7] and paths[1] is not None
+
+
+@pytest.mark.parametrize("tile_cfg", [(8, 128), (8, 256), (16, 128), (16, 256), (32, 128), (32, 256), (64, 128),
+                                      (64, 256)])
+def test_every_relax_configuration_is_bit_exact(engine, oracle, tile_cfg):
+    """The autotuner may pick any tile height / CTA width: each must reproduce the oracle."""
+    rng = np.random.default_rng(sum(tile_cfg))
+    for trial in range(6):
+        req = _random_case(rng, trial, directed=trial % 2 == 1, max_side=90, max_layers=3)
+        if req is None:
+            continue
+        exp = oracle.isolated_batch(req, retry_full=False, mode="field")
+        board = engine.board(req.grid, req.x_edge_costs, req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+        batch = mrcuda.Batch(board, req.nets, req.windows, retry_full=False)
+        batch.set_config(*tile_cfg)
+        batch.launch()
+        got = batch.finish()
+        assert (got.paths, got.search_costs) == exp, (tile_cfg, trial)
+        batch.close()
+        board.close()
