@@ -4,8 +4,12 @@
 Workload (default): the congestion board — 512x512x4, 256 nets, directed edge
 prices, exact polygon outline, windows by net_window — one "step" routes every
 net of the batch (complete u32 fields over every window + canonical paths).
+`--workload plain` is the 128x128x2 board with 64 nets and whole-board fields;
+`--workload uneven` is 4096 independent one-net instances of log-normal size
+and 2-8 layers, staged as one multi-board batch.  The launch sequence is
+replayed as a captured CUDA graph (`--no-graph` launches kernel by kernel).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload W]
 
 One JSON line on rank 0.  `value` is whole-job nets/s with the board and nets
 resident in HBM (device time from CUDA events on the launching stream, L2
@@ -58,11 +62,59 @@ def _traffic_per_launch(kernel_profile: str):
 def _workload(name: str, rank: int, nets: int = 0):
     from mrcuda import workloads as W
 
+    if name == "uneven":
+        s = W.uneven_instances(seed=3 + 1000 * rank, n_instances=nets or 4096)
+        return Job(s.instances, s.meta)
     if name == "plain":
         wl = W.plain_board(seed=1 + 1000 * rank)
     else:
         wl = W.congestion_board(seed=2, net_seed=None if rank == 0 else 2 + 1000 * rank)
-    return W.scaled(wl, nets) if nets else wl
+    wl = W.scaled(wl, nets) if nets else wl
+    return Job([wl], wl.meta)
+
+
+class Job:
+    """One bench step's work: the nets of one or more boards (instances),
+    staged as one batch; net i belongs to boards[net_board[i]]."""
+
+    def __init__(self, boards, meta):
+        self.boards = boards
+        self.meta = meta
+        self.nets, self.windows, self.net_board = [], [], []
+        for k, wl in enumerate(boards):
+            self.nets += wl.nets
+            self.windows += wl.windows
+            self.net_board += [k] * len(wl.nets)
+
+    def window_cells(self) -> int:
+        return sum(wl.window_cells() for wl in self.boards)
+
+    def algorithmic_bytes(self) -> int:
+        return sum(wl.window_cells() * wl.bytes_per_cell() for wl in self.boards)
+
+    def bytes_per_cell(self) -> float:
+        return self.algorithmic_bytes() / max(self.window_cells(), 1)
+
+    def requests(self):
+        return [wl.request() for wl in self.boards]
+
+    def route(self, eng):
+        """The public host-buffer call: one request, or many instances."""
+        if len(self.boards) == 1:
+            return eng.route_isolated_batch(self.boards[0].request()).paths
+        return [p for r in eng.route_instances(self.requests()) for p in r.paths]
+
+    def h2d_bytes(self) -> int:
+        b = 0
+        for wl in self.boards:
+            g = wl.grid
+            b += (g.cost.nbytes + (g.board_constraint.nbytes if g.board_constraint is not None else 0)
+                  + (g.via_forbidden.nbytes if g.via_forbidden is not None else 0)
+                  + (wl.directed.nbytes if wl.directed is not None else 0)
+                  + 4 * (len(wl.x) + len(wl.y) + len(wl.vias)) + len(wl.vias) + 40 * len(wl.nets)
+                  + 16 * len(wl.windows) + 4 * sum(len(nt.passable_pads) + len(nt.via_passable_pads)
+                                                   for nt in wl.nets))
+        return b
 
 
 class ClockSampler:
@@ -112,7 +164,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _cpu_sample_rate(wl, n_sample: int, threads: int = 0):
+def _cpu_sample_rate(job, n_sample: int, threads: int = 0):
     """The oracle's A* alone-path search (window, then full board) on a sample of
     nets, all host threads: nets/s.  Checker code only; never the measured GPU path."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -120,13 +172,28 @@ def _cpu_sample_rate(wl, n_sample: int, threads: int = 0):
     from mrcuda.types import IsolatedRouteRequest
 
     o = orc.get()
-    req = wl.request()
-    sub = IsolatedRouteRequest(req.grid, req.nets[:n_sample], req.windows[:n_sample], req.x_edge_costs,
-                               req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+    if len(job.boards) == 1:
+        req = job.boards[0].request()
+        sub = IsolatedRouteRequest(req.grid, req.nets[:n_sample], req.windows[:n_sample], req.x_edge_costs,
+                                   req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+        t0 = time.perf_counter()
+        o.isolated_batch(sub, retry_full=True, mode="astar", threads=threads)
+        dt = time.perf_counter() - t0
+        return n_sample / dt, dt
+    # instances: one search per instance, spread over the host threads
+    from concurrent.futures import ThreadPoolExecutor
+
+    reqs = []
+    for wl in job.boards:
+        if len(reqs) >= n_sample:
+            break
+        reqs.append(wl.request())
+    n = sum(len(r.nets) for r in reqs)
     t0 = time.perf_counter()
-    o.isolated_batch(sub, retry_full=True, mode="astar", threads=threads)
+    with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+        list(ex.map(lambda r: o.isolated_batch(r, retry_full=True, mode="astar", threads=1), reqs))
     dt = time.perf_counter() - t0
-    return n_sample / dt, dt
+    return n / dt, dt
 
 
 def run_reference(args):
@@ -135,7 +202,7 @@ def run_reference(args):
         return 0
     wl = _workload(args.workload, 0, args.nets)
     cores = os.cpu_count() or 1
-    n_sample = min(args.cpu_sample, len(wl.nets))
+    n_sample = min(args.cpu_sample or (2048 if len(wl.boards) > 1 else 128), len(wl.nets))
     for _ in range(args.warmup):
         _cpu_sample_rate(wl, max(n_sample // 4, 1))
     rates = []
@@ -149,7 +216,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": wl.meta["workload"], "windows": wl.meta.get("windows")},
+        "config": {"workload": wl.meta["workload"], "windows": wl.meta.get("windows"), "nets": len(wl.nets)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{n_sample} of {len(wl.nets)} nets per step: A* alone-path search "
                                    f"(window, then full board), {cores} host threads"},
@@ -180,9 +247,15 @@ def run_engine(args):
 
     wl = _workload(args.workload, rank, args.nets)
     eng = mrcuda.Engine(local)
-    board = eng.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
-    batch = mrcuda.Batch(board, wl.nets, wl.windows, retry_full=True, time_kernels=True)
-    tuned = batch.autotune() if not args.no_autotune else None  # setup, outside the timed region
+    boards = [eng.board(b.grid, b.x, b.y, b.vias, b.directed) for b in wl.boards]
+    if len(boards) == 1:
+        batch = mrcuda.Batch(boards[0], wl.nets, wl.windows, retry_full=True, time_kernels=True)
+    else:
+        batch = mrcuda.Batch(boards, wl.nets, wl.windows, retry_full=True, time_kernels=True, net_board=wl.net_board)
+    # setup, outside the timed region: tile autotune, then capture the launch sequence as a graph
+    tuned = batch.autotune() if not args.no_autotune else None
+    if not args.no_graph:
+        batch.capture_graph()
     stream = torch.cuda.Stream()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
@@ -226,29 +299,25 @@ def run_engine(args):
     value = len(wl.nets) * world / (ms_max / 1000.0)
 
     # end to end through the public call with host buffers
-    req = wl.request()
     e2e_steps = max(1, min(args.steps, 5))
-    eng.route_isolated_batch(req)
+    wl.route(eng)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        out = eng.route_isolated_batch(req)
+        out_paths = wl.route(eng)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = len(wl.nets) * world / float(e2e_t.item())
-    h2d = (wl.grid.cost.nbytes + (wl.grid.board_constraint.nbytes if wl.grid.board_constraint is not None else 0)
-           + (wl.directed.nbytes if wl.directed is not None else 0) + 4 * (len(wl.x) + len(wl.y) + len(wl.vias))
-           + len(wl.vias) + 40 * len(wl.nets) + 16 * len(wl.windows)
-           + 4 * sum(len(nt.passable_pads) + len(nt.via_passable_pads) for nt in wl.nets))
-    d2h = 8 * (len(wl.nets) + 1) + 4 * len(wl.nets) + 4 * sum(len(p) for p in out.paths if p) + 4
-    assert out.paths == first.paths, "end-to-end call disagrees with the resident batch"
+    h2d = wl.h2d_bytes()
+    d2h = 8 * (len(wl.nets) + 1) + 4 * len(wl.nets) + 4 * sum(len(p) for p in out_paths if p) + 4
+    assert out_paths == first.paths, "end-to-end call disagrees with the resident batch"
 
-    # roofline of the dominant kernel (relax_tiles_kernel)
+    # roofline of the dominant kernel (relax_rounds_kernel)
     peak, peak_kind = _peaks()
-    alg_bytes = wl.window_cells() * wl.bytes_per_cell() + 4 * path_cells
+    alg_bytes = wl.algorithmic_bytes() + 4 * path_cells
     relax_avg = statistics.fmean(relax_ms) if relax_ms and min(relax_ms) > 0 else ms
     achieved = alg_bytes / (relax_avg / 1000.0) / 1e9
     traffic = _traffic_per_launch(f"relax_rounds_{args.workload}.md")
@@ -259,29 +328,34 @@ def run_engine(args):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl.meta["workload"], "nets_per_rank": len(wl.nets), "window_cells": wl.window_cells(),
                    "routed": routed, "retried": first.retried, "l2": "flushed between steps (512 MiB write)",
-                   "windows": wl.meta.get("windows"), "autotuned": tuned},
+                   "windows": wl.meta.get("windows"), "autotuned": tuned, "graph": not args.no_graph,
+                   "instances": len(wl.boards)},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": batch.kernel_launches * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "relax_rounds_kernel",
                      "kernel_ms": relax_avg, "algorithmic_bytes_per_launch": int(alg_bytes),
-                     "bytes_per_cell": wl.bytes_per_cell(), "tile_activations": work["activations"],
+                     "bytes_per_cell": round(wl.bytes_per_cell(), 3), "tile_activations": work["activations"],
                      "in_tile_sweeps": work["sweeps"], "rounds": work["rounds"], "tiles": work["tiles"]},
         "clocks": clk,
     }
 
     if rank == 0 and world == 1 and not args.no_plain:
-        ps = min(args.plain_sample, len(wl.nets))
-        sub = mrcuda.IsolatedRouteRequest(req.grid, req.nets[:ps], req.windows[:ps], req.x_edge_costs,
-                                          req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+        ps = min(args.plain_sample or (64 if len(wl.boards) > 1 else 8), len(wl.nets))
         t0 = time.perf_counter()
-        pl = eng.route_isolated_plain(sub)
+        if len(wl.boards) == 1:
+            req = wl.boards[0].request()
+            sub = mrcuda.IsolatedRouteRequest(req.grid, req.nets[:ps], req.windows[:ps], req.x_edge_costs,
+                                              req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+            pl_paths = eng.route_isolated_plain(sub).paths
+        else:
+            pl_paths = [p for b in wl.boards[:ps] for p in eng.route_isolated_plain(b.request()).paths]
         dt = time.perf_counter() - t0
-        assert pl.paths == first.paths[:ps], "plain form disagrees with the batched engine"
+        assert pl_paths == first.paths[:ps], "plain form disagrees with the batched engine"
         line["plain"] = {"value": ps / dt, "unit": UNIT, "sample": f"first {ps} nets, one net per launch sequence"}
         line["vs_plain"] = value / (ps / dt)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        n_sample = min(args.cpu_sample, len(wl.nets))
+        n_sample = min(args.cpu_sample or (2048 if len(wl.boards) > 1 else 128), len(wl.nets))
         rate, dt = _cpu_sample_rate(wl, n_sample)
         cores = os.cpu_count() or 1
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
@@ -290,7 +364,8 @@ def run_engine(args):
     if rank == 0:
         print(json.dumps(line))
     batch.close()
-    board.close()
+    for b in boards:
+        b.close()
     eng.close()
     if dist:
         dist.destroy_process_group()
@@ -303,10 +378,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["congestion", "plain"], default="congestion")
+    ap.add_argument("--workload", choices=["congestion", "plain", "uneven"], default="congestion")
     ap.add_argument("--nets", type=int, default=0, help="route only the first N nets (0 = all)")
-    ap.add_argument("--cpu-sample", type=int, default=128)
-    ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--cpu-sample", type=int, default=0, help="nets timed on the CPU (0 = workload default)")
+    ap.add_argument("--plain-sample", type=int, default=0, help="nets timed one per launch (0 = workload default)")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of a CUDA graph")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")

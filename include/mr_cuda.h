@@ -151,6 +151,13 @@ mrc_status mrc_route_lee(mrc_context *ctx, const mrc_grid *grid, const mrc_net *
 mrc_status mrc_distance_fields(mrc_context *ctx, const mrc_grid *grid, const uint32_t *sources, uint32_t n_sources,
                                uint32_t *fields);
 
+/* Many independent instances (each its own board, nets and windows; layer
+ * counts may differ) solved in ONE persistent launch.  Results are concatenated
+ * in instance order: the nets of instance k follow those of instance k-1.  The
+ * retry, when flagged, re-solves a net on its own instance's full board. */
+mrc_status mrc_route_instances(mrc_context *ctx, const mrc_isolated_request *instances, uint32_t n_instances,
+                               uint32_t flags, mrc_result **out);
+
 /* ---- results ---------------------------------------------------------------- */
 
 uint32_t mrc_result_count(const mrc_result *r);
@@ -180,6 +187,13 @@ void mrc_board_destroy(mrc_board *board);
  * net_window (negotiated.rs:568-594). */
 mrc_status mrc_batch_create(mrc_context *ctx, const mrc_board *board, const mrc_net *nets, uint32_t n_nets,
                             const mrc_window *windows, uint32_t flags, mrc_batch **out);
+/* A batch over several resident boards: net i belongs to boards[net_board[i]]. */
+mrc_status mrc_batch_create_multi(mrc_context *ctx, const mrc_board *const *boards, uint32_t n_boards,
+                                  const mrc_net *nets, const uint32_t *net_board, uint32_t n_nets,
+                                  const mrc_window *windows, uint32_t flags, mrc_batch **out);
+/* Capture the batch's launch sequence (resets, relax, path kernels) into a CUDA
+ * graph; later mrc_batch_launch calls replay it with one cudaGraphLaunch. */
+mrc_status mrc_batch_capture_graph(mrc_context *ctx, mrc_batch *batch);
 /* Enqueue the whole window solve (fields + canonical paths) on `stream`
  * (a cudaStream_t, NULL = the context's stream) without any host sync. */
 mrc_status mrc_batch_launch(mrc_context *ctx, mrc_batch *batch, void *stream);

@@ -58,6 +58,8 @@ struct DevField {
     uint32_t vpad_off, n_vpads; // sorted via exemptions in the pad arena
     uint32_t out;               // output slot (the net's request index)
     uint32_t tile_off;          // first tile of this field in the tile-state arrays
+    uint32_t board;             // index of this field's board in the batch's board array
+    uint32_t pad_;
 };
 
 // Control block of one batch launch (device memory, zeroed before launch).

@@ -161,6 +161,7 @@ mrc_status view_grid(const mrc_grid *g, GridView *v) {
 struct NetCopy {
     uint32_t src, dst;
     std::vector<uint32_t> pads, vpads;  // sorted, unique
+    uint32_t board = 0;                 // index into the batch's boards
 };
 
 bool sorted_contains(const std::vector<uint32_t> &v, uint32_t c) { return std::binary_search(v.begin(), v.end(), c); }
@@ -326,6 +327,91 @@ mrc_status board_build(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *
 
 }  // namespace
 
+namespace {
+
+// Boards of many instances uploaded with one copy: each board's device arrays
+// are 256-byte-aligned slices of one pool block.  The boards keep no host copy;
+// their views point at the caller's arrays for the duration of the call.
+struct BoardPack {
+    DBuf data;
+    std::vector<std::unique_ptr<mrc_board>> boards;
+};
+
+mrc_status board_pack_build(mrc_context *ctx, const mrc_isolated_request *inst, uint32_t n, BoardPack *pk) {
+    struct Off {
+        size_t cost, flags, x, y, via, dir;
+    };
+    std::vector<Off> offs(n);
+    size_t total = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = total;
+        total += (std::max<size_t>(bytes, 4) + 255) & ~(size_t)255;
+        return o;
+    };
+    pk->boards.clear();
+    for (uint32_t k = 0; k < n; ++k) {
+        std::unique_ptr<mrc_board> b(new mrc_board());
+        MRC_TRY(view_grid(inst[k].grid, &b->view));
+        const GridView &g = b->view;
+        const mrc_edges &e = inst[k].edges;
+        const uint32_t ex = g.w ? g.w - 1 : 0, ey = g.h ? g.h - 1 : 0, ev = g.layers - 1;
+        if (e.n_x_edge_costs != ex || e.n_y_edge_costs != ey || e.n_via_edge_costs != ev)
+            return fail(MRC_ERR_INVALID_ARGUMENT, "instance " + std::to_string(k) + ": edge vectors do not match its grid");
+        if ((ex && !e.x_edge_costs) || (ey && !e.y_edge_costs) || (ev && (!e.via_edge_costs || !e.via_allowed)))
+            return fail(MRC_ERR_INVALID_ARGUMENT, "instance " + std::to_string(k) + ": edge price pointer is NULL");
+        b->ctx = ctx;
+        b->directed = e.directed_in_costs != nullptr;
+        Off &o = offs[k];
+        o.cost = take(g.n * 4);
+        o.flags = (g.board || g.via_forbidden) ? take(g.n) : SIZE_MAX;
+        o.x = take((size_t)ex * 4);
+        o.y = take((size_t)ey * 4);
+        o.via = take((size_t)std::max(ev, 1u) * 4);
+        o.dir = b->directed ? take(g.n * 16) : SIZE_MAX;
+        pk->boards.push_back(std::move(b));
+    }
+    std::vector<uint8_t> host(total);
+    for (uint32_t k = 0; k < n; ++k) {
+        const GridView &g = pk->boards[k]->view;
+        const mrc_edges &e = inst[k].edges;
+        const Off &o = offs[k];
+        std::memcpy(host.data() + o.cost, g.cost, g.n * 4);
+        if (o.flags != SIZE_MAX) {
+            uint8_t *fl = host.data() + o.flags;
+            for (uint64_t i = 0; i < g.n; ++i)
+                fl[i] = (uint8_t)((g.board ? g.board[i] : 0) | (g.via_forbidden && g.via_forbidden[i] ? kStaticVia : 0));
+        }
+        if (e.n_x_edge_costs) std::memcpy(host.data() + o.x, e.x_edge_costs, (size_t)e.n_x_edge_costs * 4);
+        if (e.n_y_edge_costs) std::memcpy(host.data() + o.y, e.y_edge_costs, (size_t)e.n_y_edge_costs * 4);
+        uint32_t *via = reinterpret_cast<uint32_t *>(host.data() + o.via);
+        uint32_t mask = 0;
+        for (uint32_t i = 0; i < e.n_via_edge_costs; ++i) {
+            via[i] = e.via_edge_costs[i];
+            if (e.via_allowed[i]) mask |= 1u << i;
+        }
+        if (o.dir != SIZE_MAX) std::memcpy(host.data() + o.dir, e.directed_in_costs, g.n * 16);
+        pk->boards[k]->dev.via_mask = mask;
+    }
+    MRC_TRY(upload(ctx, pk->data, host.data(), host.size(), "upload instance boards"));
+    unsigned char *base = pk->data.as<unsigned char>();
+    for (uint32_t k = 0; k < n; ++k) {
+        mrc_board &b = *pk->boards[k];
+        const Off &o = offs[k];
+        b.dev.w = b.view.w;
+        b.dev.h = b.view.h;
+        b.dev.layers = b.view.layers;
+        b.dev.cost = reinterpret_cast<const uint32_t *>(base + o.cost);
+        b.dev.flags = o.flags != SIZE_MAX ? base + o.flags : nullptr;
+        b.dev.x_edge = reinterpret_cast<const uint32_t *>(base + o.x);
+        b.dev.y_edge = reinterpret_cast<const uint32_t *>(base + o.y);
+        b.dev.via_edge = reinterpret_cast<const uint32_t *>(base + o.via);
+        b.dev.directed = o.dir != SIZE_MAX ? reinterpret_cast<const uint4 *>(base + o.dir) : nullptr;
+    }
+    return MRC_OK;
+}
+
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // Results
 
@@ -346,7 +432,9 @@ struct mrc_result {
 
 struct mrc_batch {
     mrc_context *ctx = nullptr;
-    const mrc_board *board = nullptr;
+    std::vector<const mrc_board *> boards;  // a batch may span many boards
+    uint32_t max_layers = 1;
+    bool directed_any = false;
     uint32_t flags = 0;
     std::vector<NetCopy> nets;
     std::vector<mrc_window> windows;
@@ -354,18 +442,20 @@ struct mrc_batch {
     uint64_t total_cells = 0;
     uint32_t total_tiles = 0, max_tiles = 0, tile_h = 32, threads = kRelaxThreads, grid = 1;
     size_t smem = 0;
-    DBuf d_fields, d_pads, d_lab, d_tstamp, d_tvisit, d_lists, d_costs, d_lens, d_offsets, d_cells, d_ctl, d_out;
+    DBuf d_boards, d_fields, d_pads, d_lab, d_tstamp, d_tvisit, d_lists, d_costs, d_lens, d_offsets, d_cells, d_ctl,
+        d_out;
     uint32_t launches = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t graph = nullptr;  // captured launch sequence (mrc_batch_capture_graph)
     ~mrc_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
 };
 
 namespace {
-
 
 // Tile height: every row and column pass keeps 4*L*TH lanes busy, so prefer
 // L*TH = 64 (all 256 threads), then the tallest tile that still fits three CTAs
@@ -392,10 +482,13 @@ uint32_t tune_key(uint32_t layers, bool directed) { return layers * 2u + (direct
 // per-tile buffers.  Re-run by the autotuner for every candidate.
 mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     mrc_context *ctx = bt->ctx;
-    const mrc_board *board = bt->board;
+    if (bt->graph) {  // a captured graph bakes in the old layout
+        cudaGraphExecDestroy(bt->graph);
+        bt->graph = nullptr;
+    }
     bt->tile_h = tile_h;
     bt->threads = threads;
-    bt->smem = relax_smem_bytes(board->view.layers, tile_h, board->directed);
+    bt->smem = relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any);
     uint64_t toff = 0;
     uint32_t max_tiles = 1;
     for (DevField &f : bt->fields) {
@@ -420,30 +513,35 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     return MRC_OK;
 }
 
-mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> nets,
+mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, std::vector<NetCopy> nets,
                        std::vector<mrc_window> windows, uint32_t flags, mrc_batch *bt) {
-    const GridView &g = board->view;
     bt->ctx = ctx;
-    bt->board = board;
+    bt->boards = std::move(boards);
     bt->flags = flags;
     bt->nets = std::move(nets);
     bt->windows = std::move(windows);
+    bt->max_layers = 1;
+    bt->directed_any = false;
+    for (const mrc_board *b : bt->boards) {
+        bt->max_layers = std::max(bt->max_layers, b->view.layers);
+        bt->directed_any = bt->directed_any || b->directed;
+    }
     const uint32_t n = (uint32_t)bt->nets.size();
     uint32_t tile_h = 0, threads = kRelaxThreads;
     size_t smem = 0;
-    auto tuned = ctx->tuned.find(tune_key(g.layers, board->directed));
+    auto tuned = ctx->tuned.find(tune_key(bt->max_layers, bt->directed_any));
     if (tuned != ctx->tuned.end()) {
         tile_h = tuned->second.first;
         threads = tuned->second.second;
     } else {
-        MRC_TRY(choose_tile(ctx, g.layers, board->directed, &tile_h, &smem));
+        MRC_TRY(choose_tile(ctx, bt->max_layers, bt->directed_any, &tile_h, &smem));
     }
     // largest windows first: the persistent CTAs then finish together
     std::vector<uint32_t> order(n);
     std::iota(order.begin(), order.end(), 0u);
     auto cells_of = [&](uint32_t i) {
         const mrc_window &w = bt->windows[i];
-        return (uint64_t)(w.x1 - w.x0 + 1) * (w.y1 - w.y0 + 1) * g.layers;
+        return (uint64_t)(w.x1 - w.x0 + 1) * (w.y1 - w.y0 + 1) * bt->boards[bt->nets[i].board]->view.layers;
     };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cells_of(a) > cells_of(b); });
     std::vector<uint32_t> pads;
@@ -470,9 +568,15 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
         pads.insert(pads.end(), nc.vpads.begin(), nc.vpads.end());
         f.out = i;
         f.tile_off = 0;
+        f.board = nc.board;
+        f.pad_ = 0;
         if (pads.size() > 0xFFFFFFF0u) return fail(MRC_ERR_LIMIT, "pad lists exceed 2^32 entries");
     }
     bt->total_cells = off;
+    std::vector<DevBoard> devs;
+    devs.reserve(bt->boards.size());
+    for (const mrc_board *b : bt->boards) devs.push_back(b->dev);
+    MRC_TRY(upload(ctx, bt->d_boards, devs.data(), devs.size() * sizeof(DevBoard), "upload board table"));
     MRC_TRY(batch_layout(bt, tile_h, threads));
     MRC_TRY(upload(ctx, bt->d_pads, pads.data(), pads.size() * 4, "upload pads"));
     MRC_TRY(bt->d_lab.get(ctx, std::max<uint64_t>(off, 1) * 8, "labels"));
@@ -491,7 +595,7 @@ mrc_status batch_build(mrc_context *ctx, const mrc_board *board, std::vector<Net
 
 PathArgs path_args(const mrc_batch *bt) {
     PathArgs pa;
-    pa.board = bt->board->dev;
+    pa.boards = bt->d_boards.as<DevBoard>();
     pa.fields = bt->d_fields.as<DevField>();
     pa.n_fields = (uint32_t)bt->fields.size();
     pa.pads = bt->d_pads.as<uint32_t>();
@@ -506,15 +610,18 @@ PathArgs path_args(const mrc_batch *bt) {
     return pa;
 }
 
-mrc_status batch_launch(mrc_batch *bt, cudaStream_t st) {
+// The launch sequence of one batch: reset, relax, paths (+ fields).
+// Under stream capture the events become event-record nodes of the graph, so a
+// replay still times the relax kernel alone.
+mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
     const uint32_t n = (uint32_t)bt->fields.size();
-    bt->stream = st;
-    bt->launches = 0;
+    uint32_t launches = 0;
     MRC_CUDA(cudaMemsetAsync(bt->d_ctl.p, 0, sizeof(Ctl), st), "reset control block");
     MRC_CUDA(cudaMemsetAsync(bt->d_tstamp.p, 0, (size_t)bt->total_tiles * 4, st), "reset tile stamps");
     MRC_CUDA(cudaMemsetAsync(bt->d_tvisit.p, 0, (size_t)bt->total_tiles * 4, st), "reset tile flags");
     RelaxArgs ra;
-    ra.board = bt->board->dev;
+    ra.boards = bt->d_boards.as<DevBoard>();
+    ra.max_layers = bt->max_layers;
     ra.fields = bt->d_fields.as<DevField>();
     ra.n_fields = n;
     ra.pads = bt->d_pads.as<uint32_t>();
@@ -527,19 +634,30 @@ mrc_status batch_launch(mrc_batch *bt, cudaStream_t st) {
     ra.tile_h = bt->tile_h;
     ra.round_limit = 64u * bt->max_tiles + 4096u;
     if (n) {
-        if (bt->ev0) MRC_CUDA(cudaEventRecord(bt->ev0, st), "record event");
+        const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+        if (bt->ev0) MRC_CUDA(cudaEventRecordWithFlags(bt->ev0, st, rec), "record event");
         MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st), "launch relax kernel");
-        if (bt->ev1) MRC_CUDA(cudaEventRecord(bt->ev1, st), "record event");
-        bt->launches++;
+        if (bt->ev1) MRC_CUDA(cudaEventRecordWithFlags(bt->ev1, st, rec), "record event");
+        launches++;
     }
     const PathArgs pa = path_args(bt);
     MRC_CUDA(path_launch(pa, st), "launch path kernels");
-    bt->launches += n ? 2 : 1;
+    launches += n ? 2 : 1;
     if (bt->d_out.p && n) {
         MRC_CUDA(fields_launch(pa, bt->d_out.as<uint32_t>(), bt->total_cells, st), "launch field emit");
-        bt->launches++;
+        launches++;
     }
+    bt->launches = launches;
     return MRC_OK;
+}
+
+mrc_status batch_launch(mrc_batch *bt, cudaStream_t st) {
+    bt->stream = st;
+    if (bt->graph) {
+        MRC_CUDA(cudaGraphLaunch(bt->graph, st), "replay graph");
+        return MRC_OK;
+    }
+    return batch_enqueue(bt, st, false);
 }
 
 mrc_status status_error(uint32_t status) {
@@ -550,7 +668,7 @@ mrc_status status_error(uint32_t status) {
     return fail(MRC_ERR_BACKEND_UNAVAILABLE, "tile queue overflow");
 }
 
-// Copy one batch's outputs into `r` at the given result slots.
+// Copy one batch's outputs (indexed like bt->nets).
 mrc_status batch_collect(mrc_batch *bt, bool keep_fields, std::vector<uint32_t> *costs,
                          std::vector<std::vector<uint32_t>> *paths, std::vector<std::vector<uint32_t>> *fields) {
     cudaStream_t st = bt->stream;
@@ -573,25 +691,24 @@ mrc_status batch_collect(mrc_batch *bt, bool keep_fields, std::vector<uint32_t> 
         if (bt->total_cells && bt->d_out.p)
             MRC_CUDA(cudaMemcpy(all.data(), bt->d_out.p, bt->total_cells * 4, cudaMemcpyDeviceToHost), "read fields");
         for (const DevField &f : bt->fields) {
-            const uint64_t c = (uint64_t)f.ww * f.wh * bt->board->view.layers;
+            const uint64_t c = (uint64_t)f.ww * f.wh * bt->boards[f.board]->view.layers;
             (*fields)[f.out].assign(all.begin() + f.lab_off, all.begin() + f.lab_off + c);
         }
     }
     return MRC_OK;
 }
 
-// Run a batch synchronously and, with MRC_FLAG_RETRY_FULL, re-solve on the full
+// Run a batch synchronously and, with MRC_FLAG_RETRY_FULL, re-solve on its full
 // board every net whose window solve was unreachable (cli/src/lib.rs:574-607).
-mrc_status solve(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> nets, std::vector<mrc_window> wins,
-                 uint32_t flags, mrc_result **out, mrc_batch *prepared) {
-    const GridView &g = board->view;
+mrc_status solve(mrc_context *ctx, std::vector<const mrc_board *> boards, std::vector<NetCopy> nets,
+                 std::vector<mrc_window> wins, uint32_t flags, mrc_result **out, mrc_batch *prepared) {
     const bool keep = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
     std::unique_ptr<mrc_batch> own;
     mrc_batch *bt = prepared;
     if (!bt) {
         own.reset(new mrc_batch());
         bt = own.get();
-        MRC_TRY(batch_build(ctx, board, std::move(nets), std::move(wins), flags, bt));
+        MRC_TRY(batch_build(ctx, std::move(boards), std::move(nets), std::move(wins), flags, bt));
         MRC_TRY(batch_launch(bt, ctx->stream));
     }
     std::vector<uint32_t> costs;
@@ -603,17 +720,20 @@ mrc_status solve(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> 
     r->field_windows = bt->windows;
     if (flags & MRC_FLAG_RETRY_FULL) {
         std::vector<uint32_t> idx;
-        for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t i = 0; i < n; ++i) {
+            const GridView &g = bt->boards[bt->nets[i].board]->view;
             if (costs[i] == kMax && !is_full(bt->windows[i], g.w, g.h)) idx.push_back(i);
+        }
         if (!idx.empty()) {
             std::vector<NetCopy> rn;
             std::vector<mrc_window> rw;
             for (uint32_t i : idx) {
                 rn.push_back(bt->nets[i]);
+                const GridView &g = bt->boards[bt->nets[i].board]->view;
                 rw.push_back(full_window(g.w, g.h));
             }
             mrc_batch retry;
-            MRC_TRY(batch_build(ctx, board, std::move(rn), std::move(rw), flags, &retry));
+            MRC_TRY(batch_build(ctx, bt->boards, std::move(rn), std::move(rw), flags & ~MRC_FLAG_TIME_KERNELS, &retry));
             MRC_TRY(batch_launch(&retry, bt->stream ? bt->stream : ctx->stream));
             std::vector<uint32_t> c2;
             std::vector<std::vector<uint32_t>> p2, f2;
@@ -622,7 +742,7 @@ mrc_status solve(mrc_context *ctx, const mrc_board *board, std::vector<NetCopy> 
                 costs[idx[k]] = c2[k];
                 paths[idx[k]] = std::move(p2[k]);
                 if (keep) fields[idx[k]] = std::move(f2[k]);
-                r->field_windows[idx[k]] = full_window(g.w, g.h);
+                r->field_windows[idx[k]] = retry.windows[k];
             }
             r->retried = (uint32_t)idx.size();
         }
@@ -768,7 +888,7 @@ mrc_status mrc_route_isolated_batch(mrc_context *ctx, const mrc_isolated_request
         (*out)->field_offsets.assign(1, 0);
         return MRC_OK;
     }
-    return solve(ctx, &board, std::move(nets), std::move(wins), flags, out, nullptr);
+    return solve(ctx, {&board}, std::move(nets), std::move(wins), flags, out, nullptr);
 }
 
 mrc_status mrc_route_lee(mrc_context *ctx, const mrc_grid *grid, const mrc_net *nets, uint32_t n_nets,
@@ -795,7 +915,7 @@ mrc_status mrc_route_lee(mrc_context *ctx, const mrc_grid *grid, const mrc_net *
         return MRC_OK;
     }
     std::vector<mrc_window> wins(nc.size(), full_window(g.w, g.h));
-    return solve(ctx, &board, std::move(nc), std::move(wins), 0, out, nullptr);
+    return solve(ctx, {&board}, std::move(nc), std::move(wins), 0, out, nullptr);
 }
 
 mrc_status mrc_distance_fields(mrc_context *ctx, const mrc_grid *grid, const uint32_t *sources, uint32_t n_sources,
@@ -828,11 +948,47 @@ mrc_status mrc_distance_fields(mrc_context *ctx, const mrc_grid *grid, const uin
     MRC_TRY(board_build(ctx, grid, &e, false, &board));
     std::vector<mrc_window> wins(nc.size(), full_window(g.w, g.h));
     mrc_result *r = nullptr;
-    MRC_TRY(solve(ctx, &board, std::move(nc), std::move(wins), MRC_FLAG_KEEP_FIELDS, &r, nullptr));
+    MRC_TRY(solve(ctx, {&board}, std::move(nc), std::move(wins), MRC_FLAG_KEEP_FIELDS, &r, nullptr));
     std::unique_ptr<mrc_result> hold(r);
     for (size_t k = 0; k < slot.size(); ++k)
         std::memcpy(fields + (size_t)slot[k] * g.n, r->fields.data() + r->field_offsets[k], (size_t)g.n * 4);
     return MRC_OK;
+}
+
+mrc_status mrc_route_instances(mrc_context *ctx, const mrc_isolated_request *instances, uint32_t n_instances,
+                               uint32_t flags, mrc_result **out) {
+    if (!ctx || !out || (n_instances && !instances)) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, flags);
+    if (lock.st != MRC_OK) return lock.st;
+    MRC_TRY(set_device(ctx));
+    std::vector<NetCopy> nets;
+    std::vector<mrc_window> wins;
+    for (uint32_t k = 0; k < n_instances; ++k) {
+        GridView g;
+        MRC_TRY(view_grid(instances[k].grid, &g));
+        if (instances[k].n_nets && !instances[k].windows)
+            return fail(MRC_ERR_INVALID_ARGUMENT, "instance " + std::to_string(k) + ": windows is NULL");
+        std::vector<NetCopy> nk;
+        MRC_TRY(validate_nets(g, instances[k].nets, instances[k].n_nets, &nk));
+        std::vector<mrc_window> wk;
+        MRC_TRY(collect_windows(g, nk, instances[k].windows, &wk));
+        for (NetCopy &c : nk) c.board = k;
+        nets.insert(nets.end(), std::make_move_iterator(nk.begin()), std::make_move_iterator(nk.end()));
+        wins.insert(wins.end(), wk.begin(), wk.end());
+    }
+    if (nets.empty()) {
+        *out = new mrc_result();
+        (*out)->offsets.assign(1, 0);
+        (*out)->has_fields = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
+        (*out)->field_offsets.assign(1, 0);
+        return MRC_OK;
+    }
+    BoardPack pk;
+    MRC_TRY(board_pack_build(ctx, instances, n_instances, &pk));
+    std::vector<const mrc_board *> boards;
+    for (auto &b : pk.boards) boards.push_back(b.get());
+    return solve(ctx, std::move(boards), std::move(nets), std::move(wins), flags, out, nullptr);
 }
 
 uint32_t mrc_result_count(const mrc_result *r) { return r ? r->n : 0; }
@@ -882,10 +1038,70 @@ mrc_status mrc_batch_create(mrc_context *ctx, const mrc_board *board, const mrc_
     std::vector<mrc_window> wins;
     MRC_TRY(collect_windows(board->view, nc, windows, &wins));
     std::unique_ptr<mrc_batch> bt(new mrc_batch());
-    MRC_TRY(batch_build(ctx, board, std::move(nc), std::move(wins), flags, bt.get()));
+    MRC_TRY(batch_build(ctx, {board}, std::move(nc), std::move(wins), flags, bt.get()));
     MRC_CUDA(cudaStreamSynchronize(ctx->stream), "stage batch");
     *out = bt.release();
     return MRC_OK;
+}
+
+mrc_status mrc_batch_create_multi(mrc_context *ctx, const mrc_board *const *boards, uint32_t n_boards,
+                                  const mrc_net *nets, const uint32_t *net_board, uint32_t n_nets,
+                                  const mrc_window *windows, uint32_t flags, mrc_batch **out) {
+    if (!ctx || !out || !boards || !n_boards || (n_nets && !net_board))
+        return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, flags);
+    if (lock.st != MRC_OK) return lock.st;
+    MRC_TRY(set_device(ctx));
+    std::vector<NetCopy> nc(n_nets);
+    std::vector<mrc_window> wins(n_nets);
+    for (uint32_t i = 0; i < n_nets; ++i) {
+        const uint32_t k = net_board[i];
+        if (k >= n_boards || !boards[k]) return fail(MRC_ERR_INVALID_ARGUMENT, "net board index out of range");
+        std::vector<NetCopy> one;
+        MRC_TRY(validate_nets(boards[k]->view, nets + i, 1, &one));
+        std::vector<mrc_window> w;
+        MRC_TRY(collect_windows(boards[k]->view, one, windows ? windows + i : nullptr, &w));
+        nc[i] = std::move(one[0]);
+        nc[i].board = k;
+        wins[i] = w[0];
+    }
+    std::unique_ptr<mrc_batch> bt(new mrc_batch());
+    MRC_TRY(batch_build(ctx, std::vector<const mrc_board *>(boards, boards + n_boards), std::move(nc), std::move(wins),
+                        flags, bt.get()));
+    MRC_CUDA(cudaStreamSynchronize(ctx->stream), "stage batch");
+    *out = bt.release();
+    return MRC_OK;
+}
+
+mrc_status mrc_batch_capture_graph(mrc_context *ctx, mrc_batch *batch) {
+    if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    if (batch->graph) {
+        cudaGraphExecDestroy(batch->graph);
+        batch->graph = nullptr;
+    }
+    cudaStream_t cs = nullptr;
+    MRC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    mrc_status rc = MRC_OK;
+    if (e == cudaSuccess) {
+        rc = batch_enqueue(batch, cs, true);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+        if (rc == MRC_OK && e2 != cudaSuccess) rc = fail(MRC_ERR_BACKEND_UNAVAILABLE, std::string("end capture: ") + cudaGetErrorString(e2));
+    } else {
+        rc = fail(MRC_ERR_BACKEND_UNAVAILABLE, std::string("begin capture: ") + cudaGetErrorString(e));
+    }
+    if (rc == MRC_OK) {
+        e = cudaGraphInstantiate(&batch->graph, g, 0);
+        if (e != cudaSuccess) rc = fail(MRC_ERR_BACKEND_UNAVAILABLE, std::string("instantiate graph: ") + cudaGetErrorString(e));
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    (void)cudaGetLastError();
+    return rc;
 }
 
 mrc_status mrc_batch_launch(mrc_context *ctx, mrc_batch *batch, void *stream) {
@@ -901,7 +1117,7 @@ mrc_status mrc_batch_finish(mrc_context *ctx, mrc_batch *batch, mrc_result **out
     Lock lock(ctx, 0);
     MRC_TRY(set_device(ctx));
     if (!batch->stream) return fail(MRC_ERR_INVALID_ARGUMENT, "batch was never launched");
-    return solve(ctx, batch->board, {}, {}, batch->flags, out, batch);
+    return solve(ctx, batch->boards, {}, {}, batch->flags, out, batch);
 }
 
 mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile_h, uint32_t *threads,
@@ -909,7 +1125,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
     Lock lock(ctx, 0);
     MRC_TRY(set_device(ctx));
-    const uint32_t layers = batch->board->view.layers;
+    const uint32_t layers = batch->max_layers;
     const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     MRC_CUDA(cudaEventCreate(&e0), "create event");
@@ -918,7 +1134,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     uint32_t best_th = batch->tile_h, best_nt = batch->threads;
     mrc_status rc = MRC_OK;
     for (uint32_t th : {8u, 16u, 32u, 64u}) {
-        if (relax_smem_bytes(layers, th, batch->board->directed) > hard) continue;
+        if (relax_smem_bytes(layers, th, batch->directed_any) > hard) continue;
         for (uint32_t nt : {128u, 256u}) {
             if (4u * layers * th < nt / 2) continue;  // most lanes would idle in the line passes
             rc = batch_layout(batch, th, nt);
@@ -945,7 +1161,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     cudaEventDestroy(e1);
     if (rc != MRC_OK) return rc;
     MRC_TRY(batch_layout(batch, best_th, best_nt));
-    ctx->tuned[tune_key(layers, batch->board->directed)] = {best_th, best_nt};
+    ctx->tuned[tune_key(layers, batch->directed_any)] = {best_th, best_nt};
     if (tile_h) *tile_h = best_th;
     if (threads) *threads = best_nt;
     if (best_ms) *best_ms = best;
@@ -959,7 +1175,7 @@ mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t til
     Lock lock(ctx, 0);
     MRC_TRY(set_device(ctx));
     const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
-    if (relax_smem_bytes(batch->board->view.layers, tile_h, batch->board->directed) > hard)
+    if (relax_smem_bytes(batch->max_layers, tile_h, batch->directed_any) > hard)
         return fail(MRC_ERR_LIMIT, "tile does not fit in shared memory");
     return batch_layout(batch, tile_h, threads);
 }
@@ -1031,7 +1247,8 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + kPlainTileH - 1) / kPlainTileH);
     std::vector<uint32_t> pads(net.pads);
     pads.insert(pads.end(), net.vpads.begin(), net.vpads.end());
-    DBuf d_pads, d_a, d_b, d_ctl, d_field, d_costs, d_lens, d_off, d_cells, d_vis, d_out;
+    DBuf d_pads, d_a, d_b, d_ctl, d_field, d_costs, d_lens, d_off, d_cells, d_vis, d_out, d_board;
+    MRC_TRY(upload(ctx, d_board, &board->dev, sizeof(DevBoard), "plain board"));
     MRC_TRY(upload(ctx, d_pads, pads.data(), pads.size() * 4, "plain pads"));
     MRC_TRY(upload(ctx, d_field, &f, sizeof(f), "plain field"));
     MRC_TRY(d_a.get(ctx, wc * 8, "plain labels"));
@@ -1074,7 +1291,7 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     MRC_TRY(d_off.get(ctx, 16, "plain offsets"));
     MRC_TRY(d_cells.get(ctx, wc * 4, "plain path"));
     PathArgs pt;
-    pt.board = board->dev;
+    pt.boards = d_board.as<DevBoard>();
     pt.fields = d_field.as<DevField>();
     pt.n_fields = 1;
     pt.pads = d_pads.as<uint32_t>();
@@ -1282,6 +1499,8 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
         f.out = i;
         const uint64_t t = (uint64_t)((f.ww + 31) / 32) * ((f.wh + tile_h - 1) / tile_h);
         f.tile_off = (uint32_t)std::min<uint64_t>(tiles, 0xFFFFFFFFull);
+        f.board = 0;
+        f.pad_ = 0;
         tiles += t;
         max_tiles = (uint32_t)std::max<uint64_t>(max_tiles, t);
     }
@@ -1290,6 +1509,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     const bool has_flags = g.board || g.via_forbidden;
     Carve c;
     const size_t o_ctl = c.take(sizeof(Ctl)), o_fields = c.take(n * sizeof(DevField)), o_pads = c.take(pads.size() * 4);
+    const size_t o_btab = c.take(sizeof(DevBoard));
     const size_t o_cost = c.take(g.n * 4), o_flags = has_flags ? c.take(g.n) : 0;
     const size_t o_vf = g.via_forbidden ? c.take(g.n) : 0, o_dir = directed ? c.take(g.n * 16) : 0;
     const size_t o_x = c.take((size_t)ex * 4), o_y = c.take((size_t)ey * 4), o_via = c.take((size_t)std::max(ev, 1u) * 4);
@@ -1343,12 +1563,14 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     b.via_edge = reinterpret_cast<const uint32_t *>(s + o_via);
     b.directed = directed ? reinterpret_cast<const uint4 *>(s + o_dir) : nullptr;
 
+    MRC_CUDA(cudaMemcpyAsync(s + o_btab, &b, sizeof(DevBoard), cudaMemcpyHostToDevice, st), "upload board table");
     int per_sm = 0;
     MRC_CUDA(relax_configure(tile_h, kRelaxThreads, smem), "configure relax kernel");
     MRC_CUDA(relax_occupancy(tile_h, kRelaxThreads, smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     RelaxArgs ra;
-    ra.board = b;
+    ra.boards = reinterpret_cast<const DevBoard *>(s + o_btab);
+    ra.max_layers = g.layers;
     ra.fields = reinterpret_cast<const DevField *>(s + o_fields);
     ra.n_fields = n;
     ra.pads = reinterpret_cast<const uint32_t *>(s + o_pads);
@@ -1362,7 +1584,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     ra.round_limit = 64u * max_tiles + 4096u;
     MRC_CUDA(relax_launch(ra, (uint32_t)dev->sms * (uint32_t)per_sm, kRelaxThreads, smem, st), "launch relax kernel");
     PathArgs pa;
-    pa.board = b;
+    pa.boards = ra.boards;
     pa.fields = ra.fields;
     pa.n_fields = n;
     pa.pads = ra.pads;

@@ -20,7 +20,8 @@ constexpr uint32_t kStatusQueueOverflow = 1u << 3;
 constexpr uint32_t kStatusBarrier = 1u << 4;
 
 struct RelaxArgs {
-    DevBoard board;
+    const DevBoard *boards;     // device array, indexed by DevField::board
+    uint32_t max_layers;        // the largest layer count among the boards (sizes the tile)
     const DevField *fields;     // ascending lab_off
     uint32_t n_fields;
     const uint32_t *pads;       // sorted pad lists, indexed by DevField offsets
@@ -35,7 +36,7 @@ struct RelaxArgs {
 };
 
 struct PathArgs {
-    DevBoard board;
+    const DevBoard *boards;
     const DevField *fields;
     uint32_t n_fields;
     const uint32_t *pads;

@@ -300,17 +300,8 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
 template <int TH, int NT>
 __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const DevBoard b = a.board;
-    const uint32_t L = b.layers;
     const uint32_t SW = kTW + 2, SH = TH + 2;
-    const uint32_t nsm = L * SH * SW;
     Tile<TH> tile;
-    tile.lab = reinterpret_cast<u64 *>(smem_raw);
-    tile.st = reinterpret_cast<uint32_t *>(tile.lab + nsm);
-    tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kTW);
-    tile.cold = tile.rowd + L * TH;
-    tile.stackd = tile.cold + L * kTW;
-    tile.L = L;
     __shared__ u64 s_item;
     __shared__ uint32_t s_push[4];
     __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
@@ -322,6 +313,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
     // ---- round 0: every field's source tile ---------------------------------
     for (uint32_t fi = blockIdx.x * blockDim.x + tid; fi < a.n_fields; fi += gridDim.x * blockDim.x) {
         const DevField f = a.fields[fi];
+        const DevBoard b = a.boards[f.board];
         const uint32_t plane = b.w * b.h;
         const uint32_t sr = f.src % plane, sx = sr % b.w, sy = sr / b.w;
         const uint8_t sfl = b.flags ? b.flags[f.src] : 0;
@@ -360,6 +352,15 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             if (item == kInf) break;
             const uint32_t fi = (uint32_t)(item >> 32), t = (uint32_t)item;
             const DevField f = a.fields[fi];
+            const DevBoard b = a.boards[f.board];
+            const uint32_t L = b.layers;  // the shared tile is laid out for this board's layers
+            const uint32_t nsm = L * SH * SW;
+            tile.lab = reinterpret_cast<u64 *>(smem_raw);
+            tile.st = reinterpret_cast<uint32_t *>(tile.lab + nsm);
+            tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kTW);
+            tile.cold = tile.rowd + L * TH;
+            tile.stackd = tile.cold + L * kTW;
+            tile.L = L;
             const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
             const uint32_t txi = t % ntx, tyi = t / ntx;
             const int tx0 = (int)(f.x0 + txi * kTW), ty0 = (int)(f.y0 + tyi * TH);
@@ -565,19 +566,20 @@ __device__ __forceinline__ u64 field_label(const PathArgs &a, const DevField &f,
 __global__ void __launch_bounds__(1024) path_offsets_kernel(PathArgs a) {
     __shared__ unsigned long long warp_sums[32];
     __shared__ unsigned long long carry;
-    const uint32_t plane = a.board.w * a.board.h;
     // phase 1: cost and length of every field, stored at its output slot
     for (uint32_t i = threadIdx.x; i < a.n_fields; i += blockDim.x) {
         const DevField f = a.fields[i];
+        const DevBoard b = a.boards[f.board];
+        const uint32_t plane = b.w * b.h;
         const uint32_t dl = f.dst / plane, dr = f.dst % plane;
-        const uint32_t dx = dr % a.board.w, dy = dr / a.board.w;
+        const uint32_t dx = dr % b.w, dy = dr / b.w;
         uint32_t cost = kMax, len = 0;
         if (dx >= f.x0 && dx < f.x0 + f.ww && dy >= f.y0 && dy < f.y0 + f.wh) {
             const u64 v = field_label(a, f, dx - f.x0, dy - f.y0, dl);
             cost = (uint32_t)(v >> 32);
             if (cost != kMax) len = (uint32_t)v + 1u;
             // a simple path never has more cells than its window
-            if ((uint64_t)len > (uint64_t)f.ww * f.wh * a.board.layers) {
+            if ((uint64_t)len > (uint64_t)f.ww * f.wh * b.layers) {
                 atomicOr(a.status, kStatusPathBroken);
                 len = 0;
             }
@@ -668,7 +670,7 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
     const DevField f = a.fields[warp];
     const uint32_t len = a.lens[f.out];
     if (len == 0) return;
-    const DevBoard b = a.board;
+    const DevBoard b = a.boards[f.board];
     const uint32_t plane = b.w * b.h;
     const uint32_t ntx = (f.ww + kTW - 1) / kTW;
     uint32_t *out = a.cells + a.offsets[f.out];
@@ -813,9 +815,21 @@ cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int 
 }
 
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st) {
+    // Cooperative (all CTAs co-resident, checked by the driver against occupancy);
+    // the attribute form is also what stream capture records as a graph node.
     RelaxArgs copy = a;
     void *args[] = {&copy};
-    return cudaLaunchCooperativeKernel(relax_fn(a.tile_h, threads), dim3(grid), dim3(threads), args, smem, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, relax_fn(a.tile_h, threads), args);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {

@@ -157,6 +157,9 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
                                              C.POINTER(C.c_float)]),
             "mrc_batch_destroy": (None, [vp]),
             "mrc_net_windows": (C.c_int, [u32, u32, u32, vp, u32, vp]),
+            "mrc_route_instances": (C.c_int, [vp, vp, u32, u32, C.POINTER(vp)]),
+            "mrc_batch_create_multi": (C.c_int, [vp, vp, u32, vp, vp, u32, vp, u32, C.POINTER(vp)]),
+            "mrc_batch_capture_graph": (C.c_int, [vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -286,13 +289,16 @@ class Board:
 
 
 class Batch:
-    """A validated batch of nets staged against a resident Board."""
+    """A validated batch of nets staged against one resident Board, or against
+    several (``board`` a sequence and ``net_board[i]`` the board of net i)."""
 
-    def __init__(self, board: Board, nets: Sequence[NetEndpoints],
+    def __init__(self, board, nets: Sequence[NetEndpoints],
                  windows: Optional[Sequence[IsolatedRouteWindow]] = None, retry_full: bool = True,
-                 keep_fields: bool = False, time_kernels: bool = False):
+                 keep_fields: bool = False, time_kernels: bool = False, net_board: Optional[Sequence[int]] = None):
+        boards = list(board) if isinstance(board, (list, tuple)) else [board]
         self.board = board
-        self.engine = board.engine
+        self.boards = boards
+        self.engine = boards[0].engine
         self.n = len(nets)
         self.keep_fields = keep_fields
         flags = ((MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
@@ -300,9 +306,24 @@ class Batch:
         m = _Marshal()
         h = C.c_void_p()
         e = self.engine
-        e._check(e.lib.mrc_batch_create(e.ctx, board.handle, m.nets(nets), len(nets), m.windows(windows), flags,
-                                        C.byref(h)))
+        if net_board is None and len(boards) == 1:
+            e._check(e.lib.mrc_batch_create(e.ctx, boards[0].handle, m.nets(nets), len(nets), m.windows(windows),
+                                            flags, C.byref(h)))
+        else:
+            if net_board is None or len(net_board) != len(nets):
+                raise InvalidArgument("net_board must give one board index per net")
+            handles = (C.c_void_p * len(boards))(*[b.handle for b in boards])
+            m.keep.append(handles)
+            nb = _u32(net_board)
+            e._check(e.lib.mrc_batch_create_multi(e.ctx, C.cast(handles, C.c_void_p), len(boards), m.nets(nets),
+                                                  m.arr(nb) if nb.size else None, len(nets), m.windows(windows),
+                                                  flags, C.byref(h)))
         self.handle = h
+
+    def capture_graph(self) -> None:
+        """Record the launch sequence as a CUDA graph; later launches replay it."""
+        e = self.engine
+        e._check(e.lib.mrc_batch_capture_graph(e.ctx, self.handle))
 
     def launch(self, stream: int = 0) -> None:
         """Enqueue the solve on a cudaStream_t (an integer handle, 0 = the engine's stream)."""
@@ -403,6 +424,30 @@ class Engine:
         res = C.c_void_p()
         self._check(self.lib.mrc_route_isolated_batch(self.ctx, C.byref(r), flags, C.byref(res)))
         return _take_result(self.lib, res, len(req.nets), keep_fields)
+
+    def route_instances(self, requests: Sequence[IsolatedRouteRequest], retry_full: bool = True,
+                        keep_fields: bool = False) -> List[IsolatedBatchResult]:
+        """Solve many independent instances (own board, nets, windows) in one
+        persistent launch; one result per instance."""
+        m = _Marshal()
+        reqs = (_Request * max(len(requests), 1))()
+        for k, rq in enumerate(requests):
+            reqs[k] = self._request(m, rq)
+        flags = (MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
+        res = C.c_void_p()
+        self._check(self.lib.mrc_route_instances(self.ctx, C.cast(reqs, C.c_void_p), len(requests), flags,
+                                                 C.byref(res)))
+        total = sum(len(rq.nets) for rq in requests)
+        allr = _take_result(self.lib, res, total, keep_fields)
+        out, o = [], 0
+        for rq in requests:
+            n = len(rq.nets)
+            sl = slice(o, o + n)
+            out.append(IsolatedBatchResult(allr.paths[sl], allr.search_costs[sl],
+                                           allr.fields[sl] if allr.fields is not None else None,
+                                           allr.field_windows[sl] if allr.field_windows is not None else None))
+            o += n
+        return out
 
     def route_isolated_plain(self, req: IsolatedRouteRequest, retry_full: bool = True,
                              keep_fields: bool = False) -> IsolatedBatchResult:

@@ -12,6 +12,10 @@ fixed seed and every distribution choice is recorded in ``Workload.meta``.
                         via 30, an exact 12-vertex star-radial polygon outline
                         rasterised to node and directed-edge bits with a 3-cell
                         clearance, 256 nets, windows by net_window.
+* ``uneven_instances`` — 4096 independent one-net instances whose bounding
+                        boxes have log-normal sides (median 96, sigma 0.5,
+                        clamped 16-1024), 2-8 layers, pad clusters with keepout
+                        halos and courtyard edge bits, unit steps, via 10.
 """
 from __future__ import annotations
 
@@ -188,3 +192,128 @@ def scaled(wl: Workload, n_nets: int) -> Workload:
     """The same board with only the first `n_nets` nets (parity-test sizes)."""
     return Workload(wl.name, wl.grid, wl.nets[:n_nets], wl.windows[:n_nets], wl.x, wl.y, wl.vias, wl.directed,
                     dict(wl.meta, n_nets=n_nets))
+
+
+@dataclass
+class InstanceSet:
+    """Many independent instances (each its own board and nets) solved together."""
+
+    name: str
+    instances: List[Workload]
+    meta: Dict = field(default_factory=dict)
+
+    def requests(self) -> List[IsolatedRouteRequest]:
+        return [w.request() for w in self.instances]
+
+    @property
+    def n_nets(self) -> int:
+        return sum(len(w.nets) for w in self.instances)
+
+    def window_cells(self) -> int:
+        return sum(w.window_cells() for w in self.instances)
+
+    def algorithmic_bytes(self) -> int:
+        """Sum over instances of window cells x bytes per cell (paths excluded)."""
+        return sum(w.window_cells() * w.bytes_per_cell() for w in self.instances)
+
+
+def _footprint(rng, w: int, h: int) -> Optional[tuple]:
+    """One pad cluster: 4-40 pads in one or two rows on a 2-5 cell pitch."""
+    n_pads = int(rng.integers(4, 41))
+    pitch = int(rng.integers(2, 6))
+    halo = int(rng.integers(1, 3))
+    rows = 1 if n_pads < 8 or rng.random() < 0.5 else 2
+    gap = 3 * pitch
+    per_row = (n_pads + rows - 1) // rows
+    vertical = bool(rng.random() < 0.5)
+    along, across = (h, w) if vertical else (w, h)
+    room = along - 2 * halo - 2
+    per_row = max(1, min(per_row, room // pitch + 1))
+    span_along = (per_row - 1) * pitch
+    span_across = (rows - 1) * gap
+    if span_along + 2 * halo + 2 > along or span_across + 2 * halo + 2 > across:
+        rows, span_across = 1, 0
+        if span_along + 2 * halo + 2 > along:
+            return None
+    a0 = int(rng.integers(halo + 1, along - halo - span_along))
+    c0 = int(rng.integers(halo + 1, across - halo - span_across))
+    pads = []
+    for r in range(rows):
+        for i in range(per_row):
+            a, c = a0 + i * pitch, c0 + r * gap
+            pads.append((c, a) if vertical else (a, c))
+    return pads, halo
+
+
+def uneven_instances(seed: int = 3, n_instances: int = 4096, median: float = 96.0, sigma: float = 0.5,
+                     lo: int = 16, hi: int = 1024, min_layers: int = 2, max_layers: int = 8) -> InstanceSet:
+    """Independent two-pin instances of uneven size, one net each; an instance is
+    its net's bounding box, solved whole (window = the instance).
+
+    Box side ~ LogNormal(ln median, sigma) clamped to [lo, hi], per axis; layers
+    uniform in [min_layers, max_layers]; unit enter weights, unit x/y steps, via
+    10.  Two to four pad clusters (4-40 pads, one or two rows, 2-5 cell pitch) on
+    the top or bottom layer: pads and a 1-2 cell keepout halo are obstacles;
+    the cluster's courtyard (its bounding box grown by the halo + 1) refuses
+    planar steps entering it on the pad layer (incoming directed-edge bits), so
+    a trace reaches a pad through its own halo or a via.  The net joins a pad of
+    the first cluster to a pad of the second; its passable pads are both pads
+    and their halo cells."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_instances):
+        w = int(np.clip(round(median * np.exp(sigma * rng.standard_normal())), lo, hi))
+        h = int(np.clip(round(median * np.exp(sigma * rng.standard_normal())), lo, hi))
+        layers = int(rng.integers(min_layers, max_layers + 1))
+        dims = Dims(w, h, layers)
+        cost = np.ones((layers, h, w), dtype=np.uint32)
+        board = np.zeros((layers, h, w), dtype=np.uint8)
+        clusters = []
+        n_cl = int(rng.integers(2, 5))
+        for _ in range(n_cl * 4):
+            if len(clusters) == n_cl:
+                break
+            fp = _footprint(rng, w, h)
+            if fp is None:
+                continue
+            pads, halo = fp
+            layer = 0 if rng.random() < 0.7 else layers - 1
+            clusters.append((pads, halo, layer))
+        if len(clusters) < 2:  # too small for two footprints: two single pads
+            clusters = [([(2, 2)], 1, 0), ([(w - 3, h - 3)], 1, layers - 1)]
+        own = {}
+        for ci, (pads, halo, layer) in enumerate(clusters):
+            xs = [p[0] for p in pads]
+            ys = [p[1] for p in pads]
+            bx0, bx1 = max(min(xs) - halo - 1, 0), min(max(xs) + halo + 1, w - 1)
+            by0, by1 = max(min(ys) - halo - 1, 0), min(max(ys) + halo + 1, h - 1)
+            pl = board[layer]
+            # courtyard: a step from outside the box into its border is refused
+            if bx0 > 0:
+                pl[by0:by1 + 1, bx0] |= BOARD_EDGE_NEG_X
+            if bx1 < w - 1:
+                pl[by0:by1 + 1, bx1] |= BOARD_EDGE_POS_X
+            if by0 > 0:
+                pl[by0, bx0:bx1 + 1] |= BOARD_EDGE_NEG_Y
+            if by1 < h - 1:
+                pl[by1, bx0:bx1 + 1] |= BOARD_EDGE_POS_Y
+            for (px, py) in pads:
+                cost[layer, max(py - halo, 0):py + halo + 1, max(px - halo, 0):px + halo + 1] = OBSTACLE
+            if ci < 2:
+                px, py = pads[int(rng.integers(0, len(pads)))]
+                cells = [dims.idx3(x, y, layer) for y in range(max(py - halo, 0), min(py + halo, h - 1) + 1)
+                         for x in range(max(px - halo, 0), min(px + halo, w - 1) + 1)]
+                own[ci] = (dims.idx3(px, py, layer), cells)
+        src, src_cells = own[0]
+        dst, dst_cells = own[1]
+        pads_list = sorted(set(src_cells) | set(dst_cells))
+        net = NetEndpoints(f"u{k}", src, dst, pads_list)
+        grid = Grid(dims, cost.reshape(-1), board.reshape(-1))
+        out.append(Workload("uneven", grid, [net], [IsolatedRouteWindow.full(dims)], np.ones(w - 1, np.uint32),
+                            np.ones(h - 1, np.uint32), [10] * (layers - 1), None, {}))
+    meta = {"workload": f"uneven instances, {n_instances} nets", "seed": seed,
+            "side": f"LogNormal(ln {median:g}, sigma {sigma:g}) clamped {lo}-{hi}, per axis",
+            "layers": f"uniform {min_layers}-{max_layers}", "pads": "2-4 clusters of 4-40 pads, 1-2 rows, "
+            "pitch 2-5, 1-2 cell keepout halo (obstacles), courtyard incoming-edge bits on the pad layer",
+            "step": 1, "via": 10, "windows": "whole instance (the net's bounding box)"}
+    return InstanceSet("uneven", out, meta)
