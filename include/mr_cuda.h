@@ -274,6 +274,68 @@ mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_request *req, voi
                                             uint64_t *path_offsets, uint32_t *path_cells,
                                             uint64_t path_cells_capacity);
 
+/* ---- snapshot negotiation rounds -------------------------------------------- */
+
+/* One negotiation round on a frozen price snapshot, on the device: the Jacobi
+ * iteration of NegotiatedRouter (crates/mr-cpu/src/negotiated.rs:1610-1991)
+ * with occupancy and history kept per directed planar edge slot instead of per
+ * cell.  Each round:
+ *   1. dirty set: round 0 every net; later, every net that is unrouted or whose
+ *      path uses a planar edge that two or more nets used after the previous
+ *      round (the reference's prev_overused test, :1632-1642);
+ *   2. rip-up: the dirty nets' old paths leave `present`;
+ *   3. snapshot: price(slot) = base == 0xFFFFFFFF ? 0xFFFFFFFF
+ *        : min(base + history + pfac * present_weight * present, 0xFFFFFFFE),
+ *      pfac = 1 + round (priced_with_base :2768-2795, passable_search_cost);
+ *   4. every dirty net is solved alone on the snapshot (the isolated batch:
+ *      window, then full-board retry, canonical paths);
+ *   5. merge: the new paths enter `present` (unrouted nets contribute nothing);
+ *   6. history += history_step on every slot whose edge two or more nets use
+ *      (:1929-1948), then the next dirty set is computed.
+ * The snapshot is the request's directed in-price plane, so the cell enter
+ * weight multiplies the whole price; with unit enter weights (the negotiation
+ * boards) this is the reference's base*enter + congestion.  Slots of an
+ * undirected edge {a, b}: b's slot "from a" and a's slot "from b", both counted.
+ * This entry point has no single counterpart in the reference (its rounds run
+ * on the CPU); the round semantics above are the reference's, on edges. */
+typedef struct mrc_negotiation mrc_negotiation;
+
+typedef struct {
+    uint32_t present_weight; /* SCALE in the reference: 16 */
+    uint32_t history_step;   /* added per overused edge and round */
+} mrc_negotiation_params;
+
+typedef struct {
+    uint32_t round, pfac;
+    uint32_t dirty;           /* nets routed this round */
+    uint32_t routed;          /* of those, reached their target */
+    uint32_t retried;         /* of those, needed the full-board retry */
+    uint32_t next_dirty;      /* nets the next round will route */
+    uint64_t overused_edges;  /* undirected planar edges used by >= 2 nets after the merge */
+    uint64_t window_cells;    /* cells solved (windows + retries) */
+    uint64_t path_cells;      /* cells on the current paths of all nets */
+    float round_ms;           /* device-timeline time of the round on the engine stream */
+} mrc_round_stats;
+
+/* The request gives the board (grid, edges), the nets and their windows.  Base
+ * planar prices come from edges.directed_in_costs or, when it is NULL, from the
+ * per-axis prices (in-price from -x at x = x_edge_costs[x-1], and so on). */
+mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *req,
+                                  const mrc_negotiation_params *params, mrc_negotiation **out);
+/* Runs the next round.  A round with no dirty net does nothing (converged). */
+mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *neg, mrc_round_stats *stats);
+/* Current paths of every net (CSR, request order; an empty path = unrouted).
+ * The pointers stay valid until the next round or destroy. */
+mrc_status mrc_negotiation_paths(const mrc_negotiation *neg, uint32_t *n_nets, const uint64_t **offsets,
+                                 const uint32_t **cells);
+/* Copies 4 u32 per cell (slots -y, -x, +x, +y) of the occupancy, history and
+ * the last snapshot's prices to host buffers; any of them may be NULL. */
+mrc_status mrc_negotiation_read(mrc_context *ctx, mrc_negotiation *neg, uint32_t *present, uint32_t *history,
+                                uint32_t *snapshot);
+/* Nets the next round will route (ascending). */
+mrc_status mrc_negotiation_dirty(const mrc_negotiation *neg, uint32_t *n, const uint32_t **nets);
+void mrc_negotiation_destroy(mrc_negotiation *neg);
+
 /* net_window (negotiated.rs:568-594) for a batch of nets. */
 mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
                            mrc_window *out);

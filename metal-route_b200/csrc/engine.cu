@@ -9,12 +9,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -93,11 +95,45 @@ class Pool {
 
 }  // namespace
 
+namespace {
+
+// Pinned host staging reused across calls: host inputs are gathered here by
+// several threads and reach HBM with full-rate asynchronous copies.
+struct HostStage {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t done = nullptr;  // the last copy out of the stage
+    ~HostStage() {
+        if (p) cudaFreeHost(p);
+        if (done) cudaEventDestroy(done);
+    }
+    cudaError_t reserve(size_t n) {
+        if (!done) {
+            cudaError_t e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        cudaError_t e = cudaEventSynchronize(done);  // no copy may still read the old contents
+        if (e != cudaSuccess) return e;
+        if (n <= bytes) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t want = std::max(n + n / 4, (size_t)64 << 20);
+        e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        bytes = want;
+        return cudaSuccess;
+    }
+};
+
+}  // namespace
+
 struct mrc_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::mutex mu;
     Pool pool;
+    HostStage stage;
     int sms = 148;
     size_t smem_optin = 0;
     // autotuned relax configuration per (layers, directed): tile height, CTA width
@@ -370,29 +406,67 @@ mrc_status board_pack_build(mrc_context *ctx, const mrc_isolated_request *inst, 
         o.dir = b->directed ? take(g.n * 16) : SIZE_MAX;
         pk->boards.push_back(std::move(b));
     }
-    std::vector<uint8_t> host(total);
-    for (uint32_t k = 0; k < n; ++k) {
+    MRC_TRY(pk->data.get(ctx, std::max<size_t>(total, 256), "instance boards"));
+    MRC_CUDA(ctx->stage.reserve(total), "pinned staging buffer");
+    unsigned char *host = static_cast<unsigned char *>(ctx->stage.p);
+    auto fill = [&](uint32_t k) {
         const GridView &g = pk->boards[k]->view;
         const mrc_edges &e = inst[k].edges;
         const Off &o = offs[k];
-        std::memcpy(host.data() + o.cost, g.cost, g.n * 4);
+        std::memcpy(host + o.cost, g.cost, g.n * 4);
         if (o.flags != SIZE_MAX) {
-            uint8_t *fl = host.data() + o.flags;
-            for (uint64_t i = 0; i < g.n; ++i)
-                fl[i] = (uint8_t)((g.board ? g.board[i] : 0) | (g.via_forbidden && g.via_forbidden[i] ? kStaticVia : 0));
+            uint8_t *fl = host + o.flags;
+            if (!g.via_forbidden) {
+                std::memcpy(fl, g.board, g.n);
+            } else {
+                for (uint64_t i = 0; i < g.n; ++i)
+                    fl[i] = (uint8_t)((g.board ? g.board[i] : 0) | (g.via_forbidden[i] ? kStaticVia : 0));
+            }
         }
-        if (e.n_x_edge_costs) std::memcpy(host.data() + o.x, e.x_edge_costs, (size_t)e.n_x_edge_costs * 4);
-        if (e.n_y_edge_costs) std::memcpy(host.data() + o.y, e.y_edge_costs, (size_t)e.n_y_edge_costs * 4);
-        uint32_t *via = reinterpret_cast<uint32_t *>(host.data() + o.via);
+        if (e.n_x_edge_costs) std::memcpy(host + o.x, e.x_edge_costs, (size_t)e.n_x_edge_costs * 4);
+        if (e.n_y_edge_costs) std::memcpy(host + o.y, e.y_edge_costs, (size_t)e.n_y_edge_costs * 4);
+        uint32_t *via = reinterpret_cast<uint32_t *>(host + o.via);
         uint32_t mask = 0;
         for (uint32_t i = 0; i < e.n_via_edge_costs; ++i) {
             via[i] = e.via_edge_costs[i];
             if (e.via_allowed[i]) mask |= 1u << i;
         }
-        if (o.dir != SIZE_MAX) std::memcpy(host.data() + o.dir, e.directed_in_costs, g.n * 16);
+        if (o.dir != SIZE_MAX) std::memcpy(host + o.dir, e.directed_in_costs, g.n * 16);
         pk->boards[k]->dev.via_mask = mask;
+    };
+    // Worker threads fill instances in index order; this thread ships every
+    // completed prefix of >= 32 MB to the device while the rest is still filled.
+    const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const uint32_t nthreads = total > (64u << 20) ? std::min(hw, n) : 1;
+    std::vector<std::atomic<uint8_t>> done(n);
+    for (auto &d : done) d.store(0, std::memory_order_relaxed);
+    std::atomic<uint32_t> next{0};
+    std::vector<std::thread> workers;
+    auto work = [&]() {
+        for (uint32_t k; (k = next.fetch_add(1, std::memory_order_relaxed)) < n;) {
+            fill(k);
+            done[k].store(1, std::memory_order_release);
+        }
+    };
+    for (uint32_t t = 1; t < nthreads; ++t) workers.emplace_back(work);
+    if (nthreads == 1) work();
+    size_t shipped = 0;
+    uint32_t ready = 0;
+    cudaError_t ce = cudaSuccess;
+    while (shipped < total && ce == cudaSuccess) {
+        while (ready < n && done[ready].load(std::memory_order_acquire)) ++ready;
+        const size_t upto = ready == n ? total : offs[ready].cost;
+        if (upto > shipped && (upto - shipped >= (32u << 20) || ready == n)) {
+            ce = cudaMemcpyAsync(pk->data.as<unsigned char>() + shipped, host + shipped, upto - shipped,
+                                 cudaMemcpyHostToDevice, ctx->stream);
+            shipped = upto;
+        } else {
+            std::this_thread::yield();
+        }
     }
-    MRC_TRY(upload(ctx, pk->data, host.data(), host.size(), "upload instance boards"));
+    for (auto &t : workers) t.join();
+    MRC_CUDA(ce, "upload instance boards");
+    MRC_CUDA(cudaEventRecord(ctx->stage.done, ctx->stream), "stage event");
     unsigned char *base = pk->data.as<unsigned char>();
     for (uint32_t k = 0; k < n; ++k) {
         mrc_board &b = *pk->boards[k];
@@ -1213,6 +1287,258 @@ void mrc_batch_destroy(mrc_batch *batch) {
         delete batch;
     } else {
         delete batch;
+    }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Snapshot negotiation rounds (negotiated.rs:1610-1991 on directed planar edge
+// slots; the device kernels are in negotiate.cu).
+
+struct mrc_negotiation {
+    mrc_context *ctx = nullptr;
+    std::unique_ptr<mrc_board> base;   // base board; dev.directed = base prices
+    std::unique_ptr<mrc_board> snap;   // the same board priced by the snapshot
+    mrc_negotiation_params params{16, 1};
+    std::vector<NetCopy> nets;
+    std::vector<mrc_window> windows;
+    std::vector<std::vector<uint32_t>> paths;
+    std::vector<uint64_t> offsets;     // CSR of `paths` (host copy of d_off/d_cells)
+    std::vector<uint32_t> cells;
+    std::vector<uint32_t> dirty;       // nets of the next round
+    uint32_t round = 0;
+    DBuf d_present, d_history, d_snap, d_off, d_cells, d_list, d_flags, d_count;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~mrc_negotiation() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+mrc_status negotiation_upload_paths(mrc_negotiation *ng) {
+    mrc_context *ctx = ng->ctx;
+    const uint32_t n = (uint32_t)ng->nets.size();
+    ng->offsets.assign(n + 1, 0);
+    uint64_t o = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        ng->offsets[i] = o;
+        o += ng->paths[i].size();
+    }
+    ng->offsets[n] = o;
+    ng->cells.clear();
+    ng->cells.reserve(o);
+    for (auto &p : ng->paths) ng->cells.insert(ng->cells.end(), p.begin(), p.end());
+    MRC_TRY(upload(ctx, ng->d_off, ng->offsets.data(), ng->offsets.size() * 8, "upload path offsets"));
+    MRC_TRY(upload(ctx, ng->d_cells, ng->cells.data(), ng->cells.size() * 4, "upload path cells"));
+    return MRC_OK;
+}
+
+OccupancyArgs negotiation_occupancy(mrc_negotiation *ng, uint32_t n_list, bool add) {
+    OccupancyArgs a;
+    a.offsets = ng->d_off.as<unsigned long long>();
+    a.cells = ng->d_cells.as<uint32_t>();
+    a.list = ng->d_list.as<uint32_t>();
+    a.n_list = n_list;
+    a.w = ng->base->view.w;
+    a.plane = ng->base->view.w * ng->base->view.h;
+    a.present = ng->d_present.as<uint32_t>();
+    a.add = add;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *req,
+                                  const mrc_negotiation_params *params, mrc_negotiation **out) {
+    if (!ctx || !req || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    std::unique_ptr<mrc_negotiation> ng(new mrc_negotiation());
+    ng->ctx = ctx;
+    if (params) ng->params = *params;
+    GridView g;
+    MRC_TRY(view_grid(req->grid, &g));
+    const mrc_edges &e = req->edges;
+    std::vector<uint32_t> dir;
+    mrc_edges eb = e;
+    if (!e.directed_in_costs) {
+        // per-axis prices as in-prices; slots without a neighbour are never read
+        const uint32_t ex = g.w ? g.w - 1 : 0, ey = g.h ? g.h - 1 : 0;
+        if (e.n_x_edge_costs != ex || e.n_y_edge_costs != ey || (ex && !e.x_edge_costs) || (ey && !e.y_edge_costs))
+            return fail(MRC_ERR_INVALID_ARGUMENT, "edge price vectors do not match the grid");
+        dir.resize(g.n * 4);
+        for (uint64_t c = 0; c < g.n; ++c) {
+            const uint32_t r = (uint32_t)(c % ((uint64_t)g.w * g.h)), x = r % g.w, y = r / g.w;
+            dir[4 * c + 0] = y > 0 ? e.y_edge_costs[y - 1] : kMax;
+            dir[4 * c + 1] = x > 0 ? e.x_edge_costs[x - 1] : kMax;
+            dir[4 * c + 2] = x + 1 < g.w ? e.x_edge_costs[x] : kMax;
+            dir[4 * c + 3] = y + 1 < g.h ? e.y_edge_costs[y] : kMax;
+        }
+        eb.directed_in_costs = dir.data();
+    }
+    ng->base.reset(new mrc_board());
+    MRC_TRY(board_build(ctx, req->grid, &eb, true, ng->base.get()));
+    MRC_TRY(validate_nets(ng->base->view, req->nets, req->n_nets, &ng->nets));
+    MRC_TRY(collect_windows(ng->base->view, ng->nets, req->windows, &ng->windows));
+    const uint32_t n = req->n_nets;
+    const size_t slots = (size_t)g.n * 16;
+    MRC_TRY(ng->d_present.get(ctx, std::max<size_t>(slots, 16), "occupancy"));
+    MRC_TRY(ng->d_history.get(ctx, std::max<size_t>(slots, 16), "history"));
+    MRC_TRY(ng->d_snap.get(ctx, std::max<size_t>(slots, 16), "snapshot prices"));
+    MRC_CUDA(cudaMemsetAsync(ng->d_present.p, 0, slots, ctx->stream), "clear occupancy");
+    MRC_CUDA(cudaMemsetAsync(ng->d_history.p, 0, slots, ctx->stream), "clear history");
+    MRC_TRY(ng->d_flags.get(ctx, std::max<size_t>(n, 4), "dirty flags"));
+    MRC_TRY(ng->d_count.get(ctx, 8, "overuse count"));
+    ng->snap.reset(new mrc_board());
+    ng->snap->ctx = ctx;
+    ng->snap->view = ng->base->view;
+    ng->snap->directed = true;
+    ng->snap->dev = ng->base->dev;
+    ng->snap->dev.directed = ng->d_snap.as<uint4>();
+    ng->paths.assign(n, {});
+    ng->dirty.resize(n);
+    std::iota(ng->dirty.begin(), ng->dirty.end(), 0u);
+    MRC_TRY(negotiation_upload_paths(ng.get()));
+    MRC_CUDA(cudaEventCreate(&ng->ev0), "create event");
+    MRC_CUDA(cudaEventCreate(&ng->ev1), "create event");
+    MRC_CUDA(cudaStreamSynchronize(ctx->stream), "negotiation setup");
+    *out = ng.release();
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *ng, mrc_round_stats *st) {
+    if (!ctx || !ng || !st) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    std::memset(st, 0, sizeof(*st));
+    st->round = ng->round;
+    st->pfac = 1 + ng->round;
+    const uint32_t n_dirty = (uint32_t)ng->dirty.size();
+    st->dirty = n_dirty;
+    if (!n_dirty) {
+        st->path_cells = ng->cells.size();
+        return MRC_OK;
+    }
+    const GridView &g = ng->base->view;
+    cudaStream_t s = ctx->stream;
+    MRC_CUDA(cudaEventRecord(ng->ev0, s), "record event");
+    // 2. rip-up of the dirty nets' current paths
+    MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
+    MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, false), s), "rip-up");
+    // 3. the frozen snapshot
+    SnapshotArgs sa;
+    sa.base = ng->base->dev.directed;
+    sa.present = ng->d_present.as<uint4>();
+    sa.history = ng->d_history.as<uint4>();
+    sa.out = ng->d_snap.as<uint4>();
+    sa.n = g.n;
+    sa.pfac = st->pfac;
+    sa.weight = ng->params.present_weight;
+    MRC_CUDA(snapshot_launch(sa, s), "price snapshot");
+    // 4. the dirty nets, alone on the snapshot (window, then full-board retry)
+    std::vector<NetCopy> nets;
+    std::vector<mrc_window> wins;
+    nets.reserve(n_dirty);
+    for (uint32_t i : ng->dirty) {
+        nets.push_back(ng->nets[i]);
+        wins.push_back(ng->windows[i]);
+    }
+    mrc_result *raw = nullptr;
+    MRC_TRY(solve(ctx, {ng->snap.get()}, std::move(nets), std::move(wins), MRC_FLAG_RETRY_FULL, &raw, nullptr));
+    std::unique_ptr<mrc_result> res(raw);
+    for (uint32_t k = 0; k < n_dirty; ++k) {
+        const uint32_t i = ng->dirty[k];
+        ng->paths[i].assign(res->cells.begin() + res->offsets[k], res->cells.begin() + res->offsets[k + 1]);
+        if (!ng->paths[i].empty()) st->routed++;
+        const mrc_window &w0 = ng->windows[i], &w1 = res->field_windows[k];
+        const uint64_t c0 = (uint64_t)(w0.x1 - w0.x0 + 1) * (w0.y1 - w0.y0 + 1) * g.layers;
+        const bool retried = w1.x0 != w0.x0 || w1.y0 != w0.y0 || w1.x1 != w0.x1 || w1.y1 != w0.y1;
+        st->window_cells += c0 + (retried ? g.n : 0);
+        st->retried += retried;
+    }
+    // 5. merge: the new paths enter the occupancy
+    MRC_TRY(negotiation_upload_paths(ng));
+    MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
+    MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, true), s), "merge paths");
+    // 6. history on overused edges, then the next dirty set
+    MRC_CUDA(cudaMemsetAsync(ng->d_count.p, 0, 8, s), "clear count");
+    OveruseArgs oa;
+    oa.present = ng->d_present.as<uint4>();
+    oa.history = ng->d_history.as<uint4>();
+    oa.n = g.n;
+    oa.step = ng->params.history_step;
+    oa.count = ng->d_count.as<unsigned long long>();
+    MRC_CUDA(overuse_launch(oa, s), "overuse scan");
+    const uint32_t n = (uint32_t)ng->nets.size();
+    DirtyArgs da;
+    da.offsets = ng->d_off.as<unsigned long long>();
+    da.cells = ng->d_cells.as<uint32_t>();
+    da.n_nets = n;
+    da.w = g.w;
+    da.plane = g.w * g.h;
+    da.present = ng->d_present.as<uint32_t>();
+    da.flags = ng->d_flags.as<uint8_t>();
+    MRC_CUDA(dirty_launch(da, s), "dirty scan");
+    MRC_CUDA(cudaEventRecord(ng->ev1, s), "record event");
+    std::vector<uint8_t> flags(n);
+    unsigned long long slots = 0;
+    if (n) MRC_CUDA(cudaMemcpyAsync(flags.data(), ng->d_flags.p, n, cudaMemcpyDeviceToHost, s), "read dirty flags");
+    MRC_CUDA(cudaMemcpyAsync(&slots, ng->d_count.p, 8, cudaMemcpyDeviceToHost, s), "read overuse count");
+    MRC_CUDA(cudaStreamSynchronize(s), "negotiation round");
+    MRC_CUDA(cudaEventElapsedTime(&st->round_ms, ng->ev0, ng->ev1), "round time");
+    ng->dirty.clear();
+    for (uint32_t i = 0; i < n; ++i)
+        if (flags[i]) ng->dirty.push_back(i);
+    st->overused_edges = slots / 2;
+    st->next_dirty = (uint32_t)ng->dirty.size();
+    st->path_cells = ng->cells.size();
+    ng->round++;
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_paths(const mrc_negotiation *ng, uint32_t *n_nets, const uint64_t **offsets,
+                                 const uint32_t **cells) {
+    if (!ng || !n_nets || !offsets || !cells) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *n_nets = (uint32_t)ng->nets.size();
+    *offsets = ng->offsets.data();
+    *cells = ng->cells.data();
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_read(mrc_context *ctx, mrc_negotiation *ng, uint32_t *present, uint32_t *history,
+                                uint32_t *snapshot) {
+    if (!ctx || !ng) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    const size_t bytes = (size_t)ng->base->view.n * 16;
+    if (present) MRC_CUDA(cudaMemcpy(present, ng->d_present.p, bytes, cudaMemcpyDeviceToHost), "read occupancy");
+    if (history) MRC_CUDA(cudaMemcpy(history, ng->d_history.p, bytes, cudaMemcpyDeviceToHost), "read history");
+    if (snapshot) MRC_CUDA(cudaMemcpy(snapshot, ng->d_snap.p, bytes, cudaMemcpyDeviceToHost), "read snapshot");
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_dirty(const mrc_negotiation *ng, uint32_t *n, const uint32_t **nets) {
+    if (!ng || !n || !nets) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *n = (uint32_t)ng->dirty.size();
+    *nets = ng->dirty.data();
+    return MRC_OK;
+}
+
+void mrc_negotiation_destroy(mrc_negotiation *ng) {
+    if (!ng) return;
+    mrc_context *ctx = ng->ctx;
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        delete ng;
+    } else {
+        delete ng;
     }
 }
 

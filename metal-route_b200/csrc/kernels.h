@@ -59,6 +59,47 @@ struct PlainArgs {
     uint32_t *changed;
 };
 
+// Snapshot negotiation (negotiate.cu).  Occupancy / history / prices are
+// uint4 per cell over the directed planar in-edge slots (-y, -x, +x, +y).
+struct OccupancyArgs {
+    const unsigned long long *offsets;  // path CSR of every net
+    const uint32_t *cells;
+    const uint32_t *list;               // nets to apply (nullable = nets 0..n_list-1)
+    uint32_t n_list;
+    uint32_t w, plane;
+    uint32_t *present;                  // 4 per cell
+    bool add;                           // add the paths (true) or rip them up (false)
+};
+
+struct SnapshotArgs {
+    const uint4 *base, *present, *history;
+    uint4 *out;
+    uint64_t n;                         // cells
+    uint32_t pfac, weight;
+};
+
+struct OveruseArgs {
+    const uint4 *present;
+    uint4 *history;
+    uint64_t n;
+    uint32_t step;
+    unsigned long long *count;          // overused slots (2 per undirected edge)
+};
+
+struct DirtyArgs {
+    const unsigned long long *offsets;
+    const uint32_t *cells;
+    uint32_t n_nets;
+    uint32_t w, plane;
+    const uint32_t *present;
+    uint8_t *flags;                     // 1 = route again next round
+};
+
+cudaError_t occupancy_launch(const OccupancyArgs &a, cudaStream_t st);
+cudaError_t snapshot_launch(const SnapshotArgs &a, cudaStream_t st);
+cudaError_t overuse_launch(const OveruseArgs &a, cudaStream_t st);
+cudaError_t dirty_launch(const DirtyArgs &a, cudaStream_t st);
+
 // Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);
 // The relax kernel is instantiated for threads in {128, 256} per CTA.

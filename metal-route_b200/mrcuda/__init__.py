@@ -33,6 +33,7 @@ from .api import (  # noqa: F401
     IterationLimit,
     LimitExceeded,
     MalformedGrid,
+    Negotiation,
     OutOfMemory,
     RouterError,
     exported_symbols,

@@ -111,6 +111,16 @@ class _Request(C.Structure):
                 ("windows", C.c_void_p), ("edges", _Edges)]
 
 
+class _NegParams(C.Structure):
+    _fields_ = [("present_weight", C.c_uint32), ("history_step", C.c_uint32)]
+
+
+class _RoundStats(C.Structure):
+    _fields_ = [("round", C.c_uint32), ("pfac", C.c_uint32), ("dirty", C.c_uint32), ("routed", C.c_uint32),
+                ("retried", C.c_uint32), ("next_dirty", C.c_uint32), ("overused_edges", C.c_uint64),
+                ("window_cells", C.c_uint64), ("path_cells", C.c_uint64), ("round_ms", C.c_float)]
+
+
 _lib = None
 _lib_lock = threading.Lock()
 
@@ -160,6 +170,12 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_route_instances": (C.c_int, [vp, vp, u32, u32, C.POINTER(vp)]),
             "mrc_batch_create_multi": (C.c_int, [vp, vp, u32, vp, vp, u32, vp, u32, C.POINTER(vp)]),
             "mrc_batch_capture_graph": (C.c_int, [vp, vp]),
+            "mrc_negotiation_create": (C.c_int, [vp, C.POINTER(_Request), C.POINTER(_NegParams), C.POINTER(vp)]),
+            "mrc_negotiation_round": (C.c_int, [vp, vp, C.POINTER(_RoundStats)]),
+            "mrc_negotiation_paths": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u64p), C.POINTER(u32p)]),
+            "mrc_negotiation_read": (C.c_int, [vp, vp, vp, vp, vp]),
+            "mrc_negotiation_dirty": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32p)]),
+            "mrc_negotiation_destroy": (None, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -176,7 +192,25 @@ def exported_symbols() -> List[str]:
 
 
 def _u32(a) -> np.ndarray:
+    if type(a) is np.ndarray and a.dtype == np.uint32 and a.ndim == 1 and a.flags.c_contiguous:
+        return a
     return np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1))
+
+
+_VIA_CACHE = {}
+
+
+def _via_arrays(vias):
+    """(prices u32, allowed u8) for an Option<u32> via vector, shared between
+    requests with the same vector (arrays are never written)."""
+    key = tuple(vias)
+    hit = _VIA_CACHE.get(key)
+    if hit is None:
+        hit = (np.array([0 if v is None else int(v) for v in key], dtype=np.uint32),
+               np.array([0 if v is None else 1 for v in key], dtype=np.uint8))
+        if len(_VIA_CACHE) < 4096:
+            _VIA_CACHE[key] = hit
+    return hit
 
 
 class _Marshal:
@@ -189,7 +223,10 @@ class _Marshal:
         if a is None:
             return None
         self.keep.append(a)
-        return a.ctypes.data
+        try:
+            return C.addressof(C.c_char.from_buffer(a))
+        except (TypeError, ValueError):  # read-only or empty buffer
+            return a.ctypes.data
 
     def grid(self, g: Grid) -> _Grid:
         s = _Grid(g.dims.w, g.dims.h, g.dims.layers, self.arr(g.cost), self.arr(g.board_constraint),
@@ -218,8 +255,7 @@ class _Marshal:
 
     def edges(self, x, y, vias, directed=None) -> _Edges:
         xe, ye = _u32(x), _u32(y)
-        ve = np.array([0 if v is None else int(v) for v in vias], dtype=np.uint32)
-        va = np.array([0 if v is None else 1 for v in vias], dtype=np.uint8)
+        ve, va = _via_arrays(vias)
         d = None if directed is None else _u32(directed)
         e = _Edges(self.arr(xe) if xe.size else None, xe.size, self.arr(ye) if ye.size else None, ye.size,
                    self.arr(ve) if ve.size else None, self.arr(va) if va.size else None, ve.size, self.arr(d))
@@ -379,6 +415,67 @@ class Batch:
             pass
 
 
+class Negotiation:
+    """Snapshot negotiation rounds on the device (mrc_negotiation_*): each
+    round rips up the dirty nets, prices a frozen snapshot
+    base + history + pfac * present_weight * present per directed planar edge
+    slot, routes the dirty nets alone on it, merges them back and adds
+    history_step to every edge two or more nets use."""
+
+    def __init__(self, engine: "Engine", req: IsolatedRouteRequest, present_weight: int = 16,
+                 history_step: int = 1):
+        self.engine = engine
+        self.n = len(req.nets)
+        self.dims = req.grid.dims
+        m = _Marshal()
+        r = engine._request(m, req)
+        h = C.c_void_p()
+        engine._check(engine.lib.mrc_negotiation_create(engine.ctx, C.byref(r),
+                                                        C.byref(_NegParams(present_weight, history_step)),
+                                                        C.byref(h)))
+        self.handle = h
+
+    def round(self) -> dict:
+        st = _RoundStats()
+        e = self.engine
+        e._check(e.lib.mrc_negotiation_round(e.ctx, self.handle, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in _RoundStats._fields_}
+
+    def paths(self) -> List[Optional[List[int]]]:
+        n, off, cells = C.c_uint32(), C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+        self.engine._check(self.engine.lib.mrc_negotiation_paths(self.handle, C.byref(n), C.byref(off),
+                                                                 C.byref(cells)))
+        o = np.ctypeslib.as_array(off, shape=(n.value + 1,)).copy()
+        total = int(o[-1])
+        c = np.ctypeslib.as_array(cells, shape=(total,)).copy() if total else np.zeros(0, np.uint32)
+        return [c[o[i]:o[i + 1]].tolist() if o[i + 1] > o[i] else None for i in range(n.value)]
+
+    def read(self):
+        """(present, history, snapshot) as uint32 arrays of shape (cells, 4)."""
+        cells = len(self.dims)
+        out = [np.zeros((cells, 4), np.uint32) for _ in range(3)]
+        m = _Marshal()
+        e = self.engine
+        e._check(e.lib.mrc_negotiation_read(e.ctx, self.handle, m.arr(out[0]), m.arr(out[1]), m.arr(out[2])))
+        return tuple(out)
+
+    def dirty(self) -> List[int]:
+        n, p = C.c_uint32(), C.POINTER(C.c_uint32)()
+        self.engine._check(self.engine.lib.mrc_negotiation_dirty(self.handle, C.byref(n), C.byref(p)))
+        return np.ctypeslib.as_array(p, shape=(n.value,)).tolist() if n.value else []
+
+    def close(self):
+        if self.handle:
+            self.engine.lib.mrc_negotiation_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Engine:
     """One CUDA context of the engine (one per process per device)."""
 
@@ -479,6 +576,9 @@ class Engine:
     def board(self, grid: Grid, x, y, vias, directed=None) -> Board:
         return Board(self, grid, x, y, vias, directed)
 
+    def negotiation(self, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1) -> Negotiation:
+        return Negotiation(self, req, present_weight, history_step)
+
 
 def net_windows(dims, nets: Sequence[NetEndpoints]) -> List[IsolatedRouteWindow]:
     """net_window (negotiated.rs:568-594), computed by the library."""
@@ -537,7 +637,7 @@ class CudaIsolatedProvider:
 
 
 __all__ = [
-    "Engine", "Board", "Batch", "CudaIsolatedProvider", "IsolatedBatchResult", "BoardRoute", "RouteResult",
+    "Engine", "Board", "Batch", "Negotiation", "CudaIsolatedProvider", "IsolatedBatchResult", "BoardRoute", "RouteResult",
     "RouterError", "InvalidArgument", "MalformedGrid", "InvalidEndpoint", "BackendUnavailable", "Busy",
     "IterationLimit", "OutOfMemory", "LimitExceeded", "net_windows", "load_library", "exported_symbols",
     "COST_MAX", "NO_PATH",

@@ -317,3 +317,61 @@ def uneven_instances(seed: int = 3, n_instances: int = 4096, median: float = 96.
             "pitch 2-5, 1-2 cell keepout halo (obstacles), courtyard incoming-edge bits on the pad layer",
             "step": 1, "via": 10, "windows": "whole instance (the net's bounding box)"}
     return InstanceSet("uneven", out, meta)
+
+
+def snapshot_board(seed: int = 4, w: int = 2048, h: int = 2048, layers: int = 6, n_nets: int = 3000,
+                   median: float = 300.0, sigma: float = 0.5, blocked_frac: float = 0.05,
+                   via_cost: int = 30) -> Workload:
+    """The board of the snapshot negotiation rounds.
+
+    Undirected planar edge prices 10 + Geom(p=0.5) (failures before the first
+    success), stored on both in-edge slots; unit enter weights; keepout
+    rectangles 8-64 cells a side on random layers until `blocked_frac` of the
+    cells are obstacles; via 30.  Two-pin nets: source uniform over free cells,
+    Manhattan distance ~ LogNormal(ln median, sigma) clamped to [8, w + h - 2],
+    split uniformly between x and y with random signs, target on a random
+    layer (redrawn until free); windows by net_window."""
+    rng = np.random.default_rng(seed)
+    dims = Dims(w, h, layers)
+    n = len(dims)
+    cost = np.ones((layers, h, w), dtype=np.uint32)
+    target = int(blocked_frac * n)
+    blocked = 0
+    while blocked < target:
+        rw, rh = int(rng.integers(8, 65)), int(rng.integers(8, 65))
+        x0, y0 = int(rng.integers(0, max(w - rw, 0) + 1)), int(rng.integers(0, max(h - rh, 0) + 1))
+        l = int(rng.integers(0, layers))
+        sl = cost[l, y0:y0 + rh, x0:x0 + rw]
+        blocked += int((sl != OBSTACLE).sum())
+        sl[...] = OBSTACLE
+    d = np.full((layers, h, w, 4), OBSTACLE, dtype=np.uint32)
+    ex = (10 + rng.geometric(0.5, (layers, h, max(w - 1, 0))) - 1).astype(np.uint32)
+    ey = (10 + rng.geometric(0.5, (layers, max(h - 1, 0), w)) - 1).astype(np.uint32)
+    d[:, :, 1:, 1] = ex  # x -> x+1 enters from -x
+    d[:, :, :-1, 2] = ex
+    d[:, 1:, :, 0] = ey
+    d[:, :-1, :, 3] = ey
+    grid = Grid(dims, cost.reshape(-1))
+    free = cost.reshape(-1) != OBSTACLE
+    nets = []
+    while len(nets) < n_nets:
+        src = int(rng.integers(0, n))
+        if not free[src]:
+            continue
+        sx, sy, _ = dims.xyz(src)
+        dist = int(np.clip(round(median * np.exp(sigma * rng.standard_normal())), 8, w + h - 2))
+        dx = int(round(dist * rng.random()))
+        dy = dist - dx
+        tx = int(np.clip(sx + (dx if rng.random() < 0.5 else -dx), 0, w - 1))
+        ty = int(np.clip(sy + (dy if rng.random() < 0.5 else -dy), 0, h - 1))
+        dst = dims.idx3(tx, ty, int(rng.integers(0, layers)))
+        if not free[dst] or dst == src:
+            continue
+        nets.append(NetEndpoints(f"s{len(nets)}", src, dst))
+    wins = [_net_window(dims, nt) for nt in nets]
+    meta = {"workload": f"snapshot negotiation {w}x{h}x{layers}, {n_nets} nets", "seed": seed,
+            "edge_price": "10 + Geom(p=0.5) per undirected planar edge, Geom support {0,1,...}",
+            "keepouts": f"rectangles 8-64 cells a side, {blocked_frac:.0%} of cells", "via": via_cost,
+            "manhattan": f"LogNormal(ln {median:g}, sigma {sigma:g}) clamped [8, w+h-2]", "windows": "net_window"}
+    return Workload("snapshot", grid, nets, wins, np.full(w - 1, 10, np.uint32), np.full(h - 1, 10, np.uint32),
+                    [via_cost] * (layers - 1), d.reshape(-1), meta)

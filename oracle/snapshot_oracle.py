@@ -1,0 +1,135 @@
+"""CPU restatement of one snapshot negotiation round (the checker of
+mrc_negotiation_round).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/ as the checker; the product never
+imports it.
+
+The round is the reference's Jacobi negotiation iteration
+(crates/mr-cpu/src/negotiated.rs:1610-1991) with occupancy and history kept
+per directed planar edge slot (the generalisation the engine implements; the
+reference counts cells):
+
+* dirty set (:1632-1642): round 0 every net; later, every net with no path or
+  whose path uses an edge that two or more nets used after the previous round;
+* rip-up of the dirty nets' old paths (:1771-1790);
+* frozen snapshot price per slot: base == MAX ? MAX
+  : min(base + history + pfac * present_weight * present, MAX - 1), with
+  pfac = 1 + round (priced_with_base :2768-2795, passable_search_cost
+  :1171-1173);
+* each dirty net routed alone on the snapshot by the oracle's astar_buf
+  (window, then the full board: :1720-1760);
+* merge in net-index order (:1771-1812), then history += history_step on every
+  slot whose count is >= 2 (the group overuse scan and history bump,
+  :1923-1948, on edges).
+
+Slots per cell are (-y, -x, +x, +y) in-edges; an undirected edge {a, b} counts
+at b's slot "from a" and at a's slot "from b".
+"""
+from __future__ import annotations
+
+from typing import List, Optional
+
+import numpy as np
+
+from mrcuda.types import COST_MAX, IsolatedRouteRequest
+
+CAP = COST_MAX - 1
+
+
+def edge_slots(path: List[int], w: int, plane: int):
+    """(cells, slots) arrays of both slots of every planar step of a path."""
+    if not path or len(path) < 2:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    p = np.asarray(path, dtype=np.int64)
+    a, b = p[:-1], p[1:]
+    same = (a // plane) == (b // plane)
+    d = b - a
+    cells, slots = [], []
+    for delta, sb, sa in ((1, 1, 2), (-1, 2, 1), (w, 0, 3), (-w, 3, 0)):
+        m = same & (d == delta)
+        if delta == 1:
+            m &= (a % plane) % w + 1 < w
+        elif delta == -1:
+            m &= (a % plane) % w > 0
+        cells += [b[m], a[m]]
+        slots += [np.full(int(m.sum()), sb), np.full(int(m.sum()), sa)]
+    return np.concatenate(cells), np.concatenate(slots)
+
+
+def base_prices(req: IsolatedRouteRequest) -> np.ndarray:
+    """Base in-prices (cells, 4): the directed plane, or the per-axis prices."""
+    dims = req.grid.dims
+    n = len(dims)
+    if req.directed_in_costs is not None:
+        return np.asarray(req.directed_in_costs, dtype=np.uint32).reshape(n, 4).copy()
+    x = np.asarray(req.x_edge_costs, dtype=np.uint32)
+    y = np.asarray(req.y_edge_costs, dtype=np.uint32)
+    out = np.full((dims.layers, dims.h, dims.w, 4), COST_MAX, dtype=np.uint32)
+    if dims.h > 1:
+        out[:, 1:, :, 0] = y[:, None]
+        out[:, :-1, :, 3] = y[:, None]
+    if dims.w > 1:
+        out[:, :, 1:, 1] = x[None, :]
+        out[:, :, :-1, 2] = x[None, :]
+    return out.reshape(n, 4)
+
+
+class SnapshotNegotiation:
+    def __init__(self, oracle, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1,
+                 threads: int = 0):
+        self.o = oracle
+        self.req = req
+        self.dims = req.grid.dims
+        self.weight = int(present_weight)
+        self.step = int(history_step)
+        self.threads = threads
+        n = len(self.dims)
+        self.base = base_prices(req)
+        self.present = np.zeros((n, 4), dtype=np.uint32)
+        self.history = np.zeros((n, 4), dtype=np.uint32)
+        self.snapshot = None
+        self.paths: List[Optional[List[int]]] = [None] * len(req.nets)
+        self.dirty = list(range(len(req.nets)))
+        self.round_no = 0
+
+    def _apply(self, path, delta: int):
+        c, s = edge_slots(path or [], self.dims.w, self.dims.plane)
+        if c.size:
+            (np.add if delta > 0 else np.subtract).at(self.present, (c, s), np.uint32(1))
+
+    def round(self) -> dict:
+        pfac = 1 + self.round_no
+        dirty = self.dirty
+        stats = {"round": self.round_no, "pfac": pfac, "dirty": len(dirty)}
+        if not dirty:
+            return stats
+        for i in dirty:
+            self._apply(self.paths[i], -1)
+        b = self.base.astype(np.uint64)
+        price = b + self.history.astype(np.uint64) + np.uint64(pfac * self.weight) * self.present.astype(np.uint64)
+        snap = np.minimum(price, np.uint64(CAP)).astype(np.uint32)
+        snap[self.base == COST_MAX] = COST_MAX
+        self.snapshot = snap
+        r = self.req
+        sub = IsolatedRouteRequest(r.grid, [r.nets[i] for i in dirty], [r.windows[i] for i in dirty],
+                                   r.x_edge_costs, r.y_edge_costs, r.via_edge_costs, snap.reshape(-1))
+        new_paths, _ = self.o.isolated_batch(sub, retry_full=True, mode="astar", threads=self.threads)
+        for i, p in zip(dirty, new_paths):  # merge in net-index order
+            self.paths[i] = p
+            self._apply(p, +1)
+        over = self.present >= 2
+        h = self.history.astype(np.uint64) + over.astype(np.uint64) * np.uint64(self.step)
+        self.history = np.minimum(h, np.uint64(COST_MAX)).astype(np.uint32)
+        nxt = []
+        for i, p in enumerate(self.paths):
+            if not p:
+                nxt.append(i)
+                continue
+            c, s = edge_slots(p, self.dims.w, self.dims.plane)
+            if c.size and bool((self.present[c, s] >= 2).any()):
+                nxt.append(i)
+        self.dirty = nxt
+        stats.update(routed=sum(1 for i in dirty if self.paths[i]), overused_edges=int(over.sum()) // 2,
+                     next_dirty=len(nxt))
+        self.round_no += 1
+        return stats

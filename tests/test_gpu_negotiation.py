@@ -1,0 +1,103 @@
+"""Snapshot negotiation rounds on the device vs the CPU snapshot oracle.
+
+Every round must agree exactly: the dirty set, every net's path, the price
+snapshot, the per-edge occupancy and history, and the round statistics.
+"""
+import numpy as np
+import pytest
+
+import mrcuda
+from mrcuda import workloads as W
+from mrcuda.types import Dims, Grid, IsolatedRouteRequest, IsolatedRouteWindow, NetEndpoints
+
+from snapshot_oracle import SnapshotNegotiation
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = mrcuda.Engine(0)
+    yield e
+    e.close()
+
+
+def _run_both(engine, oracle, req, rounds, weight=16, step=1, check_arrays=True):
+    dev = engine.negotiation(req, present_weight=weight, history_step=step)
+    cpu = SnapshotNegotiation(oracle, req, present_weight=weight, history_step=step)
+    history = []
+    for r in range(rounds):
+        a = dev.round()
+        b = cpu.round()
+        assert a["dirty"] == b["dirty"], (r, a, b)
+        if not b["dirty"]:
+            break
+        for k in ("pfac", "routed", "overused_edges", "next_dirty"):
+            assert a[k] == b[k], (r, k, a, b)
+        assert dev.paths() == cpu.paths, r
+        assert dev.dirty() == cpu.dirty, r
+        if check_arrays:
+            present, hist, snap = dev.read()
+            np.testing.assert_array_equal(present, cpu.present, err_msg=f"present, round {r}")
+            np.testing.assert_array_equal(hist, cpu.history, err_msg=f"history, round {r}")
+            np.testing.assert_array_equal(snap, cpu.snapshot, err_msg=f"snapshot, round {r}")
+        history.append(a)
+    dev.close()
+    return history
+
+
+def test_rounds_match_the_oracle_on_a_congested_board(engine, oracle):
+    wl = W.snapshot_board(w=160, h=128, layers=3, n_nets=80, median=60)
+    hist = _run_both(engine, oracle, wl.request(), rounds=8)
+    assert hist[0]["overused_edges"] > 0 and hist[-1]["dirty"] < hist[0]["dirty"]
+    assert all(h["round_ms"] > 0 for h in hist)
+
+
+def test_axis_prices_own_pads_and_other_weights(engine, oracle):
+    """Base prices from the per-axis vectors, obstacles, own pads, a zero
+    history step and a large congestion weight."""
+    wl = W.plain_board(seed=21, w=96, h=80, layers=2, n_nets=40)
+    req = wl.request()
+    rng = np.random.default_rng(5)
+    nets = []
+    for nt in req.nets:
+        pads = sorted({int(c) for c in rng.integers(0, len(req.grid.dims), 2)})
+        nets.append(NetEndpoints(nt.net, nt.src, nt.dst, pads))
+    req = IsolatedRouteRequest(req.grid, nets, [mrcuda.net_windows(req.grid.dims, [n])[0] for n in nets],
+                               rng.integers(1, 20, 95).astype(np.uint32), rng.integers(1, 20, 79).astype(np.uint32),
+                               [7])
+    _run_both(engine, oracle, req, rounds=5, weight=200, step=0)
+    _run_both(engine, oracle, req, rounds=5, weight=1, step=5)
+
+
+def test_windows_that_need_the_retry(engine, oracle):
+    """Tight windows around a wall: the retry runs on the snapshot board."""
+    dims = Dims(40, 20, 2)
+    cost = np.ones((2, 20, 40), np.uint32)
+    cost[:, 0:18, 20] = 0xFFFFFFFF
+    grid = Grid(dims, cost.reshape(-1))
+    nets = [NetEndpoints(f"w{i}", dims.idx3(2 + i, 2 + i, 0), dims.idx3(37 - i, 3 + i, i % 2)) for i in range(8)]
+    wins = [IsolatedRouteWindow(0, 0, 39, 12)] * len(nets)
+    req = IsolatedRouteRequest(grid, nets, wins, [10] * 39, [10] * 19, [30])
+    hist = _run_both(engine, oracle, req, rounds=6)
+    assert hist[0]["retried"] == len(nets)
+
+
+def test_converged_rounds_do_nothing(engine, oracle):
+    dims = Dims(30, 30, 1)
+    grid = Grid.filled(dims, 1)
+    nets = [NetEndpoints("a", dims.idx(1, 1), dims.idx(10, 1)), NetEndpoints("b", dims.idx(1, 20), dims.idx(10, 20))]
+    req = IsolatedRouteRequest(grid, nets, [IsolatedRouteWindow.full(dims)] * 2, [10] * 29, [10] * 29, [])
+    neg = engine.negotiation(req)
+    first = neg.round()
+    assert first["dirty"] == 2 and first["overused_edges"] == 0 and first["next_dirty"] == 0
+    paths = neg.paths()
+    again = neg.round()
+    assert again["dirty"] == 0 and neg.paths() == paths
+    neg.close()
+
+
+def test_medium_board_rounds(engine, oracle):
+    """512x512x4, 300 nets, 4 rounds: paths, statistics and arrays."""
+    wl = W.snapshot_board(seed=8, w=512, h=512, layers=4, n_nets=300, median=120)
+    _run_both(engine, oracle, wl.request(), rounds=4)

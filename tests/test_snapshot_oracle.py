@@ -1,0 +1,78 @@
+"""CPU checks of the snapshot negotiation oracle (no GPU).
+
+The oracle's round is pinned here by hand-checkable boards: slot bookkeeping,
+a corridor two nets must share (overuse can never clear, so history grows by
+one step per round on exactly the corridor edges), a detour that negotiation
+finds, and the occupancy invariant (present == recount of the current paths).
+"""
+import numpy as np
+
+from mrcuda import workloads as W
+from mrcuda.types import COST_MAX, Dims, Grid, IsolatedRouteRequest, IsolatedRouteWindow, NetEndpoints
+
+from snapshot_oracle import SnapshotNegotiation, base_prices, edge_slots
+
+
+def _recount(neg):
+    cnt = np.zeros_like(neg.present)
+    for p in neg.paths:
+        c, s = edge_slots(p or [], neg.dims.w, neg.dims.plane)
+        np.add.at(cnt, (c, s), 1)
+    return cnt
+
+
+def test_edge_slots_of_a_path():
+    dims = Dims(4, 3, 2)
+    # (0,0,0) -> (1,0,0) -> (1,1,0) -> via -> (1,1,1) -> (0,1,1)
+    p = [dims.idx3(0, 0, 0), dims.idx3(1, 0, 0), dims.idx3(1, 1, 0), dims.idx3(1, 1, 1), dims.idx3(0, 1, 1)]
+    c, s = edge_slots(p, dims.w, dims.plane)
+    got = sorted(zip(c.tolist(), s.tolist()))
+    exp = sorted([(p[1], 1), (p[0], 2),      # +x step: b from -x, a from +x
+                  (p[2], 0), (p[1], 3),      # +y step: b from -y, a from +y
+                  (p[4], 2), (p[3], 1)])     # -x step: b from +x, a from -x
+    assert got == exp
+
+
+def test_base_prices_from_axis_vectors():
+    dims = Dims(3, 2, 1)
+    req = IsolatedRouteRequest(Grid.filled(dims, 1), [], [], [5, 6], [7], [])
+    b = base_prices(req).reshape(2, 3, 4)
+    assert b[0, 1].tolist() == [COST_MAX, 5, 6, 7]
+    assert b[1, 2].tolist() == [7, 6, COST_MAX, COST_MAX]
+
+
+def test_shared_corridor_accumulates_history(oracle):
+    """A one-cell-wide corridor both nets must use: every round both nets are
+    dirty again and each corridor edge gains exactly one history step."""
+    dims = Dims(9, 5, 1)
+    cost = np.full((5, 9), COST_MAX, np.uint32)
+    cost[:, 0] = 1
+    cost[:, 8] = 1
+    cost[2, :] = 1  # corridor along y = 2
+    grid = Grid(dims, cost.reshape(-1))
+    nets = [NetEndpoints("a", dims.idx(0, 0), dims.idx(8, 0)), NetEndpoints("b", dims.idx(0, 4), dims.idx(8, 4))]
+    req = IsolatedRouteRequest(grid, nets, [IsolatedRouteWindow.full(dims)] * 2, [10] * 8, [10] * 4, [])
+    neg = SnapshotNegotiation(oracle, req, history_step=3)
+    for r in range(4):
+        st = neg.round()
+        assert st["dirty"] == 2 and st["routed"] == 2 and st["next_dirty"] == 2
+        assert st["overused_edges"] == 8  # the 8 corridor edges
+        np.testing.assert_array_equal(neg.present, _recount(neg))
+        corridor = [dims.idx(x, 2) for x in range(1, 9)]
+        assert (neg.history[corridor, 1] == 3 * (r + 1)).all()
+
+
+def test_negotiation_spreads_nets_and_keeps_the_invariant(oracle):
+    wl = W.snapshot_board(w=120, h=96, layers=2, n_nets=50, median=50)
+    neg = SnapshotNegotiation(oracle, wl.request())
+    first = neg.round()
+    assert first["overused_edges"] > 0
+    np.testing.assert_array_equal(neg.present, _recount(neg))
+    for _ in range(6):
+        st = neg.round()
+        np.testing.assert_array_equal(neg.present, _recount(neg))
+        if not st["dirty"]:
+            break
+    assert st.get("overused_edges", 0) < first["overused_edges"]
+    # the snapshot never prices a blocked base edge
+    assert (neg.snapshot[neg.base == COST_MAX] == COST_MAX).all()
