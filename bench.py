@@ -458,13 +458,107 @@ def run_snapshot(args):
     return 0
 
 
+def _run_trace(eng, trace, slots, max_batch):
+    """Replays a Poisson trace through a server; returns (latencies ms, nets,
+    makespan s, server stats).  Arrivals are submitted on their own thread at
+    their trace times; latency is the server's submit -> result time."""
+    import threading
+
+    srv = eng.server(slots=slots, max_batch_requests=max_batch)
+    for _, wl in trace[:3]:  # warm-up
+        srv.wait(srv.submit(wl.request()))
+    reqs = [(t, wl.request()) for t, wl in trace]
+    tickets = [None] * len(reqs)
+    ready = threading.Semaphore(0)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for i, (t, rq) in enumerate(reqs):
+            d = t0 + t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(rq)
+            ready.release()
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    lat, nets = [], 0
+    for i in range(len(reqs)):
+        ready.acquire()
+        res, info = srv.wait(tickets[i])
+        lat.append(info["total_ms"])
+        nets += len(res.paths)
+    makespan = time.perf_counter() - t0
+    th.join()
+    st = srv.stats()
+    srv.close()
+    return lat, nets, makespan, st
+
+
+def run_serving(args):
+    """Serving: Poisson arrivals of congestion-style boards (side log-uniform
+    64-1024, 2-6 layers, 16-512 nets) at several rates through the
+    continuous-batching server and through a one-request-at-a-time loop (the
+    same server with one launch of one request at a time)."""
+    import numpy as np
+    import torch
+
+    import mrcuda
+    from mrcuda import workloads as W
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return 0
+    pool = W.serving_pool(n_boards=16)
+    eng = mrcuda.Engine(local)
+    rates = [float(r) for r in args.rates.split(",")]
+    rows = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for rate in rates:
+        n = max(20, min(int(rate * args.serve_seconds), args.serve_max))
+        trace = W.serving_trace(pool, rate, n, seed=int(rate))
+        row = {"rate_req_s": rate, "requests": n}
+        for name, slots, mb in (("batched", args.slots, 64), ("one_at_a_time", 1, 1)):
+            lat, nets, span, st = _run_trace(eng, trace, slots, mb)
+            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "nets_per_s": nets / span, "req_per_s": n / span, "launches": st["launches"],
+                         "largest_launch": st["largest_launch"], "peak_gb": st["peak_bytes"] / 1e9}
+        rows.append(row)
+    clk = clocks.stop()
+    top = rows[-1]["batched"]
+    line = {
+        "metric": METRIC, "value": top["nets_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(rates),
+        "warmup": 3, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "serving: Poisson arrivals, boards side log-uniform 64-1024, 2-6 layers, "
+                               "16-512 nets (log-uniform), generated as the congestion board",
+                   "slots": args.slots, "hbm_budget": 0.8, "rates": rows},
+        "e2e": {"value": top["nets_per_s"], "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "every request goes through the public submit/wait calls with host buffers"},
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+        "vs_one_at_a_time": top["nets_per_s"] / max(rows[-1]["one_at_a_time"]["nets_per_s"], 1e-9),
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["congestion", "plain", "uneven", "snapshot"], default="congestion")
+    ap.add_argument("--workload", choices=["congestion", "plain", "uneven", "snapshot", "serving"],
+                    default="congestion")
+    ap.add_argument("--rates", default="20,50,100,200,400", help="serving: offered request rates (req/s)")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: seconds of arrivals per rate")
+    ap.add_argument("--serve-max", type=int, default=600, help="serving: most requests per rate")
+    ap.add_argument("--slots", type=int, default=2, help="serving: launches in flight")
     ap.add_argument("--nets", type=int, default=0, help="route only the first N nets (0 = all)")
     ap.add_argument("--cpu-sample", type=int, default=0, help="nets timed on the CPU (0 = workload default)")
     ap.add_argument("--plain-sample", type=int, default=0, help="nets timed one per launch (0 = workload default)")
@@ -477,6 +571,8 @@ def main():
         return run_reference(args)
     if args.workload == "snapshot":
         return run_snapshot(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_engine(args)
 
 

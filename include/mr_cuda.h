@@ -336,6 +336,63 @@ mrc_status mrc_negotiation_read(mrc_context *ctx, mrc_negotiation *neg, uint32_t
 mrc_status mrc_negotiation_dirty(const mrc_negotiation *neg, uint32_t *n, const uint32_t **nets);
 void mrc_negotiation_destroy(mrc_negotiation *neg);
 
+/* ---- serving: continuous batching behind the /solve seam --------------------- */
+
+/* A request loop in front of the engine, for the reference's /solve route
+ * (crates/mr-server/src/lib.rs:381-448, one synchronous solve per request on a
+ * worker thread, no batching or admission).  Requests are submitted from any
+ * thread and return at once with a ticket; one dispatcher thread
+ *   - admits queued requests in arrival order while the device memory they
+ *     need (boards, labels, paths, tile state) fits the HBM budget
+ *     (hbm_fraction of the device's memory, minus what was in use at creation),
+ *   - merges every admitted request with the same flags, up to
+ *     max_batch_requests / max_batch_cells, into ONE persistent launch over
+ *     all of their boards (each request's board is uploaded into HBM and stays
+ *     there while it is solved),
+ *   - keeps up to `slots` such launches in flight on separate streams, each
+ *     with 1/slots of the co-resident grid, so requests that arrive while
+ *     others run are staged and launched beside them instead of queueing
+ *     behind them,
+ *   - reaps finished launches (with each request's full-board retry) and hands
+ *     every request its own result.
+ * A request's result is identical to mrc_route_isolated_batch on the same
+ * request alone (bit for bit).  This entry point has no counterpart in the
+ * reference. */
+typedef struct mrc_server mrc_server;
+
+typedef struct {
+    float hbm_fraction;           /* admission budget, fraction of device memory (0.8) */
+    uint32_t slots;               /* launches in flight at once (>= 1) */
+    uint32_t max_batch_requests;  /* requests merged into one launch (>= 1) */
+    uint64_t max_batch_cells;     /* window cells per launch (0 = no limit) */
+    uint32_t max_layers;          /* largest layer count accepted (sizes the tile; <= 12) */
+} mrc_server_params;
+
+typedef struct {
+    double queue_ms;              /* submit -> staged for launch */
+    double run_ms;                /* launch -> results on the host */
+    double total_ms;              /* submit -> results on the host */
+    uint32_t batch_requests;      /* requests that shared its launch */
+    uint32_t status;              /* mrc_status of this request */
+    uint64_t batch_id;
+} mrc_request_info;
+
+mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, mrc_server **out);
+/* Validates the request and queues it.  The request's arrays (grid, edges,
+ * nets, pads, windows) are BORROWED: they must stay valid and unchanged until
+ * mrc_server_wait for this ticket has returned.  Flags: RETRY_FULL, KEEP_FIELDS. */
+mrc_status mrc_server_submit(mrc_server *srv, const mrc_isolated_request *req, uint32_t flags, uint64_t *ticket);
+/* Waits up to timeout_ms (0 = forever) for a ticket; on success hands over its
+ * result (free with mrc_result_free).  MRC_ERR_BUSY = still running at the
+ * timeout (the ticket stays valid); any other error is the request's own. */
+mrc_status mrc_server_wait(mrc_server *srv, uint64_t ticket, uint32_t timeout_ms, mrc_result **out,
+                           mrc_request_info *info);
+/* out[0..7]: submitted, completed, failed, launches, largest launch (requests),
+ * peak in-flight bytes, budget bytes, queued now. */
+mrc_status mrc_server_stats(mrc_server *srv, uint64_t out[8]);
+/* Finishes everything queued and in flight, then stops the dispatcher. */
+void mrc_server_destroy(mrc_server *srv);
+
 /* net_window (negotiated.rs:568-594) for a batch of nets. */
 mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
                            mrc_window *out);

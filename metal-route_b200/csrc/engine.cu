@@ -10,7 +10,10 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -522,6 +525,11 @@ struct mrc_batch {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;  // captured launch sequence (mrc_batch_capture_graph)
+    // Set before batch_build by callers that run several batches at once: a
+    // fixed tile configuration, a shared-memory floor (every concurrent batch
+    // has the same per-CTA footprint) and a divisor of the co-resident grid.
+    uint32_t force_tile_h = 0, force_threads = 0, grid_div = 1;
+    size_t smem_floor = 0;
     ~mrc_batch() {
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
@@ -562,7 +570,7 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     }
     bt->tile_h = tile_h;
     bt->threads = threads;
-    bt->smem = relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any);
+    bt->smem = std::max(relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any), bt->smem_floor);
     uint64_t toff = 0;
     uint32_t max_tiles = 1;
     for (DevField &f : bt->fields) {
@@ -579,7 +587,7 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
-    bt->grid = (uint32_t)ctx->sms * (uint32_t)per_sm;
+    bt->grid = std::max(1u, (uint32_t)ctx->sms * (uint32_t)per_sm / std::max(1u, bt->grid_div));
     MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
     MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
     MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
@@ -604,7 +612,10 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
     uint32_t tile_h = 0, threads = kRelaxThreads;
     size_t smem = 0;
     auto tuned = ctx->tuned.find(tune_key(bt->max_layers, bt->directed_any));
-    if (tuned != ctx->tuned.end()) {
+    if (bt->force_tile_h) {
+        tile_h = bt->force_tile_h;
+        threads = bt->force_threads ? bt->force_threads : kRelaxThreads;
+    } else if (tuned != ctx->tuned.end()) {
         tile_h = tuned->second.first;
         threads = tuned->second.second;
     } else {
@@ -772,11 +783,12 @@ mrc_status batch_collect(mrc_batch *bt, bool keep_fields, std::vector<uint32_t> 
     return MRC_OK;
 }
 
+mrc_status finish_batch(mrc_context *ctx, mrc_batch *bt, uint32_t flags, mrc_result **out);
+
 // Run a batch synchronously and, with MRC_FLAG_RETRY_FULL, re-solve on its full
 // board every net whose window solve was unreachable (cli/src/lib.rs:574-607).
 mrc_status solve(mrc_context *ctx, std::vector<const mrc_board *> boards, std::vector<NetCopy> nets,
                  std::vector<mrc_window> wins, uint32_t flags, mrc_result **out, mrc_batch *prepared) {
-    const bool keep = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
     std::unique_ptr<mrc_batch> own;
     mrc_batch *bt = prepared;
     if (!bt) {
@@ -785,6 +797,12 @@ mrc_status solve(mrc_context *ctx, std::vector<const mrc_board *> boards, std::v
         MRC_TRY(batch_build(ctx, std::move(boards), std::move(nets), std::move(wins), flags, bt));
         MRC_TRY(batch_launch(bt, ctx->stream));
     }
+    return finish_batch(ctx, bt, flags, out);
+}
+
+// Results of a launched batch (waits for it), with the full-board retry.
+mrc_status finish_batch(mrc_context *ctx, mrc_batch *bt, uint32_t flags, mrc_result **out) {
+    const bool keep = (flags & MRC_FLAG_KEEP_FIELDS) != 0;
     std::vector<uint32_t> costs;
     std::vector<std::vector<uint32_t>> paths, fields;
     MRC_TRY(batch_collect(bt, keep, &costs, &paths, &fields));
@@ -808,7 +826,8 @@ mrc_status solve(mrc_context *ctx, std::vector<const mrc_board *> boards, std::v
             }
             mrc_batch retry;
             MRC_TRY(batch_build(ctx, bt->boards, std::move(rn), std::move(rw), flags & ~MRC_FLAG_TIME_KERNELS, &retry));
-            MRC_TRY(batch_launch(&retry, bt->stream ? bt->stream : ctx->stream));
+            // on the engine stream, behind the retry batch's own uploads
+            MRC_TRY(batch_launch(&retry, ctx->stream));
             std::vector<uint32_t> c2;
             std::vector<std::vector<uint32_t>> p2, f2;
             MRC_TRY(batch_collect(&retry, keep, &c2, &p2, &f2));
@@ -1540,6 +1559,445 @@ void mrc_negotiation_destroy(mrc_negotiation *ng) {
     } else {
         delete ng;
     }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving: a dispatcher thread that admits requests by device-memory footprint,
+// merges them into multi-board launches and keeps several launches in flight.
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct ServerRequest {
+    uint64_t ticket = 0;
+    uint32_t flags = 0;
+    mrc_isolated_request req{};   // borrowed arrays
+    mrc_grid grid{};
+    std::vector<NetCopy> nets;
+    std::vector<mrc_window> windows;
+    uint64_t cells = 0;           // window cells of all nets
+    size_t footprint = 0;         // device bytes while in flight
+    Clock::time_point t_submit, t_stage, t_done;
+    bool done = false;
+    mrc_status status = MRC_OK;
+    std::string error;
+    std::unique_ptr<mrc_result> result;
+    uint32_t batch_requests = 0;
+    uint64_t batch_id = 0;
+};
+
+struct ServerBatch {
+    uint64_t id = 0;
+    mrc_server *srv = nullptr;
+    std::vector<std::shared_ptr<ServerRequest>> reqs;
+    BoardPack pack;
+    std::unique_ptr<mrc_batch> bt;
+    uint32_t slot = 0, flags = 0;
+    size_t footprint = 0;
+    bool finished = false;        // set by the stream callback (under the server mutex)
+};
+
+}  // namespace
+
+struct mrc_server {
+    mrc_context *ctx = nullptr;
+    mrc_server_params p{};
+    std::mutex mu;
+    std::condition_variable cv;       // dispatcher wake-ups
+    std::condition_variable cv_done;  // waiters
+    std::deque<std::shared_ptr<ServerRequest>> queue;
+    std::unordered_map<uint64_t, std::shared_ptr<ServerRequest>> tickets;
+    std::vector<std::unique_ptr<ServerBatch>> inflight;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> staged;
+    std::vector<bool> slot_busy;
+    size_t budget = 0, inflight_bytes = 0, peak_bytes = 0, smem_floor = 0;
+    uint32_t tile_h = 8, threads = kRelaxThreads;
+    uint64_t next_ticket = 1, next_batch = 1;
+    uint64_t submitted = 0, completed = 0, failed = 0, launches = 0, largest = 0;
+    bool stop = false, wake = false;
+    std::thread th;
+};
+
+namespace {
+
+// Device bytes a request holds while in flight (board + per-net state).
+size_t request_footprint(const ServerRequest &r, uint32_t tile_h) {
+    auto al = [](size_t b) { return (std::max<size_t>(b, 4) + 255) & ~(size_t)255; };
+    const GridView g{r.grid.w, r.grid.h, r.grid.layers ? r.grid.layers : 1u,
+                     (uint64_t)r.grid.w * r.grid.h * (r.grid.layers ? r.grid.layers : 1u)};
+    size_t b = al(g.n * 4) + al((size_t)g.w * 4) + al((size_t)g.h * 4) + al(128);
+    if (r.grid.board_constraint || r.grid.via_forbidden) b += al(g.n);
+    if (r.req.edges.directed_in_costs) b += al(g.n * 16);
+    const bool keep = (r.flags & MRC_FLAG_KEEP_FIELDS) != 0;
+    for (size_t i = 0; i < r.nets.size(); ++i) {
+        const mrc_window &w = r.windows[i];
+        const uint64_t ww = w.x1 - w.x0 + 1, wh = w.y1 - w.y0 + 1;
+        const uint64_t cells = ww * wh * g.layers;
+        const uint64_t tiles = ((ww + 31) / 32) * ((wh + tile_h - 1) / tile_h);
+        b += cells * (8 + 4 + (keep ? 4 : 0)) + tiles * (4 + 4 + 24) + sizeof(DevField) + 32 +
+             4 * (r.nets[i].pads.size() + r.nets[i].vpads.size());
+    }
+    return b + (1u << 20);
+}
+
+mrc_status server_validate(mrc_server *s, const mrc_isolated_request *req, ServerRequest *r) {
+    if (!req) return fail(MRC_ERR_INVALID_ARGUMENT, "request is NULL");
+    GridView g;
+    MRC_TRY(view_grid(req->grid, &g));
+    if (g.layers > s->p.max_layers) return fail(MRC_ERR_LIMIT, "request has more layers than the server accepts");
+    const mrc_edges &e = req->edges;
+    const uint32_t ex = g.w ? g.w - 1 : 0, ey = g.h ? g.h - 1 : 0, ev = g.layers - 1;
+    if (e.n_x_edge_costs != ex || e.n_y_edge_costs != ey || e.n_via_edge_costs != ev)
+        return fail(MRC_ERR_INVALID_ARGUMENT, "isolated batch shape does not match grid/nets");
+    if ((ex && !e.x_edge_costs) || (ey && !e.y_edge_costs) || (ev && (!e.via_edge_costs || !e.via_allowed)))
+        return fail(MRC_ERR_INVALID_ARGUMENT, "edge price pointer is NULL");
+    MRC_TRY(validate_nets(g, req->nets, req->n_nets, &r->nets));
+    MRC_TRY(collect_windows(g, r->nets, req->windows, &r->windows));
+    r->req = *req;
+    r->grid = *req->grid;
+    r->req.grid = &r->grid;
+    for (const mrc_window &w : r->windows) r->cells += (uint64_t)(w.x1 - w.x0 + 1) * (w.y1 - w.y0 + 1) * g.layers;
+    r->footprint = request_footprint(*r, s->tile_h);
+    return MRC_OK;
+}
+
+void CUDART_CB server_on_done(void *p) {
+    ServerBatch *b = static_cast<ServerBatch *>(p);
+    mrc_server *s = b->srv;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        b->finished = true;
+        s->wake = true;
+    }
+    s->cv.notify_all();
+}
+
+// Stage every request of the batch (one packed board upload, one batch) and
+// enqueue it on the slot's stream behind the staging copies.
+mrc_status server_launch(mrc_server *s, ServerBatch *b) {
+    mrc_context *ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MRC_TRY(set_device(ctx));
+    std::vector<mrc_isolated_request> inst;
+    inst.reserve(b->reqs.size());
+    for (auto &r : b->reqs) inst.push_back(r->req);
+    MRC_TRY(board_pack_build(ctx, inst.data(), (uint32_t)inst.size(), &b->pack));
+    std::vector<const mrc_board *> boards;
+    std::vector<NetCopy> nets;
+    std::vector<mrc_window> wins;
+    for (uint32_t k = 0; k < b->reqs.size(); ++k) {
+        boards.push_back(b->pack.boards[k].get());
+        for (const NetCopy &nc : b->reqs[k]->nets) {
+            nets.push_back(nc);
+            nets.back().board = k;
+        }
+        wins.insert(wins.end(), b->reqs[k]->windows.begin(), b->reqs[k]->windows.end());
+    }
+    b->bt.reset(new mrc_batch());
+    b->bt->force_tile_h = s->tile_h;
+    b->bt->force_threads = s->threads;
+    b->bt->grid_div = s->p.slots;
+    b->bt->smem_floor = s->smem_floor;
+    MRC_TRY(batch_build(ctx, std::move(boards), std::move(nets), std::move(wins), b->flags, b->bt.get()));
+    cudaStream_t st = s->streams[b->slot];
+    MRC_CUDA(cudaEventRecord(s->staged[b->slot], ctx->stream), "record staging");
+    MRC_CUDA(cudaStreamWaitEvent(st, s->staged[b->slot], 0), "wait for staging");
+    MRC_TRY(batch_launch(b->bt.get(), st));
+    MRC_CUDA(cudaLaunchHostFunc(st, server_on_done, b), "completion callback");
+    return MRC_OK;
+}
+
+// Results of one finished launch, split per request.
+void server_reap(mrc_server *s, ServerBatch *b) {
+    mrc_context *ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    mrc_result *raw = nullptr;
+    mrc_status st = set_device(ctx);
+    if (st == MRC_OK) st = finish_batch(ctx, b->bt.get(), b->flags, &raw);
+    std::unique_ptr<mrc_result> res(raw);
+    const std::string err = st == MRC_OK ? std::string() : g_err;
+    uint32_t first = 0;
+    for (auto &r : b->reqs) {
+        const uint32_t n = (uint32_t)r->nets.size();
+        r->batch_requests = (uint32_t)b->reqs.size();
+        r->batch_id = b->id;
+        if (st != MRC_OK) {
+            r->status = st;
+            r->error = err;
+        } else {
+            std::unique_ptr<mrc_result> o(new mrc_result());
+            o->n = n;
+            const uint64_t c0 = res->offsets[first], c1 = res->offsets[first + n];
+            o->costs.assign(res->costs.begin() + first, res->costs.begin() + first + n);
+            o->offsets.resize(n + 1);
+            for (uint32_t i = 0; i <= n; ++i) o->offsets[i] = res->offsets[first + i] - c0;
+            o->cells.assign(res->cells.begin() + c0, res->cells.begin() + c1);
+            o->field_windows.assign(res->field_windows.begin() + first, res->field_windows.begin() + first + n);
+            for (uint32_t i = 0; i < n; ++i) {
+                const mrc_window &a = r->windows[i], &w = o->field_windows[i];
+                o->retried += (a.x0 != w.x0 || a.y0 != w.y0 || a.x1 != w.x1 || a.y1 != w.y1) ? 1 : 0;
+            }
+            if (res->has_fields) {
+                o->has_fields = true;
+                const uint64_t f0 = res->field_offsets[first], f1 = res->field_offsets[first + n];
+                o->field_offsets.resize(n + 1);
+                for (uint32_t i = 0; i <= n; ++i) o->field_offsets[i] = res->field_offsets[first + i] - f0;
+                o->fields.assign(res->fields.begin() + f0, res->fields.begin() + f1);
+            }
+            r->result = std::move(o);
+        }
+        first += n;
+    }
+    // free the launch's device memory while the engine lock is held
+    b->bt.reset();
+    b->pack.boards.clear();
+    b->pack.data.reset();
+}
+
+void server_loop(mrc_server *s) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto free_slot = [&]() -> int {
+        for (uint32_t i = 0; i < s->slot_busy.size(); ++i)
+            if (!s->slot_busy[i]) return (int)i;
+        return -1;
+    };
+    for (;;) {
+        s->cv.wait(lk, [&] {
+            if (s->stop || s->wake) return true;
+            if (s->queue.empty() || free_slot() < 0) return false;
+            return s->inflight.empty() || s->inflight_bytes + s->queue.front()->footprint <= s->budget;
+        });
+        s->wake = false;
+        // ---- reap finished launches ----------------------------------------
+        std::vector<std::unique_ptr<ServerBatch>> done;
+        for (auto it = s->inflight.begin(); it != s->inflight.end();) {
+            if ((*it)->finished) {
+                done.push_back(std::move(*it));
+                it = s->inflight.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        if (!done.empty()) {
+            lk.unlock();
+            for (auto &b : done) server_reap(s, b.get());
+            lk.lock();
+            const auto now = Clock::now();
+            for (auto &b : done) {
+                s->inflight_bytes -= b->footprint;
+                s->slot_busy[b->slot] = false;
+                for (auto &r : b->reqs) {
+                    r->t_done = now;
+                    r->done = true;
+                    if (r->status == MRC_OK) s->completed++;
+                    else s->failed++;
+                }
+            }
+            s->cv_done.notify_all();
+            done.clear();
+        }
+        // ---- admit queued requests into new launches -------------------------
+        while (!s->queue.empty()) {
+            const int slot = free_slot();
+            if (slot < 0) break;
+            std::shared_ptr<ServerRequest> head = s->queue.front();
+            if (head->footprint > s->budget) {  // can never fit
+                s->queue.pop_front();
+                head->status = MRC_ERR_LIMIT;
+                head->error = "request needs more device memory than the admission budget";
+                head->t_stage = head->t_done = Clock::now();
+                head->done = true;
+                s->failed++;
+                s->cv_done.notify_all();
+                continue;
+            }
+            if (s->inflight_bytes + head->footprint > s->budget) break;  // wait for a launch to finish
+            std::unique_ptr<ServerBatch> b(new ServerBatch());
+            b->id = s->next_batch++;
+            b->srv = s;
+            b->slot = (uint32_t)slot;
+            b->flags = head->flags;
+            uint64_t cells = 0;
+            const auto now = Clock::now();
+            while (!s->queue.empty() && b->reqs.size() < s->p.max_batch_requests) {
+                std::shared_ptr<ServerRequest> r = s->queue.front();
+                if (r->flags != b->flags) break;
+                if (!b->reqs.empty() && s->p.max_batch_cells && cells + r->cells > s->p.max_batch_cells) break;
+                if (s->inflight_bytes + b->footprint + r->footprint > s->budget) break;
+                s->queue.pop_front();
+                r->t_stage = now;
+                cells += r->cells;
+                b->footprint += r->footprint;
+                b->reqs.push_back(std::move(r));
+            }
+            s->inflight_bytes += b->footprint;
+            s->peak_bytes = std::max(s->peak_bytes, s->inflight_bytes);
+            s->slot_busy[slot] = true;
+            s->launches++;
+            s->largest = std::max<uint64_t>(s->largest, b->reqs.size());
+            ServerBatch *raw = b.get();
+            s->inflight.push_back(std::move(b));
+            lk.unlock();
+            const mrc_status st = server_launch(s, raw);
+            const std::string err = st == MRC_OK ? std::string() : g_err;
+            if (st != MRC_OK) {
+                std::lock_guard<std::mutex> g(s->ctx->mu);
+                raw->bt.reset();
+                raw->pack.boards.clear();
+                raw->pack.data.reset();
+            }
+            lk.lock();
+            if (st != MRC_OK) {
+                for (auto it = s->inflight.begin(); it != s->inflight.end(); ++it) {
+                    if (it->get() != raw) continue;
+                    s->inflight_bytes -= raw->footprint;
+                    s->slot_busy[raw->slot] = false;
+                    for (auto &r : raw->reqs) {
+                        r->status = st;
+                        r->error = err;
+                        r->t_done = Clock::now();
+                        r->done = true;
+                        s->failed++;
+                    }
+                    s->inflight.erase(it);
+                    break;
+                }
+                s->cv_done.notify_all();
+            }
+        }
+        if (s->stop && s->queue.empty() && s->inflight.empty()) break;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, mrc_server **out) {
+    if (!ctx || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<mrc_server> s(new mrc_server());
+    s->ctx = ctx;
+    s->p = params ? *params : mrc_server_params{0.8f, 2, 64, 0, 8};
+    if (s->p.hbm_fraction <= 0.f || s->p.hbm_fraction > 1.f) s->p.hbm_fraction = 0.8f;
+    s->p.slots = std::max(1u, std::min(s->p.slots, 8u));
+    s->p.max_batch_requests = std::max(1u, s->p.max_batch_requests);
+    if (!s->p.max_layers) s->p.max_layers = 8;
+    if (s->p.max_layers > 16) return fail(MRC_ERR_LIMIT, "a server tile holds at most 16 layers");
+    {
+        Lock lock(ctx, 0);
+        MRC_TRY(set_device(ctx));
+        ctx->pool.trim();
+        size_t free_b = 0, total_b = 0;
+        MRC_CUDA(cudaMemGetInfo(&free_b, &total_b), "device memory");
+        const double allowed = (double)s->p.hbm_fraction * (double)total_b - (double)(total_b - free_b);
+        s->budget = allowed > 0 ? (size_t)allowed : 0;
+        s->tile_h = 8;
+        s->threads = kRelaxThreads;
+        s->smem_floor = relax_smem_bytes(s->p.max_layers, s->tile_h, true);
+        int per_sm = 0;
+        MRC_CUDA(relax_configure(s->tile_h, s->threads, s->smem_floor), "configure relax kernel");
+        MRC_CUDA(relax_occupancy(s->tile_h, s->threads, s->smem_floor, &per_sm), "relax occupancy");
+        if ((uint32_t)per_sm * (uint32_t)ctx->sms < s->p.slots) return fail(MRC_ERR_LIMIT, "too many slots");
+        s->streams.resize(s->p.slots);
+        s->staged.resize(s->p.slots);
+        s->slot_busy.assign(s->p.slots, false);
+        for (uint32_t i = 0; i < s->p.slots; ++i) {
+            MRC_CUDA(cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking), "server stream");
+            MRC_CUDA(cudaEventCreateWithFlags(&s->staged[i], cudaEventDisableTiming), "server event");
+        }
+    }
+    mrc_server *raw = s.get();
+    s->th = std::thread(server_loop, raw);
+    *out = s.release();
+    return MRC_OK;
+}
+
+mrc_status mrc_server_submit(mrc_server *s, const mrc_isolated_request *req, uint32_t flags, uint64_t *ticket) {
+    if (!s || !ticket) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    auto r = std::make_shared<ServerRequest>();
+    r->flags = flags & (MRC_FLAG_RETRY_FULL | MRC_FLAG_KEEP_FIELDS);
+    MRC_TRY(server_validate(s, req, r.get()));
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (s->stop) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "server is stopping");
+        r->ticket = s->next_ticket++;
+        *ticket = r->ticket;
+        s->tickets[r->ticket] = r;
+        s->queue.push_back(r);
+        s->submitted++;
+    }
+    s->cv.notify_all();
+    return MRC_OK;
+}
+
+mrc_status mrc_server_wait(mrc_server *s, uint64_t ticket, uint32_t timeout_ms, mrc_result **out,
+                           mrc_request_info *info) {
+    if (!s || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->tickets.find(ticket);
+    if (it == s->tickets.end()) return fail(MRC_ERR_INVALID_ARGUMENT, "unknown ticket");
+    std::shared_ptr<ServerRequest> r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_ms) {
+        if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+            return fail(MRC_ERR_BUSY, "request is still queued or running");
+    } else {
+        s->cv_done.wait(lk, ready);
+    }
+    s->tickets.erase(ticket);
+    if (info) {
+        info->queue_ms = ms_between(r->t_submit, r->t_stage);
+        info->run_ms = ms_between(r->t_stage, r->t_done);
+        info->total_ms = ms_between(r->t_submit, r->t_done);
+        info->batch_requests = r->batch_requests;
+        info->status = (uint32_t)r->status;
+        info->batch_id = r->batch_id;
+    }
+    if (r->status != MRC_OK) return fail(r->status, r->error);
+    *out = r->result.release();
+    return MRC_OK;
+}
+
+mrc_status mrc_server_stats(mrc_server *s, uint64_t out[8]) {
+    if (!s || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> g(s->mu);
+    out[0] = s->submitted;
+    out[1] = s->completed;
+    out[2] = s->failed;
+    out[3] = s->launches;
+    out[4] = s->largest;
+    out[5] = s->peak_bytes;
+    out[6] = s->budget;
+    out[7] = s->queue.size();
+    return MRC_OK;
+}
+
+void mrc_server_destroy(mrc_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->th.joinable()) s->th.join();
+    {
+        std::lock_guard<std::mutex> g(s->ctx->mu);
+        cudaSetDevice(s->ctx->device);
+        for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+        for (cudaEvent_t e : s->staged) cudaEventDestroy(e);
+    }
+    delete s;
 }
 
 }  // extern "C"

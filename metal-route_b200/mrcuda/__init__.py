@@ -34,6 +34,7 @@ from .api import (  # noqa: F401
     LimitExceeded,
     MalformedGrid,
     Negotiation,
+    Server,
     OutOfMemory,
     RouterError,
     exported_symbols,

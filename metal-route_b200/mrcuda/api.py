@@ -121,6 +121,16 @@ class _RoundStats(C.Structure):
                 ("window_cells", C.c_uint64), ("path_cells", C.c_uint64), ("round_ms", C.c_float)]
 
 
+class _ServerParams(C.Structure):
+    _fields_ = [("hbm_fraction", C.c_float), ("slots", C.c_uint32), ("max_batch_requests", C.c_uint32),
+                ("max_batch_cells", C.c_uint64), ("max_layers", C.c_uint32)]
+
+
+class _RequestInfo(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double),
+                ("batch_requests", C.c_uint32), ("status", C.c_uint32), ("batch_id", C.c_uint64)]
+
+
 _lib = None
 _lib_lock = threading.Lock()
 
@@ -176,6 +186,11 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_negotiation_read": (C.c_int, [vp, vp, vp, vp, vp]),
             "mrc_negotiation_dirty": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32p)]),
             "mrc_negotiation_destroy": (None, [vp]),
+            "mrc_server_create": (C.c_int, [vp, C.POINTER(_ServerParams), C.POINTER(vp)]),
+            "mrc_server_submit": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(C.c_uint64)]),
+            "mrc_server_wait": (C.c_int, [vp, C.c_uint64, u32, C.POINTER(vp), C.POINTER(_RequestInfo)]),
+            "mrc_server_stats": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+            "mrc_server_destroy": (None, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -476,6 +491,65 @@ class Negotiation:
             pass
 
 
+class Server:
+    """Continuous-batching request loop (mrc_server_*): submit from any thread,
+    wait for each ticket; admitted requests are merged into shared launches
+    under an HBM budget with `slots` launches in flight."""
+
+    def __init__(self, engine: "Engine", hbm_fraction: float = 0.8, slots: int = 2, max_batch_requests: int = 64,
+                 max_batch_cells: int = 0, max_layers: int = 8):
+        self.engine = engine
+        h = C.c_void_p()
+        prm = _ServerParams(hbm_fraction, slots, max_batch_requests, max_batch_cells, max_layers)
+        engine._check(engine.lib.mrc_server_create(engine.ctx, C.byref(prm), C.byref(h)))
+        self.handle = h
+        self._live = {}
+        self._lock = threading.Lock()
+
+    def submit(self, req: IsolatedRouteRequest, retry_full: bool = True, keep_fields: bool = False) -> int:
+        m = _Marshal()
+        r = self.engine._request(m, req)
+        flags = (MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
+        t = C.c_uint64()
+        self.engine._check(self.engine.lib.mrc_server_submit(self.handle, C.byref(r), flags, C.byref(t)))
+        with self._lock:  # the request's arrays are borrowed until its wait returns
+            self._live[t.value] = (m, len(req.nets), keep_fields)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 0):
+        """(IsolatedBatchResult, info) of a ticket; raises the request's error."""
+        res = C.c_void_p()
+        info = _RequestInfo()
+        st = self.engine.lib.mrc_server_wait(self.handle, ticket, timeout_ms, C.byref(res), C.byref(info))
+        if st == Busy.status:
+            raise Busy("request still running")
+        with self._lock:
+            _, n, keep = self._live.pop(ticket, (None, 0, False))
+        d = {f: getattr(info, f) for f, _ in _RequestInfo._fields_}
+        if st != MRC_OK:
+            msg = self.engine.lib.mrc_last_error(self.engine.ctx)
+            raise _ERRORS.get(st, RouterError)(msg.decode() if msg else "")
+        return _take_result(self.engine.lib, res, n, keep), d
+
+    def stats(self) -> dict:
+        out = (C.c_uint64 * 8)()
+        self.engine._check(self.engine.lib.mrc_server_stats(self.handle, out))
+        keys = ("submitted", "completed", "failed", "launches", "largest_launch", "peak_bytes", "budget_bytes",
+                "queued")
+        return dict(zip(keys, [int(v) for v in out]))
+
+    def close(self):
+        if self.handle:
+            self.engine.lib.mrc_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Engine:
     """One CUDA context of the engine (one per process per device)."""
 
@@ -576,6 +650,9 @@ class Engine:
     def board(self, grid: Grid, x, y, vias, directed=None) -> Board:
         return Board(self, grid, x, y, vias, directed)
 
+    def server(self, **kw) -> Server:
+        return Server(self, **kw)
+
     def negotiation(self, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1) -> Negotiation:
         return Negotiation(self, req, present_weight, history_step)
 
@@ -637,7 +714,7 @@ class CudaIsolatedProvider:
 
 
 __all__ = [
-    "Engine", "Board", "Batch", "Negotiation", "CudaIsolatedProvider", "IsolatedBatchResult", "BoardRoute", "RouteResult",
+    "Engine", "Board", "Batch", "Negotiation", "Server", "CudaIsolatedProvider", "IsolatedBatchResult", "BoardRoute", "RouteResult",
     "RouterError", "InvalidArgument", "MalformedGrid", "InvalidEndpoint", "BackendUnavailable", "Busy",
     "IterationLimit", "OutOfMemory", "LimitExceeded", "net_windows", "load_library", "exported_symbols",
     "COST_MAX", "NO_PATH",

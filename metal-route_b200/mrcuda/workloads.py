@@ -66,8 +66,16 @@ class Workload:
         return b_in + 4
 
 
+_FREE_CACHE: Dict[int, tuple] = {}
+
+
 def _pick_free(rng, grid: Grid, dims: Dims, legal: np.ndarray) -> int:
-    free = np.flatnonzero(legal)
+    hit = _FREE_CACHE.get(id(legal))
+    if hit is None or hit[0] is not legal:
+        _FREE_CACHE.clear()
+        hit = (legal, np.flatnonzero(legal))
+        _FREE_CACHE[id(legal)] = hit
+    free = hit[1]
     return int(free[rng.integers(0, free.size)])
 
 
@@ -375,3 +383,37 @@ def snapshot_board(seed: int = 4, w: int = 2048, h: int = 2048, layers: int = 6,
             "manhattan": f"LogNormal(ln {median:g}, sigma {sigma:g}) clamped [8, w+h-2]", "windows": "net_window"}
     return Workload("snapshot", grid, nets, wins, np.full(w - 1, 10, np.uint32), np.full(h - 1, 10, np.uint32),
                     [via_cost] * (layers - 1), d.reshape(-1), meta)
+
+
+def serving_pool(seed: int = 5, n_boards: int = 16, lo: int = 64, hi: int = 1024, min_layers: int = 2,
+                 max_layers: int = 6) -> List[Workload]:
+    """Boards of the serving workload, generated as the congestion board: side
+    log-uniform in [lo, hi] (square), layers uniform in [min_layers, max_layers]."""
+    rng = np.random.default_rng(seed)
+    pool = []
+    for k in range(n_boards):
+        side = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        layers = int(rng.integers(min_layers, max_layers + 1))
+        pool.append(congestion_board(seed=seed * 1000 + k, w=side, h=side, layers=layers, n_nets=0))
+    return pool
+
+
+def serving_trace(pool: List[Workload], rate: float, n_requests: int, seed: int = 6, min_nets: int = 16,
+                  max_nets: int = 512):
+    """Poisson arrivals at `rate` req/s: (arrival time s, Workload) pairs, each
+    a pool board with its own nets (count log-uniform in [min_nets, max_nets])."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        b = pool[int(rng.integers(0, len(pool)))]
+        n = int(round(np.exp(rng.uniform(np.log(min_nets), np.log(max_nets)))))
+        legal = (b.grid.board_constraint & BOARD_TRACE_NODE) == 0
+        dims = b.grid.dims
+        nets = [NetEndpoints(f"q{i}-{j}", _pick_free(rng, b.grid, dims, legal), _pick_free(rng, b.grid, dims, legal))
+                for j in range(n)]
+        wins = [_net_window(dims, nt) for nt in nets]
+        out.append((t, Workload("serving", b.grid, nets, wins, b.x, b.y, b.vias, b.directed,
+                                dict(b.meta, n_nets=n))))
+    return out
