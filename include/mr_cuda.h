@@ -382,6 +382,11 @@ mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, 
  * nets, pads, windows) are BORROWED: they must stay valid and unchanged until
  * mrc_server_wait for this ticket has returned.  Flags: RETRY_FULL, KEEP_FIELDS. */
 mrc_status mrc_server_submit(mrc_server *srv, const mrc_isolated_request *req, uint32_t flags, uint64_t *ticket);
+/* The same against a board already resident in HBM (mrc_board_create): no
+ * board upload.  The board, nets, pads and windows are borrowed until the
+ * ticket's wait returns. */
+mrc_status mrc_server_submit_resident(mrc_server *srv, const mrc_board *board, const mrc_net *nets, uint32_t n_nets,
+                                      const mrc_window *windows, uint32_t flags, uint64_t *ticket);
 /* Waits up to timeout_ms (0 = forever) for a ticket; on success hands over its
  * result (free with mrc_result_free).  MRC_ERR_BUSY = still running at the
  * timeout (the ticket stays valid); any other error is the request's own. */

@@ -528,7 +528,7 @@ struct mrc_batch {
     // Set before batch_build by callers that run several batches at once: a
     // fixed tile configuration, a shared-memory floor (every concurrent batch
     // has the same per-CTA footprint) and a divisor of the co-resident grid.
-    uint32_t force_tile_h = 0, force_threads = 0, grid_div = 1;
+    uint32_t force_tile_h = 0, force_threads = 0, grid_num = 1, grid_div = 1;
     size_t smem_floor = 0;
     ~mrc_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -587,7 +587,8 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
-    bt->grid = std::max(1u, (uint32_t)ctx->sms * (uint32_t)per_sm / std::max(1u, bt->grid_div));
+    bt->grid = std::max<uint32_t>(
+        1u, (uint32_t)((uint64_t)ctx->sms * (uint32_t)per_sm * bt->grid_num / std::max(1u, bt->grid_div)));
     MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
     MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
     MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
@@ -1580,6 +1581,7 @@ struct ServerRequest {
     uint32_t flags = 0;
     mrc_isolated_request req{};   // borrowed arrays
     mrc_grid grid{};
+    const mrc_board *resident = nullptr;  // a board already in HBM (no upload)
     std::vector<NetCopy> nets;
     std::vector<mrc_window> windows;
     uint64_t cells = 0;           // window cells of all nets
@@ -1599,7 +1601,8 @@ struct ServerBatch {
     std::vector<std::shared_ptr<ServerRequest>> reqs;
     BoardPack pack;
     std::unique_ptr<mrc_batch> bt;
-    uint32_t slot = 0, flags = 0;
+    std::vector<uint32_t> slots;  // claimed slots; the launch runs on the first one's stream
+    uint32_t flags = 0;
     size_t footprint = 0;
     bool finished = false;        // set by the stream callback (under the server mutex)
 };
@@ -1633,9 +1636,12 @@ size_t request_footprint(const ServerRequest &r, uint32_t tile_h) {
     auto al = [](size_t b) { return (std::max<size_t>(b, 4) + 255) & ~(size_t)255; };
     const GridView g{r.grid.w, r.grid.h, r.grid.layers ? r.grid.layers : 1u,
                      (uint64_t)r.grid.w * r.grid.h * (r.grid.layers ? r.grid.layers : 1u)};
-    size_t b = al(g.n * 4) + al((size_t)g.w * 4) + al((size_t)g.h * 4) + al(128);
-    if (r.grid.board_constraint || r.grid.via_forbidden) b += al(g.n);
-    if (r.req.edges.directed_in_costs) b += al(g.n * 16);
+    size_t b = 0;
+    if (!r.resident) {
+        b += al(g.n * 4) + al((size_t)g.w * 4) + al((size_t)g.h * 4) + al(128);
+        if (r.grid.board_constraint || r.grid.via_forbidden) b += al(g.n);
+        if (r.req.edges.directed_in_costs) b += al(g.n * 16);
+    }
     const bool keep = (r.flags & MRC_FLAG_KEEP_FIELDS) != 0;
     for (size_t i = 0; i < r.nets.size(); ++i) {
         const mrc_window &w = r.windows[i];
@@ -1688,13 +1694,15 @@ mrc_status server_launch(mrc_server *s, ServerBatch *b) {
     MRC_TRY(set_device(ctx));
     std::vector<mrc_isolated_request> inst;
     inst.reserve(b->reqs.size());
-    for (auto &r : b->reqs) inst.push_back(r->req);
-    MRC_TRY(board_pack_build(ctx, inst.data(), (uint32_t)inst.size(), &b->pack));
+    for (auto &r : b->reqs)
+        if (!r->resident) inst.push_back(r->req);
+    if (!inst.empty()) MRC_TRY(board_pack_build(ctx, inst.data(), (uint32_t)inst.size(), &b->pack));
     std::vector<const mrc_board *> boards;
     std::vector<NetCopy> nets;
     std::vector<mrc_window> wins;
+    uint32_t packed = 0;
     for (uint32_t k = 0; k < b->reqs.size(); ++k) {
-        boards.push_back(b->pack.boards[k].get());
+        boards.push_back(b->reqs[k]->resident ? b->reqs[k]->resident : b->pack.boards[packed++].get());
         for (const NetCopy &nc : b->reqs[k]->nets) {
             nets.push_back(nc);
             nets.back().board = k;
@@ -1704,12 +1712,13 @@ mrc_status server_launch(mrc_server *s, ServerBatch *b) {
     b->bt.reset(new mrc_batch());
     b->bt->force_tile_h = s->tile_h;
     b->bt->force_threads = s->threads;
+    b->bt->grid_num = (uint32_t)b->slots.size();
     b->bt->grid_div = s->p.slots;
     b->bt->smem_floor = s->smem_floor;
     MRC_TRY(batch_build(ctx, std::move(boards), std::move(nets), std::move(wins), b->flags, b->bt.get()));
-    cudaStream_t st = s->streams[b->slot];
-    MRC_CUDA(cudaEventRecord(s->staged[b->slot], ctx->stream), "record staging");
-    MRC_CUDA(cudaStreamWaitEvent(st, s->staged[b->slot], 0), "wait for staging");
+    cudaStream_t st = s->streams[b->slots[0]];
+    MRC_CUDA(cudaEventRecord(s->staged[b->slots[0]], ctx->stream), "record staging");
+    MRC_CUDA(cudaStreamWaitEvent(st, s->staged[b->slots[0]], 0), "wait for staging");
     MRC_TRY(batch_launch(b->bt.get(), st));
     MRC_CUDA(cudaLaunchHostFunc(st, server_on_done, b), "completion callback");
     return MRC_OK;
@@ -1793,7 +1802,7 @@ void server_loop(mrc_server *s) {
             const auto now = Clock::now();
             for (auto &b : done) {
                 s->inflight_bytes -= b->footprint;
-                s->slot_busy[b->slot] = false;
+                for (uint32_t sl : b->slots) s->slot_busy[sl] = false;
                 for (auto &r : b->reqs) {
                     r->t_done = now;
                     r->done = true;
@@ -1823,7 +1832,6 @@ void server_loop(mrc_server *s) {
             std::unique_ptr<ServerBatch> b(new ServerBatch());
             b->id = s->next_batch++;
             b->srv = s;
-            b->slot = (uint32_t)slot;
             b->flags = head->flags;
             uint64_t cells = 0;
             const auto now = Clock::now();
@@ -1838,9 +1846,21 @@ void server_loop(mrc_server *s) {
                 b->footprint += r->footprint;
                 b->reqs.push_back(std::move(r));
             }
+            // Co-resident grids: a launch takes 1/slots of the grid per slot it
+            // claims, so all launches in flight always fit on the device at once.
+            // With nothing left in the queue it claims every free slot (the whole
+            // idle device); otherwise one, leaving room for the next launch.
+            b->slots.push_back((uint32_t)slot);
+            s->slot_busy[slot] = true;
+            if (s->queue.empty()) {
+                for (uint32_t i = 0; i < s->slot_busy.size(); ++i) {
+                    if (s->slot_busy[i]) continue;
+                    s->slot_busy[i] = true;
+                    b->slots.push_back(i);
+                }
+            }
             s->inflight_bytes += b->footprint;
             s->peak_bytes = std::max(s->peak_bytes, s->inflight_bytes);
-            s->slot_busy[slot] = true;
             s->launches++;
             s->largest = std::max<uint64_t>(s->largest, b->reqs.size());
             ServerBatch *raw = b.get();
@@ -1859,7 +1879,7 @@ void server_loop(mrc_server *s) {
                 for (auto it = s->inflight.begin(); it != s->inflight.end(); ++it) {
                     if (it->get() != raw) continue;
                     s->inflight_bytes -= raw->footprint;
-                    s->slot_busy[raw->slot] = false;
+                    for (uint32_t sl : raw->slots) s->slot_busy[sl] = false;
                     for (auto &r : raw->reqs) {
                         r->status = st;
                         r->error = err;
@@ -1929,6 +1949,35 @@ mrc_status mrc_server_submit(mrc_server *s, const mrc_isolated_request *req, uin
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> g(s->mu);
+        if (s->stop) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "server is stopping");
+        r->ticket = s->next_ticket++;
+        *ticket = r->ticket;
+        s->tickets[r->ticket] = r;
+        s->queue.push_back(r);
+        s->submitted++;
+    }
+    s->cv.notify_all();
+    return MRC_OK;
+}
+
+mrc_status mrc_server_submit_resident(mrc_server *s, const mrc_board *board, const mrc_net *nets, uint32_t n_nets,
+                                      const mrc_window *windows, uint32_t flags, uint64_t *ticket) {
+    if (!s || !board || !ticket) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (board->ctx != s->ctx) return fail(MRC_ERR_INVALID_ARGUMENT, "board belongs to another context");
+    auto r = std::make_shared<ServerRequest>();
+    r->flags = flags & (MRC_FLAG_RETRY_FULL | MRC_FLAG_KEEP_FIELDS);
+    const GridView &g = board->view;
+    if (g.layers > s->p.max_layers) return fail(MRC_ERR_LIMIT, "request has more layers than the server accepts");
+    MRC_TRY(validate_nets(g, nets, n_nets, &r->nets));
+    MRC_TRY(collect_windows(g, r->nets, windows, &r->windows));
+    r->resident = board;
+    r->grid = mrc_grid{g.w, g.h, g.layers, g.cost, g.board, g.via_forbidden};
+    r->req.grid = &r->grid;
+    for (const mrc_window &w : r->windows) r->cells += (uint64_t)(w.x1 - w.x0 + 1) * (w.y1 - w.y0 + 1) * g.layers;
+    r->footprint = request_footprint(*r, s->tile_h);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "server is stopping");
         r->ticket = s->next_ticket++;
         *ticket = r->ticket;

@@ -188,6 +188,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_negotiation_destroy": (None, [vp]),
             "mrc_server_create": (C.c_int, [vp, C.POINTER(_ServerParams), C.POINTER(vp)]),
             "mrc_server_submit": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(C.c_uint64)]),
+            "mrc_server_submit_resident": (C.c_int, [vp, vp, vp, u32, vp, u32, C.POINTER(C.c_uint64)]),
             "mrc_server_wait": (C.c_int, [vp, C.c_uint64, u32, C.POINTER(vp), C.POINTER(_RequestInfo)]),
             "mrc_server_stats": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
             "mrc_server_destroy": (None, [vp]),
@@ -514,6 +515,19 @@ class Server:
         self.engine._check(self.engine.lib.mrc_server_submit(self.handle, C.byref(r), flags, C.byref(t)))
         with self._lock:  # the request's arrays are borrowed until its wait returns
             self._live[t.value] = (m, len(req.nets), keep_fields)
+        return t.value
+
+    def submit_resident(self, board: Board, nets: Sequence[NetEndpoints],
+                        windows: Optional[Sequence[IsolatedRouteWindow]] = None, retry_full: bool = True,
+                        keep_fields: bool = False) -> int:
+        """A request against a board already in HBM (no board upload)."""
+        m = _Marshal()
+        flags = (MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
+        t = C.c_uint64()
+        self.engine._check(self.engine.lib.mrc_server_submit_resident(
+            self.handle, board.handle, m.nets(nets), len(nets), m.windows(windows), flags, C.byref(t)))
+        with self._lock:
+            self._live[t.value] = (m, len(nets), keep_fields)
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 0):

@@ -407,7 +407,8 @@ def serving_trace(pool: List[Workload], rate: float, n_requests: int, seed: int 
     out = []
     for i in range(n_requests):
         t += float(rng.exponential(1.0 / rate))
-        b = pool[int(rng.integers(0, len(pool)))]
+        k = int(rng.integers(0, len(pool)))
+        b = pool[k]
         n = int(round(np.exp(rng.uniform(np.log(min_nets), np.log(max_nets)))))
         legal = (b.grid.board_constraint & BOARD_TRACE_NODE) == 0
         dims = b.grid.dims
@@ -415,5 +416,5 @@ def serving_trace(pool: List[Workload], rate: float, n_requests: int, seed: int 
                 for j in range(n)]
         wins = [_net_window(dims, nt) for nt in nets]
         out.append((t, Workload("serving", b.grid, nets, wins, b.x, b.y, b.vias, b.directed,
-                                dict(b.meta, n_nets=n))))
+                                dict(b.meta, n_nets=n, board_index=k))))
     return out

@@ -151,3 +151,25 @@ def test_submit_validation_and_unknown_tickets(engine):
     res, info = srv.wait(srv.submit(empty))
     assert res.paths == [] and info["status"] == 0
     srv.close()
+
+
+def test_resident_boards_mixed_with_uploaded_ones(engine):
+    """Requests against boards kept in HBM and requests that bring their own
+    board share launches; every result equals the request solved alone."""
+    pool = [W.congestion_board(seed=200 + k, w=96 + 40 * k, h=80 + 30 * k, layers=2 + k, n_nets=0) for k in range(3)]
+    boards = [engine.board(b.grid, b.x, b.y, b.vias, b.directed) for b in pool]
+    trace = W.serving_trace(pool, 50.0, 30, seed=4, min_nets=4, max_nets=48)
+    srv = engine.server(slots=3, max_batch_requests=16)
+    tickets = []
+    for i, (_, wl) in enumerate(trace):
+        if i % 2:
+            tickets.append(srv.submit_resident(boards[wl.meta["board_index"]], wl.nets, wl.windows))
+        else:
+            tickets.append(srv.submit(wl.request()))
+    for t, (_, wl) in zip(tickets, trace):
+        res, _ = srv.wait(t)
+        _same(res, engine.route_isolated_batch(wl.request()))
+    assert srv.stats()["largest_launch"] >= 1
+    srv.close()
+    for b in boards:
+        b.close()
