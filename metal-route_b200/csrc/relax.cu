@@ -214,6 +214,9 @@ __device__ __forceinline__ bool via_blocked(const DevField &f, const uint32_t *p
     return (cell_tile_flags(f, pads, gcell, gf) & kViaBlocked) != 0;
 }
 
+template <int TH>
+__device__ __forceinline__ bool stack_pass(const Tile<TH> &t);
+
 // One sweep of a staged tile: rows (4 lanes x 8 cells), columns (TH/8 lanes x
 // 8 cells), layer stacks (one thread each), each forward then backward, only
 // over lines whose dirty flag is set.
@@ -263,6 +266,17 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, TH - 1 - pos, line % 32); });
     if (L > 1) {
         __syncthreads();
+        ch |= stack_pass<TH>(t);
+    }
+    return ch;
+}
+
+// Layer stacks: one thread per (y, x) column of the tile, upward then downward.
+template <int TH>
+__device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
+    const uint32_t L = t.L;
+    bool ch = false;
+    {
         for (uint32_t r = threadIdx.x; r < TH * 32; r += blockDim.x) {
             if (!t.stackd[r]) continue;
             t.stackd[r] = 0;
