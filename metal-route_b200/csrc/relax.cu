@@ -33,6 +33,7 @@
 namespace mrc {
 
 constexpr uint32_t kTW = 32;  // tile width (one warp across a row)
+constexpr int kLaneCells = 4;  // cells per lane in the row / column passes
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
@@ -222,10 +223,11 @@ __device__ __forceinline__ bool stack_pass(const Tile<TH> &t);
 // over lines whose dirty flag is set.
 template <int TH>
 __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
-    constexpr int SC = TH / 8;
+    constexpr int KC = kLaneCells;          // cells per lane in a line pass
+    constexpr int SR = 32 / KC, SC = TH / KC;  // lanes per row / per column
     const uint32_t L = t.L;
     bool ch = false;
-    ch |= seg_pass<8, 4>(
+    ch |= seg_pass<KC, SR>(
         t.lab, t.st, t.rowd, L * TH, false,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / TH, y = line % TH;
@@ -235,7 +237,7 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 0); },
         [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, pos); });
     __syncwarp();
-    ch |= seg_pass<8, 4>(
+    ch |= seg_pass<KC, SR>(
         t.lab, t.st, t.rowd, L * TH, true,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / TH, y = line % TH, x = 31 - pos;
@@ -245,7 +247,7 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 33); },
         [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, 31 - pos); });
     __syncthreads();
-    ch |= seg_pass<8, SC>(
+    ch |= seg_pass<KC, SC>(
         t.lab, t.st, t.cold, L * 32, false,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / 32, x = line % 32;
@@ -255,7 +257,7 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         [&](uint32_t line) { return t.li(line / 32, 0, line % 32 + 1); },
         [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, pos, line % 32); });
     __syncwarp();
-    ch |= seg_pass<8, SC>(
+    ch |= seg_pass<KC, SC>(
         t.lab, t.st, t.cold, L * 32, true,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
             const uint32_t l = line / 32, x = line % 32, y = TH - 1 - pos;
