@@ -239,14 +239,9 @@ def run_engine(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    from mrcuda.dist import init_from_env, max_over_ranks
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = init_from_env("nccl", timeout_s=120.0, device=torch.device("cuda", local))
 
     wl = _workload(args.workload, rank, args.nets)
     eng = mrcuda.Engine(local)
@@ -295,10 +290,7 @@ def run_engine(args):
     clk = clocks.stop()
     work = batch.stats()
     ms = statistics.fmean(step_ms)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, device="cuda")
     value = len(wl.nets) * world / (ms_max / 1000.0)
 
     # end to end through the public call with host buffers
@@ -310,10 +302,7 @@ def run_engine(args):
         out_paths = wl.route(eng)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = len(wl.nets) * world / float(e2e_t.item())
+    e2e_value = len(wl.nets) * world / max_over_ranks(e2e_s, device="cuda")
     h2d = wl.h2d_bytes()
     d2h = 8 * (len(wl.nets) + 1) + 4 * len(wl.nets) + 4 * sum(len(p) for p in out_paths if p) + 4
     assert out_paths == first.paths, "end-to-end call disagrees with the resident batch"

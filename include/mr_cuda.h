@@ -398,6 +398,15 @@ mrc_status mrc_server_stats(mrc_server *srv, uint64_t out[8]);
 /* Finishes everything queued and in flight, then stops the dispatcher. */
 void mrc_server_destroy(mrc_server *srv);
 
+/* ---- self-test of the bounded device waits ---------------------------------- */
+
+/* Launches one CTA that waits at the engine's grid barrier for a CTA that never
+ * arrives.  The wait gives up after `spin_limit` polls and reports it; the call
+ * returns MRC_OK with the kernel's status bits in *status (bit 4 = barrier wait
+ * exceeded) and the device time in *elapsed_ms, and the context stays usable.
+ * No counterpart in the reference (its Metal loop waits on the host). */
+mrc_status mrc_selftest_wait_timeout(mrc_context *ctx, uint32_t spin_limit, uint32_t *status, float *elapsed_ms);
+
 /* net_window (negotiated.rs:568-594) for a batch of nets. */
 mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
                            mrc_window *out);

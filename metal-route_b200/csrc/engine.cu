@@ -2051,6 +2051,34 @@ void mrc_server_destroy(mrc_server *s) {
 
 }  // extern "C"
 
+extern "C" mrc_status mrc_selftest_wait_timeout(mrc_context *ctx, uint32_t spin_limit, uint32_t *status,
+                                                float *elapsed_ms) {
+    if (!ctx || !status) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    DBuf ctl;
+    MRC_TRY(ctl.get(ctx, sizeof(Ctl), "control block"));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MRC_CUDA(cudaEventCreate(&e0), "create event");
+    MRC_CUDA(cudaEventCreate(&e1), "create event");
+    cudaError_t ce = cudaMemsetAsync(ctl.p, 0, sizeof(Ctl), ctx->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e0, ctx->stream);
+    if (ce == cudaSuccess) ce = wait_selftest_launch(ctl.as<Ctl>(), spin_limit, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, ctx->stream);
+    uint32_t st = 0;
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(&st, &ctl.as<Ctl>()->status, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MRC_CUDA(ce, "wait self-test");
+    *status = st;
+    if (elapsed_ms) *elapsed_ms = ms;
+    return MRC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // The plain form: one net per launch sequence, a host read of the changed
 // flag after every Jacobi round (the reference's M3 loop, gpu.rs:1242-1303).

@@ -109,6 +109,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);
+cudaError_t wait_selftest_launch(Ctl *c, uint32_t spins, cudaStream_t st);
 cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, uint64_t n, cudaStream_t st);
 
 }  // namespace mrc

@@ -181,7 +181,7 @@ __device__ __forceinline__ uint32_t planar_step_g(const DevBoard &b, uint32_t ec
 // Grid-wide barrier for a cooperative launch.  The wait is bounded: after
 // kBarrierSpinLimit polls it records kStatusBarrier and returns, and every CTA
 // leaves the round loop once the status word is non-zero.
-__device__ void grid_barrier(Ctl *c, uint32_t nblocks) {
+__device__ void grid_barrier(Ctl *c, uint32_t nblocks, uint32_t spin_limit = kBarrierSpinLimit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -195,7 +195,7 @@ __device__ void grid_barrier(Ctl *c, uint32_t nblocks) {
         } else {
             uint32_t spins = 0;
             while (*gen_p == gen) {
-                if (++spins > kBarrierSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(&c->status, kStatusBarrier);
                     break;
                 }
@@ -869,6 +869,16 @@ cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cuda
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st) {
     const uint32_t threads = 256;
     plain_round_kernel<<<(uint32_t)((wcells + threads - 1) / threads), threads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// Self-test of the bounded wait: one CTA waits at the grid barrier for a CTA
+// that does not exist, so the wait must give up after `spins` polls, record
+// kStatusBarrier and return with the context intact.
+__global__ void wait_selftest_kernel(Ctl *c, uint32_t spins) { grid_barrier(c, gridDim.x + 1, spins); }
+
+cudaError_t wait_selftest_launch(Ctl *c, uint32_t spins, cudaStream_t st) {
+    wait_selftest_kernel<<<1, 32, 0, st>>>(c, spins);
     return cudaGetLastError();
 }
 

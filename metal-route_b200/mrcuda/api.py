@@ -192,6 +192,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_server_wait": (C.c_int, [vp, C.c_uint64, u32, C.POINTER(vp), C.POINTER(_RequestInfo)]),
             "mrc_server_stats": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
             "mrc_server_destroy": (None, [vp]),
+            "mrc_selftest_wait_timeout": (C.c_int, [vp, u32, C.POINTER(u32), C.POINTER(C.c_float)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -663,6 +664,13 @@ class Engine:
 
     def board(self, grid: Grid, x, y, vias, directed=None) -> Board:
         return Board(self, grid, x, y, vias, directed)
+
+    def selftest_wait_timeout(self, spin_limit: int = 1000) -> dict:
+        """Runs the bounded-wait self-test kernel (a barrier wait that cannot
+        complete) and returns its status bits and device time."""
+        st, ms = C.c_uint32(), C.c_float()
+        self._check(self.lib.mrc_selftest_wait_timeout(self.ctx, int(spin_limit), C.byref(st), C.byref(ms)))
+        return {"status": int(st.value), "ms": float(ms.value)}
 
     def server(self, **kw) -> Server:
         return Server(self, **kw)
