@@ -251,7 +251,12 @@ def run_engine(args):
     else:
         batch = mrcuda.Batch(boards, wl.nets, wl.windows, retry_full=True, time_kernels=True, net_board=wl.net_board)
     # setup, outside the timed region: tile autotune, then capture the launch sequence as a graph
-    tuned = batch.autotune() if not args.no_autotune else None
+    if args.config:
+        th, nt = (int(v) for v in args.config.split(","))
+        batch.set_config(th, nt)
+        tuned = {"tile_h": th, "threads": nt, "forced": True}
+    else:
+        tuned = batch.autotune() if not args.no_autotune else None
     if not args.no_graph:
         batch.capture_graph()
     stream = torch.cuda.Stream()
@@ -560,6 +565,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--config", default="", help="force the relax tile height and CTA width, e.g. 8,256")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
