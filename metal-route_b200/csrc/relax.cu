@@ -34,6 +34,12 @@ namespace mrc {
 
 constexpr uint32_t kTW = 32;  // tile width (one warp across a row)
 constexpr int kLaneCells = 4;  // cells per lane in the row / column passes
+// Shared-memory row pitches, padded so that the line passes' lanes fall on
+// distinct banks: labels (u64) 35 per 34-cell row (8 lanes x 4 cells per row,
+// 4 rows per warp, and the 2-lane column segments), step prices (u32) 33 per
+// 32-cell row.
+constexpr uint32_t kLabPitch = 35;
+constexpr uint32_t kStPitch = 33;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
@@ -67,10 +73,10 @@ struct Tile {
     uint8_t *stackd; // [TH][32] layer stack needs a sweep
     uint32_t L;
     __device__ __forceinline__ uint32_t li(uint32_t l, uint32_t sy, uint32_t sx) const {
-        return (l * (TH + 2) + sy) * 34u + sx;
+        return (l * (TH + 2) + sy) * kLabPitch + sx;
     }
     __device__ __forceinline__ uint32_t si(uint32_t plane, uint32_t l, uint32_t y, uint32_t x) const {
-        return ((plane * L + l) * TH + y) * 32u + x;
+        return ((plane * L + l) * TH + y) * kStPitch + x;
     }
     // a label of interior cell (l, y, x) fell: every other line through it must be swept again
     __device__ __forceinline__ void touched_by_row(uint32_t l, uint32_t y, uint32_t x) const {
@@ -370,10 +376,10 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             const DevField f = a.fields[fi];
             const DevBoard b = a.boards[f.board];
             const uint32_t L = b.layers;  // the shared tile is laid out for this board's layers
-            const uint32_t nsm = L * SH * SW;
+            const uint32_t nsm = L * SH * SW;  // staged cells (pitch kLabPitch in smem)
             tile.lab = reinterpret_cast<u64 *>(smem_raw);
-            tile.st = reinterpret_cast<uint32_t *>(tile.lab + nsm);
-            tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kTW);
+            tile.st = reinterpret_cast<uint32_t *>(tile.lab + L * SH * kLabPitch);
+            tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kStPitch);
             tile.cold = tile.rowd + L * TH;
             tile.stackd = tile.cold + L * kTW;
             tile.L = L;
@@ -413,7 +419,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
                     if (owner < 5 && s_vis[owner]) lv = __ldcg(lab + lc);
                     else if (owner == 0 && gcell == f.src) lv = 0;  // first visit of the source tile
                 }
-                tile.lab[i] = lv;
+                tile.lab[tile.li(l, sy, sx)] = lv;
             }
             // ---- step prices into every interior cell -------------------------
             for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
@@ -806,7 +812,7 @@ cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, u
 
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
     (void)directed;  // directed prices are folded into the step planes
-    return (size_t)layers * (tile_h + 2) * (kTW + 2) * 8 + (size_t)6 * layers * tile_h * kTW * 4 +
+    return (size_t)layers * (tile_h + 2) * kLabPitch * 8 + (size_t)6 * layers * tile_h * kStPitch * 4 +
            (size_t)layers * tile_h + (size_t)layers * kTW + (size_t)tile_h * kTW;
 }
 
