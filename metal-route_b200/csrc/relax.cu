@@ -34,12 +34,14 @@ namespace mrc {
 
 constexpr uint32_t kTW = 32;  // tile width (one warp across a row)
 constexpr int kLaneCells = 4;  // cells per lane in the row / column passes
-// Shared-memory row pitches, padded so that the line passes' lanes fall on
-// distinct banks: labels (u64) 35 per 34-cell row (8 lanes x 4 cells per row,
-// 4 rows per warp, and the 2-lane column segments), step prices (u32) 33 per
-// 32-cell row.
-constexpr uint32_t kLabPitch = 35;
-constexpr uint32_t kStPitch = 33;
+// Shared-memory row pitches of the staged tile: labels (u64) per 34-cell row
+// (32 + halo), step prices (u32) per 32-cell row.  (Padding them to 35 / 33
+// removes bank conflicts of the row passes but measured no faster, and the
+// extra bytes cost a resident CTA per SM on 8-layer tiles.)
+constexpr uint32_t kLabPitch = 34;
+constexpr uint32_t kStPitch = 32;
+constexpr uint32_t kFlPitch = 36;  // flag bytes per staged row (34 used)
+constexpr int kStageUnroll = 4;    // cells whose loads one thread issues together
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
@@ -71,6 +73,7 @@ struct Tile {
     uint8_t *rowd;   // [L][TH] row needs a sweep
     uint8_t *cold;   // [L][32] column needs a sweep
     uint8_t *stackd; // [TH][32] layer stack needs a sweep
+    uint8_t *fl;     // [L][TH+2][kFlPitch] board flag bytes of the tile and its halo
     uint32_t L;
     __device__ __forceinline__ uint32_t li(uint32_t l, uint32_t sy, uint32_t sx) const {
         return (l * (TH + 2) + sy) * kLabPitch + sx;
@@ -217,6 +220,14 @@ __device__ __forceinline__ uint32_t ld_status(const Ctl *c) { return *(volatile 
 
 // Flags of a window cell as a via endpoint: blocked by the board via node bit or
 // by the static via mask unless the net lists the cell as a via pad.
+// Own-pad and via-exemption lookups against the shared-memory copy of the
+// field's sorted lists when they fit (kPadCache / kVPadCache), else HBM.
+constexpr uint32_t kPadCache = 128, kVPadCache = 32;
+__device__ __forceinline__ bool own_pad(const uint32_t *s, uint32_t cap, const uint32_t *g, uint32_t n,
+                                        uint32_t key) {
+    return n <= cap ? sorted_has(s, n, key) : sorted_has(g, n, key);
+}
+
 __device__ __forceinline__ bool via_blocked(const DevField &f, const uint32_t *pads, uint32_t gcell, uint8_t gf) {
     return (cell_tile_flags(f, pads, gcell, gf) & kViaBlocked) != 0;
 }
@@ -327,6 +338,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
     __shared__ u64 s_item;
     __shared__ uint32_t s_push[4];
     __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
+    __shared__ uint32_t s_pads[kPadCache], s_vpads[kVPadCache];
 
     Ctl *ctl = a.ctl;
     const uint32_t tid = threadIdx.x;
@@ -382,6 +394,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kStPitch);
             tile.cold = tile.rowd + L * TH;
             tile.stackd = tile.cold + L * kTW;
+            tile.fl = tile.stackd + TH * kTW;
             tile.L = L;
             const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
             const uint32_t txi = t % ntx, tyi = t / ntx;
@@ -398,67 +411,142 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
                 else if (tid == 4 && tyi + 1 < nty) u = t + ntx;
                 s_vis[tid] = u == kNone ? 0u : __ldcg(a.tvisit + f.tile_off + u);
             }
+            if (f.n_pads <= kPadCache)
+                for (uint32_t i = tid; i < f.n_pads; i += blockDim.x) s_pads[i] = __ldg(a.pads + f.pad_off + i);
+            if (f.n_vpads <= kVPadCache)
+                for (uint32_t i = tid; i < f.n_vpads; i += blockDim.x) s_vpads[i] = __ldg(a.pads + f.vpad_off + i);
+            const uint32_t *gpads = a.pads + f.pad_off, *gvpads = a.pads + f.vpad_off;
+            auto is_own_pad = [&](uint32_t c) {
+                return c == f.src || c == f.dst || own_pad(s_pads, kPadCache, gpads, f.n_pads, c);
+            };
+            auto via_blk = [&](uint32_t c, uint8_t gf) {
+                if (gf & kViaNode) return true;
+                return (gf & kStaticVia) != 0 && !own_pad(s_vpads, kVPadCache, gvpads, f.n_vpads, c);
+            };
             __syncthreads();
 
-            // ---- stage labels (tile + halo ring, through L2) ------------------
-            for (uint32_t i = tid; i < nsm; i += blockDim.x) {
-                const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
-                const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
-                u64 lv = kInf;
-                if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1) {
-                    const bool hx = sx == 0 || sx == SW - 1, hy = sy == 0 || sy == SH - 1;
-                    uint32_t owner;  // which tile's label this smem cell holds
-                    if (hx && hy) owner = 5;  // corner: never read
-                    else if (sx == 0) owner = 1;
-                    else if (sx == SW - 1) owner = 2;
-                    else if (sy == 0) owner = 3;
-                    else if (sy == SH - 1) owner = 4;
-                    else owner = 0;
-                    const uint32_t gcell = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-                    const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0);
-                    if (owner < 5 && s_vis[owner]) lv = __ldcg(lab + lc);
-                    else if (owner == 0 && gcell == f.src) lv = 0;  // first visit of the source tile
+            // ---- stage labels and flag bytes (tile + halo ring) ---------------
+            // Every thread issues the loads of kStageUnroll cells before it
+            // stores any of them, so several L2 requests per thread are in
+            // flight (labels through L2 with ld.global.cg).
+            const uint32_t plane = b.w * b.h;
+            for (uint32_t i0 = tid; i0 < nsm; i0 += kStageUnroll * blockDim.x) {
+                u64 lv[kStageUnroll];
+                uint8_t fv[kStageUnroll];
+#pragma unroll
+                for (int k = 0; k < kStageUnroll; ++k) {
+                    const uint32_t i = i0 + k * blockDim.x;
+                    lv[k] = kInf;
+                    fv[k] = 0;
+                    if (i >= nsm) continue;
+                    const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
+                    const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
+                    if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1) {
+                        const bool hx = sx == 0 || sx == SW - 1, hy = sy == 0 || sy == SH - 1;
+                        uint32_t owner;  // which tile's label this smem cell holds
+                        if (hx && hy) owner = 5;  // corner: never read
+                        else if (sx == 0) owner = 1;
+                        else if (sx == SW - 1) owner = 2;
+                        else if (sy == 0) owner = 3;
+                        else if (sy == SH - 1) owner = 4;
+                        else owner = 0;
+                        const uint32_t gcell = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                        const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0);
+                        if (owner < 5 && s_vis[owner]) lv[k] = __ldcg(lab + lc);
+                        else if (owner == 0 && gcell == f.src) lv[k] = 0;  // first visit of the source tile
+                        if (b.flags) fv[k] = __ldg(b.flags + gcell);
+                    }
                 }
-                tile.lab[tile.li(l, sy, sx)] = lv;
+#pragma unroll
+                for (int k = 0; k < kStageUnroll; ++k) {
+                    const uint32_t i = i0 + k * blockDim.x;
+                    if (i >= nsm) continue;
+                    const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
+                    tile.lab[tile.li(l, sy, sx)] = lv[k];
+                    tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
+                }
             }
             // ---- step prices into every interior cell -------------------------
+            // Phase 1: independent loads only: per interior cell its cost
+            // (parked in the below-plane) and its four planar base prices
+            // (directed in-prices or axis gaps).
+            const uint32_t ncell = L * TH * kTW;
+            for (uint32_t i0 = tid; i0 < ncell; i0 += kStageUnroll * blockDim.x) {
+                uint32_t c[kStageUnroll], p0[kStageUnroll], p1[kStageUnroll], p2[kStageUnroll], p3[kStageUnroll];
+#pragma unroll
+                for (int k = 0; k < kStageUnroll; ++k) {
+                    const uint32_t i = i0 + k * blockDim.x;
+                    c[k] = p0[k] = p1[k] = p2[k] = p3[k] = kMax;
+                    if (i >= ncell) continue;
+                    const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+                    const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+                    if (gx < wx1 && gy < wy1) {
+                        const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                        c[k] = __ldg(b.cost + gc);
+                        if (b.directed) {
+                            const uint4 d4 = __ldg(b.directed + gc);
+                            p0[k] = d4.y;  // from -x
+                            p1[k] = d4.z;  // from +x
+                            p2[k] = d4.x;  // from -y
+                            p3[k] = d4.w;  // from +y
+                        } else {
+                            if (gx > wx0) p0[k] = __ldg(b.x_edge + gx - 1);
+                            if (gx + 1 < wx1) p1[k] = __ldg(b.x_edge + gx);
+                            if (gy > wy0) p2[k] = __ldg(b.y_edge + gy - 1);
+                            if (gy + 1 < wy1) p3[k] = __ldg(b.y_edge + gy);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kStageUnroll; ++k) {
+                    const uint32_t i = i0 + k * blockDim.x;
+                    if (i >= ncell) continue;
+                    const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+                    tile.st[tile.si(kFromNegX, l, y, x)] = p0[k];
+                    tile.st[tile.si(kFromPosX, l, y, x)] = p1[k];
+                    tile.st[tile.si(kFromNegY, l, y, x)] = p2[k];
+                    tile.st[tile.si(kFromPosY, l, y, x)] = p3[k];
+                    tile.st[tile.si(kFromBelow, l, y, x)] = c[k];
+                }
+            }
+            __syncthreads();
+            // Phase 2: every step price from the staged bytes (own pads and via
+            // exemptions are the only global reads left).
             for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
                 const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
                 const int gx = tx0 + (int)x, gy = ty0 + (int)y;
                 uint32_t s0 = kMax, s1 = kMax, s2 = kMax, s3 = kMax, s4 = kMax, s5 = kMax;
                 if (gx < wx1 && gy < wy1) {
                     const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-                    const uint8_t fc = b.flags ? __ldg(b.flags + gc) : 0;
-                    const uint32_t ec = cell_enter(b, f, a.pads, gc, fc);
+                    const uint8_t *flr = tile.fl + (l * SH + y + 1) * kFlPitch + x + 1;  // this cell
+                    const uint8_t fc = flr[0];
+                    const uint32_t cost = tile.st[tile.si(kFromBelow, l, y, x)];
+                    uint32_t ec;  // cell_enter on staged values
+                    if (fc & kTraceNode) ec = kMax;
+                    else if (cost != kMax) ec = cost;
+                    else ec = is_own_pad(gc) ? 1u : kMax;
                     if (ec != kMax) {
-                        if (gx > wx0) {
-                            const uint8_t fp = b.flags ? __ldg(b.flags + gc - 1) : 0;
-                            s0 = planar_step_g(b, ec, fp, fc, kEdgePosX, kEdgeNegX, gc, 1, __ldg(b.x_edge + gx - 1));
-                        }
-                        if (gx + 1 < wx1) {
-                            const uint8_t fp = b.flags ? __ldg(b.flags + gc + 1) : 0;
-                            s1 = planar_step_g(b, ec, fp, fc, kEdgeNegX, kEdgePosX, gc, 2, __ldg(b.x_edge + gx));
-                        }
-                        if (gy > wy0) {
-                            const uint8_t fp = b.flags ? __ldg(b.flags + gc - b.w) : 0;
-                            s2 = planar_step_g(b, ec, fp, fc, kEdgePosY, kEdgeNegY, gc, 0, __ldg(b.y_edge + gy - 1));
-                        }
-                        if (gy + 1 < wy1) {
-                            const uint8_t fp = b.flags ? __ldg(b.flags + gc + b.w) : 0;
-                            s3 = planar_step_g(b, ec, fp, fc, kEdgeNegY, kEdgePosY, gc, 3, __ldg(b.y_edge + gy));
-                        }
+                        const bool dir = b.directed != nullptr;
+                        auto planar = [&](uint32_t base, uint8_t fp, uint8_t out_bit, uint8_t in_bit) -> uint32_t {
+                            if (dir && base == kMax) return kMax;  // blocked directed edge
+                            if ((fp & out_bit) | (fc & in_bit)) return kMax;
+                            return capmul(base, ec);
+                        };
+                        if (gx > wx0) s0 = planar(tile.st[tile.si(kFromNegX, l, y, x)], flr[-1], kEdgePosX, kEdgeNegX);
+                        if (gx + 1 < wx1) s1 = planar(tile.st[tile.si(kFromPosX, l, y, x)], flr[1], kEdgeNegX, kEdgePosX);
+                        if (gy > wy0)
+                            s2 = planar(tile.st[tile.si(kFromNegY, l, y, x)], flr[-(int)kFlPitch], kEdgePosY, kEdgeNegY);
+                        if (gy + 1 < wy1)
+                            s3 = planar(tile.st[tile.si(kFromPosY, l, y, x)], flr[kFlPitch], kEdgeNegY, kEdgePosY);
                         if (L > 1) {
-                            const bool vc = via_blocked(f, a.pads, gc, fc);
-                            const uint32_t plane = b.w * b.h;
+                            const bool vc = via_blk(gc, fc);
                             if (l > 0 && ((b.via_mask >> (l - 1)) & 1u) && !vc) {
-                                const uint32_t gp = gc - plane;
-                                if (!via_blocked(f, a.pads, gp, b.flags ? __ldg(b.flags + gp) : 0))
-                                    s4 = capmul(__ldg(b.via_edge + l - 1), ec);
+                                const uint8_t fq = flr[-(int)(SH * kFlPitch)];
+                                if (!via_blk(gc - plane, fq)) s4 = capmul(__ldg(b.via_edge + l - 1), ec);
                             }
                             if (l + 1 < L && ((b.via_mask >> l) & 1u) && !vc) {
-                                const uint32_t gp = gc + plane;
-                                if (!via_blocked(f, a.pads, gp, b.flags ? __ldg(b.flags + gp) : 0))
-                                    s5 = capmul(__ldg(b.via_edge + l), ec);
+                                const uint8_t fq = flr[SH * kFlPitch];
+                                if (!via_blk(gc + plane, fq)) s5 = capmul(__ldg(b.via_edge + l), ec);
                             }
                         }
                     }
@@ -534,10 +622,14 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
                 if (!exists || s_push[side]) continue;
                 const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
                 if (lb == kInf) continue;
-                const uint32_t gb = (l * b.h + (uint32_t)(ty0 + (int)bsy - 1)) * b.w + (uint32_t)(tx0 + (int)bsx - 1);
                 const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
-                const uint8_t fb = b.flags ? __ldg(b.flags + gb) : 0, fn = b.flags ? __ldg(b.flags + gn) : 0;
-                const uint32_t en = cell_enter(b, f, a.pads, gn, fn);
+                const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
+                const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
+                uint32_t en = kMax;  // cell_enter of the neighbour
+                if (!(fn & kTraceNode)) {
+                    const uint32_t cn = __ldg(b.cost + gn);
+                    en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
+                }
                 if (en == kMax) continue;
                 const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
                 uint32_t gap;
@@ -813,7 +905,8 @@ cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, u
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
     (void)directed;  // directed prices are folded into the step planes
     return (size_t)layers * (tile_h + 2) * kLabPitch * 8 + (size_t)6 * layers * tile_h * kStPitch * 4 +
-           (size_t)layers * tile_h + (size_t)layers * kTW + (size_t)tile_h * kTW;
+           (size_t)layers * tile_h + (size_t)layers * kTW + (size_t)tile_h * kTW +
+           (size_t)layers * (tile_h + 2) * kFlPitch;
 }
 
 namespace {
