@@ -252,9 +252,11 @@ def run_engine(args):
         batch = mrcuda.Batch(boards, wl.nets, wl.windows, retry_full=True, time_kernels=True, net_board=wl.net_board)
     # setup, outside the timed region: tile autotune, then capture the launch sequence as a graph
     if args.config:
-        th, nt = (int(v) for v in args.config.split(","))
-        batch.set_config(th, nt)
-        tuned = {"tile_h": th, "threads": nt, "forced": True}
+        cfg = [int(v) for v in args.config.split(",")]
+        batch.set_config(cfg[0], cfg[1])
+        if len(cfg) > 2:
+            batch.set_schedule(cfg[2])
+        tuned = dict(batch.config(), forced=True)
     else:
         tuned = batch.autotune() if not args.no_autotune else None
     if not args.no_graph:
@@ -565,7 +567,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--config", default="", help="force the relax tile height and CTA width, e.g. 8,256")
+    ap.add_argument("--config", default="",
+                    help="force the relax tile height, CTA width and schedule (0 rounds, 1 queue), e.g. 8,256,1")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -208,6 +208,13 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
 /* Force a relax configuration on a batch: tile height in {8, 16, 32, 64} cells
  * and 128 or 256 threads per CTA.  MRC_ERR_LIMIT when the tile does not fit. */
 mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t tile_h, uint32_t threads);
+/* The relax schedule: 0 = bulk-synchronous rounds over a shared tile list
+ * (cooperative launch, grid barrier between rounds); 1 = one asynchronous
+ * work queue (no rounds; labels written with 64-bit atomicMin).  Both give the
+ * same labels and paths.  The autotuner tries both. */
+mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule);
+/* The batch's current tile height, CTA width and schedule. */
+mrc_status mrc_batch_config(const mrc_batch *batch, uint32_t *tile_h, uint32_t *threads, uint32_t *schedule);
 /* Kernels launched by the last mrc_batch_launch (for launch accounting). */
 uint32_t mrc_batch_kernel_launches(const mrc_batch *batch);
 /* Device milliseconds of the relax kernel of the last launch, from CUDA events

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -139,8 +140,9 @@ struct mrc_context {
     HostStage stage;
     int sms = 148;
     size_t smem_optin = 0;
-    // autotuned relax configuration per (layers, directed): tile height, CTA width
-    std::map<uint32_t, std::pair<uint32_t, uint32_t>> tuned;
+    // autotuned relax configuration per (layers, directed): tile height, CTA
+    // width, schedule (0 = bulk-synchronous rounds, 1 = asynchronous queue)
+    std::map<uint32_t, std::array<uint32_t, 3>> tuned;
 };
 
 namespace {
@@ -529,6 +531,7 @@ struct mrc_batch {
     // fixed tile configuration, a shared-memory floor (every concurrent batch
     // has the same per-CTA footprint) and a divisor of the co-resident grid.
     uint32_t force_tile_h = 0, force_threads = 0, grid_num = 1, grid_div = 1;
+    bool async_q = false;  // relax schedule: asynchronous work queue instead of rounds
     size_t smem_floor = 0;
     ~mrc_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -583,8 +586,8 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     bt->total_tiles = (uint32_t)std::max<uint64_t>(toff, 1);
     bt->max_tiles = max_tiles;
     int per_sm = 1;
-    MRC_CUDA(relax_configure(tile_h, threads, bt->smem), "configure relax kernel");
-    MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm), "relax occupancy");
+    MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q), "configure relax kernel");
+    MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
     bt->grid = std::max<uint32_t>(
@@ -617,8 +620,9 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         tile_h = bt->force_tile_h;
         threads = bt->force_threads ? bt->force_threads : kRelaxThreads;
     } else if (tuned != ctx->tuned.end()) {
-        tile_h = tuned->second.first;
-        threads = tuned->second.second;
+        tile_h = tuned->second[0];
+        threads = tuned->second[1];
+        bt->async_q = tuned->second[2] != 0;
     } else {
         MRC_TRY(choose_tile(ctx, bt->max_layers, bt->directed_any, &tile_h, &smem));
     }
@@ -719,12 +723,18 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
     ra.ctl = bt->d_ctl.as<Ctl>();
     ra.tile_h = bt->tile_h;
     ra.round_limit = 64u * bt->max_tiles + 4096u;
+    ra.activation_limit = 64ull * bt->total_tiles + 4096ull;
+    if (n && bt->async_q) {
+        MRC_CUDA(cudaMemsetAsync(bt->d_lab.p, 0xFF, bt->total_cells * 8, st), "fill label arena");
+        MRC_CUDA(cudaMemsetAsync(bt->d_lists.as<u64>() + bt->total_tiles, 0, (size_t)bt->total_tiles * 8, st),
+                 "reset queue tags");
+    }
     if (n) {
         const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
         if (bt->ev0) MRC_CUDA(cudaEventRecordWithFlags(bt->ev0, st, rec), "record event");
-        MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st), "launch relax kernel");
+        MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q), "launch relax kernel");
         if (bt->ev1) MRC_CUDA(cudaEventRecordWithFlags(bt->ev1, st, rec), "record event");
-        launches++;
+        launches += bt->async_q ? 2 : 1;  // (+ the seed kernel)
     }
     const PathArgs pa = path_args(bt);
     MRC_CUDA(path_launch(pa, st), "launch path kernels");
@@ -1226,11 +1236,15 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     MRC_CUDA(cudaEventCreate(&e1), "create event");
     float best = -1.0f;
     uint32_t best_th = batch->tile_h, best_nt = batch->threads;
+    bool best_async = batch->async_q;
     mrc_status rc = MRC_OK;
     for (uint32_t th : {8u, 16u, 32u, 64u}) {
         if (relax_smem_bytes(layers, th, batch->directed_any) > hard) continue;
-        for (uint32_t nt : {128u, 256u}) {
+        for (uint32_t cfg = 0; cfg < 4; ++cfg) {
+            const uint32_t nt = cfg & 1 ? 256u : 128u;
+            const bool async = (cfg & 2) != 0;
             if (4u * layers * th < nt / 2) continue;  // most lanes would idle in the line passes
+            batch->async_q = async;
             rc = batch_layout(batch, th, nt);
             if (rc != MRC_OK) break;
             float ms = 0.0f, sum = 0.0f;
@@ -1247,6 +1261,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
                 best = sum;
                 best_th = th;
                 best_nt = nt;
+                best_async = async;
             }
         }
         if (rc != MRC_OK) break;
@@ -1254,8 +1269,9 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != MRC_OK) return rc;
+    batch->async_q = best_async;
     MRC_TRY(batch_layout(batch, best_th, best_nt));
-    ctx->tuned[tune_key(layers, batch->directed_any)] = {best_th, best_nt};
+    ctx->tuned[tune_key(layers, batch->directed_any)] = {best_th, best_nt, best_async ? 1u : 0u};
     if (tile_h) *tile_h = best_th;
     if (threads) *threads = best_nt;
     if (best_ms) *best_ms = best;
@@ -1272,6 +1288,23 @@ mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t til
     if (relax_smem_bytes(batch->max_layers, tile_h, batch->directed_any) > hard)
         return fail(MRC_ERR_LIMIT, "tile does not fit in shared memory");
     return batch_layout(batch, tile_h, threads);
+}
+
+mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule) {
+    if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (schedule > 1) return fail(MRC_ERR_INVALID_ARGUMENT, "schedule must be 0 (rounds) or 1 (queue)");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    batch->async_q = schedule == 1;
+    return batch_layout(batch, batch->tile_h, batch->threads);
+}
+
+mrc_status mrc_batch_config(const mrc_batch *batch, uint32_t *tile_h, uint32_t *threads, uint32_t *schedule) {
+    if (!batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (tile_h) *tile_h = batch->tile_h;
+    if (threads) *threads = batch->threads;
+    if (schedule) *schedule = batch->async_q ? 1u : 0u;
+    return MRC_OK;
 }
 
 uint32_t mrc_batch_kernel_launches(const mrc_batch *batch) { return batch ? batch->launches : 0; }
@@ -2443,6 +2476,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     ra.ctl = reinterpret_cast<Ctl *>(s + o_ctl);
     ra.tile_h = tile_h;
     ra.round_limit = 64u * max_tiles + 4096u;
+    ra.activation_limit = ~0ull;
     MRC_CUDA(relax_launch(ra, (uint32_t)dev->sms * (uint32_t)per_sm, kRelaxThreads, smem, st), "launch relax kernel");
     PathArgs pa;
     pa.boards = ra.boards;

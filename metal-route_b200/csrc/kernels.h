@@ -33,6 +33,7 @@ struct RelaxArgs {
     Ctl *ctl;                   // zeroed before launch
     uint32_t tile_h;            // 32, 16 or 8
     uint32_t round_limit;       // guard on the number of rounds
+    unsigned long long activation_limit;  // guard on tile activations (asynchronous form)
 };
 
 struct PathArgs {
@@ -103,9 +104,13 @@ cudaError_t dirty_launch(const DirtyArgs &a, cudaStream_t st);
 // Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);
 // The relax kernel is instantiated for threads in {128, 256} per CTA.
-cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem);
-cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm);
-cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st);
+// `async` selects the queue-driven form (relax_async_kernel) over the
+// bulk-synchronous rounds (relax_rounds_kernel); the async form needs the label
+// arena filled with 0xFF and the queue tags (lists[cap, 2 cap)) zeroed.
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async = false);
+cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async = false);
+cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
+                         bool async = false);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);

@@ -330,20 +330,401 @@ __device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
     return ch;
 }
 
-template <int TH, int NT>
-__global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// Work queue of the asynchronous form.  count[0] = tickets handed to pushers
+// (tail), head[0] = tickets handed to poppers, count[1] = items queued or in
+// flight.  lists[0, cap) holds the items, lists[cap, 2 cap) their ticket tags
+// (ticket + 1, zeroed before launch).  A tile is queued at most once at a time
+// (its tstamp word is the queued flag), so cap = total tiles never overflows.
+constexpr uint32_t kQueueSpinLimit = 1u << 26;
+
+__device__ __forceinline__ void async_push(const RelaxArgs &a, uint32_t fi, uint32_t tile_off, uint32_t u) {
+    Ctl *c = a.ctl;
+    if (atomicExch(a.tstamp + tile_off + u, 1u) != 0u) return;  // already queued
+    atomicAdd(&c->count[1], 1u);                                  // in flight before it is visible
+    const uint32_t h = atomicAdd(&c->count[0], 1u);
+    const size_t slot = h % a.list_cap;
+    a.lists[slot] = ((u64)fi << 32) | u;
+    __threadfence();
+    atomicExch(a.lists + a.list_cap + slot, (u64)h + 1u);
+}
+
+// Next item for the calling CTA (thread 0), or kInf when no work is left.  The
+// wait is bounded: kQueueSpinLimit polls, then kStatusBarrier and an exit.
+__device__ __forceinline__ u64 async_pop(const RelaxArgs &a) {
+    Ctl *c = a.ctl;
+    const uint32_t h = atomicAdd(&c->head[0], 1u);
+    const size_t slot = h % a.list_cap;
+    const volatile u64 *tag = a.lists + a.list_cap + slot;
+    for (uint32_t spins = 0;; ++spins) {
+        if (*tag == (u64)h + 1u) {
+            __threadfence();
+            return __ldcg(a.lists + slot);
+        }
+        if (*(volatile const uint32_t *)&c->count[1] == 0u) return kInf;  // nothing queued or running
+        if (*(volatile const uint32_t *)&c->status) return kInf;
+        if (spins > kQueueSpinLimit) {
+            atomicOr(&c->status, kStatusBarrier);
+            return kInf;
+        }
+        __nanosleep(spins < 32 ? 32 : 256);
+    }
+}
+
+// One (field, tile) item: stage the tile and its halo, relax it to local
+// convergence, write it back and queue the neighbours it improves.
+template <int TH, bool ASYNC>
+__device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, uint32_t t, uint32_t round,
+                                             unsigned char *smem_raw) {
     const uint32_t SW = kTW + 2, SH = TH + 2;
     Tile<TH> tile;
-    __shared__ u64 s_item;
     __shared__ uint32_t s_push[4];
     __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
     __shared__ uint32_t s_pads[kPadCache], s_vpads[kVPadCache];
-
     Ctl *ctl = a.ctl;
     const uint32_t tid = threadIdx.x;
     const uint32_t cap = a.list_cap;
+    const DevField f = a.fields[fi];
+    const DevBoard b = a.boards[f.board];
+    const uint32_t L = b.layers;  // the shared tile is laid out for this board's layers
+    const uint32_t nsm = L * SH * SW;  // staged cells (pitch kLabPitch in smem)
+    tile.lab = reinterpret_cast<u64 *>(smem_raw);
+    tile.st = reinterpret_cast<uint32_t *>(tile.lab + L * SH * kLabPitch);
+    tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kStPitch);
+    tile.cold = tile.rowd + L * TH;
+    tile.stackd = tile.cold + L * kTW;
+    tile.fl = tile.stackd + TH * kTW;
+    tile.L = L;
+    const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
+    const uint32_t txi = t % ntx, tyi = t / ntx;
+    const int tx0 = (int)(f.x0 + txi * kTW), ty0 = (int)(f.y0 + tyi * TH);
+    const uint32_t tw = min(kTW, f.ww - txi * kTW), th = min(TH, f.wh - tyi * TH);
+    const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
+    const u64 *lab = a.lab + f.lab_off;
+    if constexpr (ASYNC) {
+        // leave the queue before reading any label: a neighbour that improves
+        // our halo after this point queues the tile again
+        if (tid == 0) {
+            atomicExch(a.tstamp + f.tile_off + t, 0u);
+            __threadfence();
+        }
+    } else if (tid < 5) {
+        uint32_t u = kNone;
+        if (tid == 0) u = t;
+        else if (tid == 1 && txi > 0) u = t - 1;
+        else if (tid == 2 && txi + 1 < ntx) u = t + 1;
+        else if (tid == 3 && tyi > 0) u = t - ntx;
+        else if (tid == 4 && tyi + 1 < nty) u = t + ntx;
+        s_vis[tid] = u == kNone ? 0u : __ldcg(a.tvisit + f.tile_off + u);
+    }
+    if (tid < 4) s_push[tid] = 0;
+    if (f.n_pads <= kPadCache)
+        for (uint32_t i = tid; i < f.n_pads; i += blockDim.x) s_pads[i] = __ldg(a.pads + f.pad_off + i);
+    if (f.n_vpads <= kVPadCache)
+        for (uint32_t i = tid; i < f.n_vpads; i += blockDim.x) s_vpads[i] = __ldg(a.pads + f.vpad_off + i);
+    const uint32_t *gpads = a.pads + f.pad_off, *gvpads = a.pads + f.vpad_off;
+    auto is_own_pad = [&](uint32_t c) {
+        return c == f.src || c == f.dst || own_pad(s_pads, kPadCache, gpads, f.n_pads, c);
+    };
+    auto via_blk = [&](uint32_t c, uint8_t gf) {
+        if (gf & kViaNode) return true;
+        return (gf & kStaticVia) != 0 && !own_pad(s_vpads, kVPadCache, gvpads, f.n_vpads, c);
+    };
+    __syncthreads();
 
+    // ---- stage labels and flag bytes (tile + halo ring) ---------------
+    // Every thread issues the loads of kStageUnroll cells before it
+    // stores any of them, so several L2 requests per thread are in
+    // flight (labels through L2 with ld.global.cg).
+    const uint32_t plane = b.w * b.h;
+    for (uint32_t i0 = tid; i0 < nsm; i0 += kStageUnroll * blockDim.x) {
+        u64 lv[kStageUnroll];
+        uint8_t fv[kStageUnroll];
+#pragma unroll
+        for (int k = 0; k < kStageUnroll; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            lv[k] = kInf;
+            fv[k] = 0;
+            if (i >= nsm) continue;
+            const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
+            const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
+            if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1) {
+                const bool hx = sx == 0 || sx == SW - 1, hy = sy == 0 || sy == SH - 1;
+                uint32_t owner;  // which tile's label this smem cell holds
+                if (hx && hy) owner = 5;  // corner: never read
+                else if (sx == 0) owner = 1;
+                else if (sx == SW - 1) owner = 2;
+                else if (sy == 0) owner = 3;
+                else if (sy == SH - 1) owner = 4;
+                else owner = 0;
+                const uint32_t gcell = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0);
+                if constexpr (ASYNC) {
+                    if (owner < 5) lv[k] = __ldcg(lab + lc);  // the arena starts at +inf
+                } else {
+                    if (owner < 5 && s_vis[owner]) lv[k] = __ldcg(lab + lc);
+                    else if (owner == 0 && gcell == f.src) lv[k] = 0;  // first visit of the source tile
+                }
+                if (b.flags) fv[k] = __ldg(b.flags + gcell);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kStageUnroll; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i >= nsm) continue;
+            const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
+            tile.lab[tile.li(l, sy, sx)] = lv[k];
+            tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
+        }
+    }
+    // ---- step prices into every interior cell -------------------------
+    // Phase 1: independent loads only: per interior cell its cost
+    // (parked in the below-plane) and its four planar base prices
+    // (directed in-prices or axis gaps).
+    const uint32_t ncell = L * TH * kTW;
+    for (uint32_t i0 = tid; i0 < ncell; i0 += kStageUnroll * blockDim.x) {
+        uint32_t c[kStageUnroll], p0[kStageUnroll], p1[kStageUnroll], p2[kStageUnroll], p3[kStageUnroll];
+#pragma unroll
+        for (int k = 0; k < kStageUnroll; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            c[k] = p0[k] = p1[k] = p2[k] = p3[k] = kMax;
+            if (i >= ncell) continue;
+            const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+            const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+            if (gx < wx1 && gy < wy1) {
+                const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                c[k] = __ldg(b.cost + gc);
+                if (b.directed) {
+                    const uint4 d4 = __ldg(b.directed + gc);
+                    p0[k] = d4.y;  // from -x
+                    p1[k] = d4.z;  // from +x
+                    p2[k] = d4.x;  // from -y
+                    p3[k] = d4.w;  // from +y
+                } else {
+                    if (gx > wx0) p0[k] = __ldg(b.x_edge + gx - 1);
+                    if (gx + 1 < wx1) p1[k] = __ldg(b.x_edge + gx);
+                    if (gy > wy0) p2[k] = __ldg(b.y_edge + gy - 1);
+                    if (gy + 1 < wy1) p3[k] = __ldg(b.y_edge + gy);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kStageUnroll; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i >= ncell) continue;
+            const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+            tile.st[tile.si(kFromNegX, l, y, x)] = p0[k];
+            tile.st[tile.si(kFromPosX, l, y, x)] = p1[k];
+            tile.st[tile.si(kFromNegY, l, y, x)] = p2[k];
+            tile.st[tile.si(kFromPosY, l, y, x)] = p3[k];
+            tile.st[tile.si(kFromBelow, l, y, x)] = c[k];
+        }
+    }
+    __syncthreads();
+    // Phase 2: every step price from the staged bytes (own pads and via
+    // exemptions are the only global reads left).
+    for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
+        const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+        const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+        uint32_t s0 = kMax, s1 = kMax, s2 = kMax, s3 = kMax, s4 = kMax, s5 = kMax;
+        if (gx < wx1 && gy < wy1) {
+            const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+            const uint8_t *flr = tile.fl + (l * SH + y + 1) * kFlPitch + x + 1;  // this cell
+            const uint8_t fc = flr[0];
+            const uint32_t cost = tile.st[tile.si(kFromBelow, l, y, x)];
+            uint32_t ec;  // cell_enter on staged values
+            if (fc & kTraceNode) ec = kMax;
+            else if (cost != kMax) ec = cost;
+            else ec = is_own_pad(gc) ? 1u : kMax;
+            if (ec != kMax) {
+                const bool dir = b.directed != nullptr;
+                auto planar = [&](uint32_t base, uint8_t fp, uint8_t out_bit, uint8_t in_bit) -> uint32_t {
+                    if (dir && base == kMax) return kMax;  // blocked directed edge
+                    if ((fp & out_bit) | (fc & in_bit)) return kMax;
+                    return capmul(base, ec);
+                };
+                if (gx > wx0) s0 = planar(tile.st[tile.si(kFromNegX, l, y, x)], flr[-1], kEdgePosX, kEdgeNegX);
+                if (gx + 1 < wx1) s1 = planar(tile.st[tile.si(kFromPosX, l, y, x)], flr[1], kEdgeNegX, kEdgePosX);
+                if (gy > wy0)
+                    s2 = planar(tile.st[tile.si(kFromNegY, l, y, x)], flr[-(int)kFlPitch], kEdgePosY, kEdgeNegY);
+                if (gy + 1 < wy1)
+                    s3 = planar(tile.st[tile.si(kFromPosY, l, y, x)], flr[kFlPitch], kEdgeNegY, kEdgePosY);
+                if (L > 1) {
+                    const bool vc = via_blk(gc, fc);
+                    if (l > 0 && ((b.via_mask >> (l - 1)) & 1u) && !vc) {
+                        const uint8_t fq = flr[-(int)(SH * kFlPitch)];
+                        if (!via_blk(gc - plane, fq)) s4 = capmul(__ldg(b.via_edge + l - 1), ec);
+                    }
+                    if (l + 1 < L && ((b.via_mask >> l) & 1u) && !vc) {
+                        const uint8_t fq = flr[SH * kFlPitch];
+                        if (!via_blk(gc + plane, fq)) s5 = capmul(__ldg(b.via_edge + l), ec);
+                    }
+                }
+            }
+        }
+        tile.st[tile.si(kFromNegX, l, y, x)] = s0;
+        tile.st[tile.si(kFromPosX, l, y, x)] = s1;
+        tile.st[tile.si(kFromNegY, l, y, x)] = s2;
+        tile.st[tile.si(kFromPosY, l, y, x)] = s3;
+        tile.st[tile.si(kFromBelow, l, y, x)] = s4;
+        tile.st[tile.si(kFromAbove, l, y, x)] = s5;
+    }
+    for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 1;
+    __syncthreads();
+
+    // ---- relax to local convergence ---------------------------------
+    const uint32_t sweep_limit = L * kTW * TH + 4;
+    uint32_t sweep = 0;
+    for (;;) {
+        const bool ch = relax_tile<TH>(tile);
+        ++sweep;
+        const int any = __syncthreads_or(ch ? 1 : 0);
+        if (!any) break;
+        if (sweep > sweep_limit) {
+            if (tid == 0) atomicOr(&ctl->status, kStatusRoundLimit);
+            break;
+        }
+    }
+
+    // ---- write back and find neighbours this tile can improve -------
+    u64 *labw = a.lab + f.lab_off;
+    if constexpr (ASYNC) {
+        // another CTA may hold this tile too (it was queued again while we ran):
+        // only labels that beat the arena are written, with a 64-bit atomicMin
+        for (uint32_t i0 = tid; i0 < L * th * tw; i0 += kStageUnroll * blockDim.x) {
+            u64 nv[kStageUnroll], ov[kStageUnroll];
+#pragma unroll
+            for (int k = 0; k < kStageUnroll; ++k) {
+                const uint32_t i = i0 + k * blockDim.x;
+                nv[k] = ov[k] = kInf;
+                if (i >= L * th * tw) continue;
+                const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
+                nv[k] = tile.lab[tile.li(l, ty + 1, tx + 1)];
+                const uint64_t lc =
+                    ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
+                if (nv[k] != kInf) ov[k] = __ldcg(labw + lc);
+            }
+#pragma unroll
+            for (int k = 0; k < kStageUnroll; ++k) {
+                const uint32_t i = i0 + k * blockDim.x;
+                if (i >= L * th * tw || nv[k] >= ov[k]) continue;
+                const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
+                const uint64_t lc =
+                    ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
+                atomicMin(labw + lc, nv[k]);
+            }
+        }
+    } else {
+        for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
+            const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
+            const uint64_t lc =
+                ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
+            labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
+        }
+    }
+    // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
+    const uint32_t nb = 2 * L * th + 2 * L * tw;
+    for (uint32_t i = tid; i < nb; i += blockDim.x) {
+        uint32_t side, l, k;
+        if (i < 2 * L * th) {
+            side = i / (L * th);
+            const uint32_t r = i % (L * th);
+            l = r / th;
+            k = r % th;
+        } else {
+            const uint32_t j = i - 2 * L * th;
+            side = 2 + j / (L * tw);
+            const uint32_t r = j % (L * tw);
+            l = r / tw;
+            k = r % tw;
+        }
+        bool exists;
+        uint32_t bsx, bsy, nsx, nsy, dir;
+        uint8_t out_bit, in_bit;
+        if (side == 0) {
+            exists = txi > 0;
+            bsx = 1; bsy = k + 1; nsx = 0; nsy = bsy;
+            dir = 2; out_bit = kEdgeNegX; in_bit = kEdgePosX;
+        } else if (side == 1) {
+            exists = txi + 1 < ntx;
+            bsx = tw; bsy = k + 1; nsx = tw + 1; nsy = bsy;
+            dir = 1; out_bit = kEdgePosX; in_bit = kEdgeNegX;
+        } else if (side == 2) {
+            exists = tyi > 0;
+            bsx = k + 1; bsy = 1; nsx = bsx; nsy = 0;
+            dir = 3; out_bit = kEdgeNegY; in_bit = kEdgePosY;
+        } else {
+            exists = tyi + 1 < nty;
+            bsx = k + 1; bsy = th; nsx = bsx; nsy = th + 1;
+            dir = 0; out_bit = kEdgePosY; in_bit = kEdgeNegY;
+        }
+        if (!exists || s_push[side]) continue;
+        const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
+        if (lb == kInf) continue;
+        const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
+        const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
+        const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
+        uint32_t en = kMax;  // cell_enter of the neighbour
+        if (!(fn & kTraceNode)) {
+            const uint32_t cn = __ldg(b.cost + gn);
+            en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
+        }
+        if (en == kMax) continue;
+        const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
+        uint32_t gap;
+        if (side == 0) gap = __ldg(b.x_edge + gx_n);
+        else if (side == 1) gap = __ldg(b.x_edge + gx_n - 1);
+        else if (side == 2) gap = __ldg(b.y_edge + gy_n);
+        else gap = __ldg(b.y_edge + gy_n - 1);
+        const u64 cand = ext2(lb, planar_step_g(b, en, fb, fn, out_bit, in_bit, gn, dir, gap), 1);
+        if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
+    }
+    __syncthreads();
+    if (tid < 5) {
+        __threadfence();  // labels before the visited flag and the queue entries
+        if (tid == 4) {
+            if constexpr (ASYNC) {
+                if (!__ldcg(a.tvisit + f.tile_off + t)) atomicExch(a.tvisit + f.tile_off + t, 1u);
+                if (atomicAdd(&ctl->activations, 1ull) >= a.activation_limit)
+                    atomicOr(&ctl->status, kStatusActivationLimit);
+            } else {
+                if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
+                atomicAdd(&ctl->activations, 1ull);
+            }
+            atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
+        } else if (s_push[tid]) {
+            const uint32_t u = tid == 0 ? t - 1 : tid == 1 ? t + 1 : tid == 2 ? t - ntx : t + ntx;
+            if constexpr (ASYNC) {
+                async_push(a, fi, f.tile_off, u);
+            } else {
+                const uint32_t want = round + 2;  // stamp s = queued for round s-1
+                if (atomicMax(a.tstamp + f.tile_off + u, want) < want) {
+                    const uint32_t nxt = (round + 1) % 3;
+                    const uint32_t idx = atomicAdd(&ctl->count[nxt], 1u);
+                    if (idx < cap) {
+                        a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | u;
+                    } else {
+                        atomicOr(&ctl->status, kStatusQueueOverflow);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if constexpr (ASYNC) {
+        if (tid == 0) {  // this item is done: its own pushes are already counted
+            __threadfence();
+            atomicSub(&ctl->count[1], 1u);
+        }
+    }
+}
+
+template <int TH, int NT>
+__global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ u64 s_item;
+    Ctl *ctl = a.ctl;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t cap = a.list_cap;
     // ---- round 0: every field's source tile ---------------------------------
     for (uint32_t fi = blockIdx.x * blockDim.x + tid; fi < a.n_fields; fi += gridDim.x * blockDim.x) {
         const DevField f = a.fields[fi];
@@ -379,290 +760,53 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             if (tid == 0) {
                 const uint32_t idx = atomicAdd(&ctl->head[cur], 1u);
                 s_item = idx < n ? __ldcg(a.lists + (size_t)cur * cap + idx) : kInf;
-                s_push[0] = s_push[1] = s_push[2] = s_push[3] = 0;
             }
             __syncthreads();
             const u64 item = s_item;
             if (item == kInf) break;
-            const uint32_t fi = (uint32_t)(item >> 32), t = (uint32_t)item;
-            const DevField f = a.fields[fi];
-            const DevBoard b = a.boards[f.board];
-            const uint32_t L = b.layers;  // the shared tile is laid out for this board's layers
-            const uint32_t nsm = L * SH * SW;  // staged cells (pitch kLabPitch in smem)
-            tile.lab = reinterpret_cast<u64 *>(smem_raw);
-            tile.st = reinterpret_cast<uint32_t *>(tile.lab + L * SH * kLabPitch);
-            tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kStPitch);
-            tile.cold = tile.rowd + L * TH;
-            tile.stackd = tile.cold + L * kTW;
-            tile.fl = tile.stackd + TH * kTW;
-            tile.L = L;
-            const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
-            const uint32_t txi = t % ntx, tyi = t / ntx;
-            const int tx0 = (int)(f.x0 + txi * kTW), ty0 = (int)(f.y0 + tyi * TH);
-            const uint32_t tw = min(kTW, f.ww - txi * kTW), th = min(TH, f.wh - tyi * TH);
-            const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
-            const u64 *lab = a.lab + f.lab_off;
-            if (tid < 5) {
-                uint32_t u = kNone;
-                if (tid == 0) u = t;
-                else if (tid == 1 && txi > 0) u = t - 1;
-                else if (tid == 2 && txi + 1 < ntx) u = t + 1;
-                else if (tid == 3 && tyi > 0) u = t - ntx;
-                else if (tid == 4 && tyi + 1 < nty) u = t + ntx;
-                s_vis[tid] = u == kNone ? 0u : __ldcg(a.tvisit + f.tile_off + u);
-            }
-            if (f.n_pads <= kPadCache)
-                for (uint32_t i = tid; i < f.n_pads; i += blockDim.x) s_pads[i] = __ldg(a.pads + f.pad_off + i);
-            if (f.n_vpads <= kVPadCache)
-                for (uint32_t i = tid; i < f.n_vpads; i += blockDim.x) s_vpads[i] = __ldg(a.pads + f.vpad_off + i);
-            const uint32_t *gpads = a.pads + f.pad_off, *gvpads = a.pads + f.vpad_off;
-            auto is_own_pad = [&](uint32_t c) {
-                return c == f.src || c == f.dst || own_pad(s_pads, kPadCache, gpads, f.n_pads, c);
-            };
-            auto via_blk = [&](uint32_t c, uint8_t gf) {
-                if (gf & kViaNode) return true;
-                return (gf & kStaticVia) != 0 && !own_pad(s_vpads, kVPadCache, gvpads, f.n_vpads, c);
-            };
-            __syncthreads();
-
-            // ---- stage labels and flag bytes (tile + halo ring) ---------------
-            // Every thread issues the loads of kStageUnroll cells before it
-            // stores any of them, so several L2 requests per thread are in
-            // flight (labels through L2 with ld.global.cg).
-            const uint32_t plane = b.w * b.h;
-            for (uint32_t i0 = tid; i0 < nsm; i0 += kStageUnroll * blockDim.x) {
-                u64 lv[kStageUnroll];
-                uint8_t fv[kStageUnroll];
-#pragma unroll
-                for (int k = 0; k < kStageUnroll; ++k) {
-                    const uint32_t i = i0 + k * blockDim.x;
-                    lv[k] = kInf;
-                    fv[k] = 0;
-                    if (i >= nsm) continue;
-                    const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
-                    const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
-                    if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1) {
-                        const bool hx = sx == 0 || sx == SW - 1, hy = sy == 0 || sy == SH - 1;
-                        uint32_t owner;  // which tile's label this smem cell holds
-                        if (hx && hy) owner = 5;  // corner: never read
-                        else if (sx == 0) owner = 1;
-                        else if (sx == SW - 1) owner = 2;
-                        else if (sy == 0) owner = 3;
-                        else if (sy == SH - 1) owner = 4;
-                        else owner = 0;
-                        const uint32_t gcell = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-                        const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0);
-                        if (owner < 5 && s_vis[owner]) lv[k] = __ldcg(lab + lc);
-                        else if (owner == 0 && gcell == f.src) lv[k] = 0;  // first visit of the source tile
-                        if (b.flags) fv[k] = __ldg(b.flags + gcell);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < kStageUnroll; ++k) {
-                    const uint32_t i = i0 + k * blockDim.x;
-                    if (i >= nsm) continue;
-                    const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
-                    tile.lab[tile.li(l, sy, sx)] = lv[k];
-                    tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
-                }
-            }
-            // ---- step prices into every interior cell -------------------------
-            // Phase 1: independent loads only: per interior cell its cost
-            // (parked in the below-plane) and its four planar base prices
-            // (directed in-prices or axis gaps).
-            const uint32_t ncell = L * TH * kTW;
-            for (uint32_t i0 = tid; i0 < ncell; i0 += kStageUnroll * blockDim.x) {
-                uint32_t c[kStageUnroll], p0[kStageUnroll], p1[kStageUnroll], p2[kStageUnroll], p3[kStageUnroll];
-#pragma unroll
-                for (int k = 0; k < kStageUnroll; ++k) {
-                    const uint32_t i = i0 + k * blockDim.x;
-                    c[k] = p0[k] = p1[k] = p2[k] = p3[k] = kMax;
-                    if (i >= ncell) continue;
-                    const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-                    const int gx = tx0 + (int)x, gy = ty0 + (int)y;
-                    if (gx < wx1 && gy < wy1) {
-                        const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-                        c[k] = __ldg(b.cost + gc);
-                        if (b.directed) {
-                            const uint4 d4 = __ldg(b.directed + gc);
-                            p0[k] = d4.y;  // from -x
-                            p1[k] = d4.z;  // from +x
-                            p2[k] = d4.x;  // from -y
-                            p3[k] = d4.w;  // from +y
-                        } else {
-                            if (gx > wx0) p0[k] = __ldg(b.x_edge + gx - 1);
-                            if (gx + 1 < wx1) p1[k] = __ldg(b.x_edge + gx);
-                            if (gy > wy0) p2[k] = __ldg(b.y_edge + gy - 1);
-                            if (gy + 1 < wy1) p3[k] = __ldg(b.y_edge + gy);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < kStageUnroll; ++k) {
-                    const uint32_t i = i0 + k * blockDim.x;
-                    if (i >= ncell) continue;
-                    const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-                    tile.st[tile.si(kFromNegX, l, y, x)] = p0[k];
-                    tile.st[tile.si(kFromPosX, l, y, x)] = p1[k];
-                    tile.st[tile.si(kFromNegY, l, y, x)] = p2[k];
-                    tile.st[tile.si(kFromPosY, l, y, x)] = p3[k];
-                    tile.st[tile.si(kFromBelow, l, y, x)] = c[k];
-                }
-            }
-            __syncthreads();
-            // Phase 2: every step price from the staged bytes (own pads and via
-            // exemptions are the only global reads left).
-            for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
-                const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-                const int gx = tx0 + (int)x, gy = ty0 + (int)y;
-                uint32_t s0 = kMax, s1 = kMax, s2 = kMax, s3 = kMax, s4 = kMax, s5 = kMax;
-                if (gx < wx1 && gy < wy1) {
-                    const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-                    const uint8_t *flr = tile.fl + (l * SH + y + 1) * kFlPitch + x + 1;  // this cell
-                    const uint8_t fc = flr[0];
-                    const uint32_t cost = tile.st[tile.si(kFromBelow, l, y, x)];
-                    uint32_t ec;  // cell_enter on staged values
-                    if (fc & kTraceNode) ec = kMax;
-                    else if (cost != kMax) ec = cost;
-                    else ec = is_own_pad(gc) ? 1u : kMax;
-                    if (ec != kMax) {
-                        const bool dir = b.directed != nullptr;
-                        auto planar = [&](uint32_t base, uint8_t fp, uint8_t out_bit, uint8_t in_bit) -> uint32_t {
-                            if (dir && base == kMax) return kMax;  // blocked directed edge
-                            if ((fp & out_bit) | (fc & in_bit)) return kMax;
-                            return capmul(base, ec);
-                        };
-                        if (gx > wx0) s0 = planar(tile.st[tile.si(kFromNegX, l, y, x)], flr[-1], kEdgePosX, kEdgeNegX);
-                        if (gx + 1 < wx1) s1 = planar(tile.st[tile.si(kFromPosX, l, y, x)], flr[1], kEdgeNegX, kEdgePosX);
-                        if (gy > wy0)
-                            s2 = planar(tile.st[tile.si(kFromNegY, l, y, x)], flr[-(int)kFlPitch], kEdgePosY, kEdgeNegY);
-                        if (gy + 1 < wy1)
-                            s3 = planar(tile.st[tile.si(kFromPosY, l, y, x)], flr[kFlPitch], kEdgeNegY, kEdgePosY);
-                        if (L > 1) {
-                            const bool vc = via_blk(gc, fc);
-                            if (l > 0 && ((b.via_mask >> (l - 1)) & 1u) && !vc) {
-                                const uint8_t fq = flr[-(int)(SH * kFlPitch)];
-                                if (!via_blk(gc - plane, fq)) s4 = capmul(__ldg(b.via_edge + l - 1), ec);
-                            }
-                            if (l + 1 < L && ((b.via_mask >> l) & 1u) && !vc) {
-                                const uint8_t fq = flr[SH * kFlPitch];
-                                if (!via_blk(gc + plane, fq)) s5 = capmul(__ldg(b.via_edge + l), ec);
-                            }
-                        }
-                    }
-                }
-                tile.st[tile.si(kFromNegX, l, y, x)] = s0;
-                tile.st[tile.si(kFromPosX, l, y, x)] = s1;
-                tile.st[tile.si(kFromNegY, l, y, x)] = s2;
-                tile.st[tile.si(kFromPosY, l, y, x)] = s3;
-                tile.st[tile.si(kFromBelow, l, y, x)] = s4;
-                tile.st[tile.si(kFromAbove, l, y, x)] = s5;
-            }
-            for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 1;
-            __syncthreads();
-
-            // ---- relax to local convergence ---------------------------------
-            const uint32_t sweep_limit = L * kTW * TH + 4;
-            uint32_t sweep = 0;
-            for (;;) {
-                const bool ch = relax_tile<TH>(tile);
-                ++sweep;
-                const int any = __syncthreads_or(ch ? 1 : 0);
-                if (!any) break;
-                if (sweep > sweep_limit) {
-                    if (tid == 0) atomicOr(&ctl->status, kStatusRoundLimit);
-                    break;
-                }
-            }
-
-            // ---- write back and find neighbours this tile can improve -------
-            u64 *labw = a.lab + f.lab_off;
-            for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
-                const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
-                const uint64_t lc =
-                    ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-                labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
-            }
-            // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
-            const uint32_t nb = 2 * L * th + 2 * L * tw;
-            for (uint32_t i = tid; i < nb; i += blockDim.x) {
-                uint32_t side, l, k;
-                if (i < 2 * L * th) {
-                    side = i / (L * th);
-                    const uint32_t r = i % (L * th);
-                    l = r / th;
-                    k = r % th;
-                } else {
-                    const uint32_t j = i - 2 * L * th;
-                    side = 2 + j / (L * tw);
-                    const uint32_t r = j % (L * tw);
-                    l = r / tw;
-                    k = r % tw;
-                }
-                bool exists;
-                uint32_t bsx, bsy, nsx, nsy, dir;
-                uint8_t out_bit, in_bit;
-                if (side == 0) {
-                    exists = txi > 0;
-                    bsx = 1; bsy = k + 1; nsx = 0; nsy = bsy;
-                    dir = 2; out_bit = kEdgeNegX; in_bit = kEdgePosX;
-                } else if (side == 1) {
-                    exists = txi + 1 < ntx;
-                    bsx = tw; bsy = k + 1; nsx = tw + 1; nsy = bsy;
-                    dir = 1; out_bit = kEdgePosX; in_bit = kEdgeNegX;
-                } else if (side == 2) {
-                    exists = tyi > 0;
-                    bsx = k + 1; bsy = 1; nsx = bsx; nsy = 0;
-                    dir = 3; out_bit = kEdgeNegY; in_bit = kEdgePosY;
-                } else {
-                    exists = tyi + 1 < nty;
-                    bsx = k + 1; bsy = th; nsx = bsx; nsy = th + 1;
-                    dir = 0; out_bit = kEdgePosY; in_bit = kEdgeNegY;
-                }
-                if (!exists || s_push[side]) continue;
-                const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
-                if (lb == kInf) continue;
-                const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
-                const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
-                const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
-                uint32_t en = kMax;  // cell_enter of the neighbour
-                if (!(fn & kTraceNode)) {
-                    const uint32_t cn = __ldg(b.cost + gn);
-                    en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
-                }
-                if (en == kMax) continue;
-                const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
-                uint32_t gap;
-                if (side == 0) gap = __ldg(b.x_edge + gx_n);
-                else if (side == 1) gap = __ldg(b.x_edge + gx_n - 1);
-                else if (side == 2) gap = __ldg(b.y_edge + gy_n);
-                else gap = __ldg(b.y_edge + gy_n - 1);
-                const u64 cand = ext2(lb, planar_step_g(b, en, fb, fn, out_bit, in_bit, gn, dir, gap), 1);
-                if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
-            }
-            __syncthreads();
-            if (tid < 5) {
-                __threadfence();  // labels before the visited flag and the queue entries
-                if (tid == 4) {
-                    if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
-                    atomicAdd(&ctl->activations, 1ull);
-                    atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
-                } else if (s_push[tid]) {
-                    const uint32_t u = tid == 0 ? t - 1 : tid == 1 ? t + 1 : tid == 2 ? t - ntx : t + ntx;
-                    const uint32_t want = round + 2;  // stamp s = queued for round s-1
-                    if (atomicMax(a.tstamp + f.tile_off + u, want) < want) {
-                        const uint32_t idx = atomicAdd(&ctl->count[nxt], 1u);
-                        if (idx < cap) {
-                            a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | u;
-                        } else {
-                            atomicOr(&ctl->status, kStatusQueueOverflow);
-                        }
-                    }
-                }
-            }
-            __syncthreads();
+            process_item<TH, false>(a, (uint32_t)(item >> 32), (uint32_t)item, round, smem_raw);
         }
         grid_barrier(ctl, gridDim.x);
+    }
+}
+
+// Asynchronous form: no rounds.  Every CTA pops items from one ticketed queue
+// and pushes the neighbours it improves; the launch ends when no item is
+// queued or in flight.  The label arena is +inf-initialised and written with
+// atomicMin, so a tile queued again while a CTA still holds it can be relaxed
+// by two CTAs at once without losing an improvement.
+template <int TH, int NT>
+__global__ void __launch_bounds__(NT) relax_async_kernel(RelaxArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ u64 s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = async_pop(a);
+        __syncthreads();
+        const u64 item = s_item;
+        if (item == kInf) break;
+        process_item<TH, true>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw);
+    }
+}
+
+// Seeds of the asynchronous form: the source label and the source tile of
+// every field whose source is inside its window and enterable.
+template <int TH>
+__global__ void async_seed_kernel(RelaxArgs a) {
+    Ctl *ctl = a.ctl;
+    for (uint32_t fi = blockIdx.x * blockDim.x + threadIdx.x; fi < a.n_fields; fi += gridDim.x * blockDim.x) {
+        const DevField f = a.fields[fi];
+        const DevBoard b = a.boards[f.board];
+        const uint32_t plane = b.w * b.h;
+        const uint32_t sl = f.src / plane, sr = f.src % plane, sx = sr % b.w, sy = sr / b.w;
+        const uint8_t sfl = b.flags ? b.flags[f.src] : 0;
+        if (sx >= f.x0 && sx < f.x0 + f.ww && sy >= f.y0 && sy < f.y0 + f.wh &&
+            cell_enter(b, f, a.pads, f.src, sfl) != kMax) {
+            a.lab[f.lab_off + ((uint64_t)sl * f.wh + (sy - f.y0)) * f.ww + (sx - f.x0)] = 0;
+            const uint32_t ntx = (f.ww + kTW - 1) / kTW;
+            const uint32_t t = ((sy - f.y0) / TH) * ntx + (sx - f.x0) / kTW;
+            __threadfence();
+            async_push(a, fi, f.tile_off, t);
+        }
     }
 }
 
@@ -910,30 +1054,57 @@ size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
 }
 
 namespace {
-const void *relax_fn(uint32_t tile_h, uint32_t threads) {
+template <int TH>
+const void *relax_fn_th(bool wide, bool async) {
+    if (async) return wide ? (const void *)relax_async_kernel<TH, 256> : (const void *)relax_async_kernel<TH, 128>;
+    return wide ? (const void *)relax_rounds_kernel<TH, 256> : (const void *)relax_rounds_kernel<TH, 128>;
+}
+
+const void *relax_fn(uint32_t tile_h, uint32_t threads, bool async) {
     const bool wide = threads >= 256;
     switch (tile_h) {
-        case 8: return wide ? (const void *)relax_rounds_kernel<8, 256> : (const void *)relax_rounds_kernel<8, 128>;
-        case 16: return wide ? (const void *)relax_rounds_kernel<16, 256> : (const void *)relax_rounds_kernel<16, 128>;
-        case 32: return wide ? (const void *)relax_rounds_kernel<32, 256> : (const void *)relax_rounds_kernel<32, 128>;
-        default: return wide ? (const void *)relax_rounds_kernel<64, 256> : (const void *)relax_rounds_kernel<64, 128>;
+        case 8: return relax_fn_th<8>(wide, async);
+        case 16: return relax_fn_th<16>(wide, async);
+        case 32: return relax_fn_th<32>(wide, async);
+        default: return relax_fn_th<64>(wide, async);
+    }
+}
+
+const void *seed_fn(uint32_t tile_h) {
+    switch (tile_h) {
+        case 8: return (const void *)async_seed_kernel<8>;
+        case 16: return (const void *)async_seed_kernel<16>;
+        case 32: return (const void *)async_seed_kernel<32>;
+        default: return (const void *)async_seed_kernel<64>;
     }
 }
 }  // namespace
 
-cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem) {
-    return cudaFuncSetAttribute(relax_fn(tile_h, threads), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async) {
+    return cudaFuncSetAttribute(relax_fn(tile_h, threads, async), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
 }
 
-cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h, threads), (int)threads, smem);
+cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h, threads, async),
+                                                         (int)threads, smem);
 }
 
-cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st) {
-    // Cooperative (all CTAs co-resident, checked by the driver against occupancy);
-    // the attribute form is also what stream capture records as a graph node.
+cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
+                         bool async) {
     RelaxArgs copy = a;
     void *args[] = {&copy};
+    if (async) {
+        // seeds, then the queue-driven kernel (a plain launch: no grid barrier,
+        // and a CTA only takes a ticket while it is resident)
+        if (a.n_fields) {
+            cudaError_t e = cudaLaunchKernel(seed_fn(a.tile_h), dim3((a.n_fields + 255) / 256), dim3(256), args, 0, st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaLaunchKernel(relax_fn(a.tile_h, threads, true), dim3(grid), dim3(threads), args, smem, st);
+    }
+    // Cooperative (all CTAs co-resident, checked by the driver against occupancy);
+    // the attribute form is also what stream capture records as a graph node.
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(threads);
@@ -944,7 +1115,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, relax_fn(a.tile_h, threads), args);
+    return cudaLaunchKernelExC(&cfg, relax_fn(a.tile_h, threads, false), args);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {

@@ -176,6 +176,9 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_batch_autotune": (C.c_int, [vp, vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                              C.POINTER(C.c_float)]),
             "mrc_batch_destroy": (None, [vp]),
+            "mrc_batch_set_schedule": (C.c_int, [vp, vp, C.c_uint32]),
+            "mrc_batch_config": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                           C.POINTER(C.c_uint32)]),
             "mrc_net_windows": (C.c_int, [u32, u32, u32, vp, u32, vp]),
             "mrc_route_instances": (C.c_int, [vp, vp, u32, u32, C.POINTER(vp)]),
             "mrc_batch_create_multi": (C.c_int, [vp, vp, u32, vp, vp, u32, vp, u32, C.POINTER(vp)]),
@@ -398,12 +401,23 @@ class Batch:
         e = self.engine
         e._check(e.lib.mrc_batch_set_config(e.ctx, self.handle, int(tile_h), int(threads)))
 
+    def set_schedule(self, schedule: int) -> None:
+        """0 = bulk-synchronous rounds, 1 = asynchronous work queue."""
+        e = self.engine
+        e._check(e.lib.mrc_batch_set_schedule(e.ctx, self.handle, int(schedule)))
+
+    def config(self) -> dict:
+        th, nt, sc = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self.engine._check(self.engine.lib.mrc_batch_config(self.handle, C.byref(th), C.byref(nt), C.byref(sc)))
+        return {"tile_h": int(th.value), "threads": int(nt.value), "schedule": int(sc.value)}
+
     def autotune(self) -> dict:
-        """Time every relax configuration on this batch and keep the fastest."""
+        """Time every relax configuration (tile height, CTA width, schedule) on
+        this batch and keep the fastest."""
         th, nt, ms = C.c_uint32(), C.c_uint32(), C.c_float()
         e = self.engine
         e._check(e.lib.mrc_batch_autotune(e.ctx, self.handle, C.byref(th), C.byref(nt), C.byref(ms)))
-        return {"tile_h": int(th.value), "threads": int(nt.value), "ms": float(ms.value)}
+        return dict(self.config(), ms=float(ms.value))
 
     def stats(self) -> dict:
         """Work counters of the last launch: tile activations, in-tile sweeps,

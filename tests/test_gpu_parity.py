@@ -269,10 +269,12 @@ def test_edge_cases_and_errors(engine):
     assert paths[0] == [7] and paths[1] is not None
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("tile_cfg", [(8, 128), (8, 256), (16, 128), (16, 256), (32, 128), (32, 256), (64, 128),
                                       (64, 256)])
-def test_every_relax_configuration_is_bit_exact(engine, oracle, tile_cfg):
-    """The autotuner may pick any tile height / CTA width: each must reproduce the oracle."""
+def test_every_relax_configuration_is_bit_exact(engine, oracle, tile_cfg, schedule):
+    """The autotuner may pick any tile height / CTA width / schedule (rounds or
+    the asynchronous queue): each must reproduce the oracle."""
     rng = np.random.default_rng(sum(tile_cfg))
     for trial in range(6):
         req = _random_case(rng, trial, directed=trial % 2 == 1, max_side=90, max_layers=3)
@@ -282,8 +284,31 @@ def test_every_relax_configuration_is_bit_exact(engine, oracle, tile_cfg):
         board = engine.board(req.grid, req.x_edge_costs, req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
         batch = mrcuda.Batch(board, req.nets, req.windows, retry_full=False)
         batch.set_config(*tile_cfg)
+        batch.set_schedule(schedule)
         batch.launch()
         got = batch.finish()
         assert (got.paths, got.search_costs) == exp, (tile_cfg, trial)
         batch.close()
         board.close()
+
+
+@pytest.mark.parametrize("tile_cfg", [(8, 256), (16, 128)])
+def test_queue_schedule_on_the_congestion_board(engine, oracle, tile_cfg):
+    """The asynchronous queue (tiles relaxed by several CTAs at once, labels
+    merged with atomicMin) on all 256 nets of the congestion board, three
+    launches in a row: every path and cost equals the oracle's."""
+    wl = W.congestion_board()
+    req = wl.request()
+    exp = oracle.isolated_batch(req, mode="astar")
+    board = engine.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
+    batch = mrcuda.Batch(board, wl.nets, wl.windows, keep_fields=True)
+    batch.set_config(*tile_cfg)
+    batch.set_schedule(1)
+    for _ in range(3):
+        batch.launch()
+        got = batch.finish()
+        assert got.paths == exp[0] and got.search_costs == exp[1]
+    _assert_fields(oracle, req, got, nets_idx={0, 7, 128, 255})
+    assert batch.config()["schedule"] == 1
+    batch.close()
+    board.close()
