@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
     grid_barrier(ctl, gridDim.x);
 
     for (uint32_t round = 0;; ++round) {
-        const uint32_t cur = round % 3, nxt = (round + 1) % 3, old = (round + 2) % 3;
+        const uint32_t cur = round % 3, old = (round + 2) % 3;
         const uint32_t n = *(volatile uint32_t *)&ctl->count[cur];
         if (n == 0 || ld_status(ctl)) break;
         if (round >= a.round_limit) {
@@ -792,7 +792,6 @@ __global__ void __launch_bounds__(NT) relax_async_kernel(RelaxArgs a) {
 // every field whose source is inside its window and enterable.
 template <int TH>
 __global__ void async_seed_kernel(RelaxArgs a) {
-    Ctl *ctl = a.ctl;
     for (uint32_t fi = blockIdx.x * blockDim.x + threadIdx.x; fi < a.n_fields; fi += gridDim.x * blockDim.x) {
         const DevField f = a.fields[fi];
         const DevBoard b = a.boards[f.board];
