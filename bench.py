@@ -319,7 +319,10 @@ def run_engine(args):
     alg_bytes = wl.algorithmic_bytes() + 4 * path_cells
     relax_avg = statistics.fmean(relax_ms) if relax_ms and min(relax_ms) > 0 else ms
     achieved = alg_bytes / (relax_avg / 1000.0) / 1e9
-    traffic = _traffic_per_launch(f"relax_rounds_{args.workload}.md")
+    sched = batch.config()
+    kname = "relax_async_kernel" if sched["schedule"] == 1 else "relax_rounds_kernel"
+    # DRAM bytes per launch from the committed ncu summary of this kernel and workload
+    traffic = _traffic_per_launch(f"{kname.replace('_kernel', '')}_{args.workload}.md")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -332,7 +335,7 @@ def run_engine(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": batch.kernel_launches * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "relax_rounds_kernel",
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": f"{kname}<{sched['tile_h']},{sched['threads']}>",
                      "kernel_ms": relax_avg, "algorithmic_bytes_per_launch": int(alg_bytes),
                      "bytes_per_cell": round(wl.bytes_per_cell(), 3), "tile_activations": work["activations"],
                      "in_tile_sweeps": work["sweeps"], "rounds": work["rounds"], "tiles": work["tiles"]},
