@@ -210,7 +210,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
 mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t tile_h, uint32_t threads);
 /* The relax schedule: 0 = bulk-synchronous rounds over a shared tile list
  * (cooperative launch, grid barrier between rounds); 1 = one asynchronous
- * work queue (no rounds; labels written with 64-bit atomicMin).  Both give the
+ * work queue (no rounds; a tile held by one CTA at a time).  Both give the
  * same labels and paths.  The autotuner tries both. */
 mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule);
 /* The batch's current tile height, CTA width and schedule. */

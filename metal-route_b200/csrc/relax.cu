@@ -337,15 +337,45 @@ __device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
 // (its tstamp word is the queued flag), so cap = total tiles never overflows.
 constexpr uint32_t kQueueSpinLimit = 1u << 26;
 
-__device__ __forceinline__ void async_push(const RelaxArgs &a, uint32_t fi, uint32_t tile_off, uint32_t u) {
+// Tile states in the tstamp word: 0 idle, 1 queued, 2 held by a CTA,
+// 3 held and improved again meanwhile (the holder queues it once more when it
+// finishes, so improvements that arrive during a relaxation share one
+// re-activation and no tile is ever relaxed by two CTAs at once).
+constexpr uint32_t kTileIdle = 0, kTileQueued = 1, kTileHeld = 2, kTileHeldDirty = 3;
+
+__device__ __forceinline__ void async_enqueue(const RelaxArgs &a, uint32_t fi, uint32_t u) {
     Ctl *c = a.ctl;
-    if (atomicExch(a.tstamp + tile_off + u, 1u) != 0u) return;  // already queued
-    atomicAdd(&c->count[1], 1u);                                  // in flight before it is visible
+    atomicAdd(&c->count[1], 1u);  // in flight before it is visible
     const uint32_t h = atomicAdd(&c->count[0], 1u);
     const size_t slot = h % a.list_cap;
     a.lists[slot] = ((u64)fi << 32) | u;
     __threadfence();
     atomicExch(a.lists + a.list_cap + slot, (u64)h + 1u);
+}
+
+__device__ __forceinline__ void async_push(const RelaxArgs &a, uint32_t fi, uint32_t tile_off, uint32_t u) {
+    uint32_t *st = a.tstamp + tile_off + u;
+    for (int tries = 0; tries < 1024; ++tries) {
+        const uint32_t old = atomicCAS(st, kTileIdle, kTileQueued);
+        if (old == kTileIdle) {
+            async_enqueue(a, fi, u);
+            return;
+        }
+        if (old == kTileQueued || old == kTileHeldDirty) return;  // it will read our labels
+        if (atomicCAS(st, kTileHeld, kTileHeldDirty) == kTileHeld) return;
+        // the holder finished in between: try again from idle
+    }
+    atomicOr(&a.ctl->status, kStatusQueueOverflow);  // the state kept changing under us
+}
+
+// Called by the holder after its write-back and pushes: release the tile, or
+// queue it again if a neighbour improved it while it was held.
+__device__ __forceinline__ void async_release(const RelaxArgs &a, uint32_t fi, uint32_t tile_off, uint32_t t) {
+    uint32_t *st = a.tstamp + tile_off + t;
+    if (atomicCAS(st, kTileHeld, kTileIdle) == kTileHeldDirty) {
+        atomicExch(st, kTileQueued);
+        async_enqueue(a, fi, t);
+    }
 }
 
 // Next item for the calling CTA (thread 0), or kInf when no work is left.  The
@@ -401,10 +431,10 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
     const u64 *lab = a.lab + f.lab_off;
     if constexpr (ASYNC) {
-        // leave the queue before reading any label: a neighbour that improves
-        // our halo after this point queues the tile again
+        // hold the tile before reading any label: a neighbour that improves our
+        // halo after this point marks it dirty, and we queue it again when done
         if (tid == 0) {
-            atomicExch(a.tstamp + f.tile_off + t, 0u);
+            atomicExch(a.tstamp + f.tile_off + t, kTileHeld);
             __threadfence();
         }
     } else if (tid < 5) {
@@ -587,39 +617,11 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
 
     // ---- write back and find neighbours this tile can improve -------
     u64 *labw = a.lab + f.lab_off;
-    if constexpr (ASYNC) {
-        // another CTA may hold this tile too (it was queued again while we ran):
-        // only labels that beat the arena are written, with a 64-bit atomicMin
-        for (uint32_t i0 = tid; i0 < L * th * tw; i0 += kStageUnroll * blockDim.x) {
-            u64 nv[kStageUnroll], ov[kStageUnroll];
-#pragma unroll
-            for (int k = 0; k < kStageUnroll; ++k) {
-                const uint32_t i = i0 + k * blockDim.x;
-                nv[k] = ov[k] = kInf;
-                if (i >= L * th * tw) continue;
-                const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
-                nv[k] = tile.lab[tile.li(l, ty + 1, tx + 1)];
-                const uint64_t lc =
-                    ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-                if (nv[k] != kInf) ov[k] = __ldcg(labw + lc);
-            }
-#pragma unroll
-            for (int k = 0; k < kStageUnroll; ++k) {
-                const uint32_t i = i0 + k * blockDim.x;
-                if (i >= L * th * tw || nv[k] >= ov[k]) continue;
-                const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
-                const uint64_t lc =
-                    ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-                atomicMin(labw + lc, nv[k]);
-            }
-        }
-    } else {
-        for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
-            const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
-            const uint64_t lc =
-                ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-            labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
-        }
+    // the tile is held by this CTA alone (both schedules), so plain stores
+    for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
+        const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
+        const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
+        labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
     }
     // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
     const uint32_t nb = 2 * L * th + 2 * L * tw;
@@ -713,6 +715,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     if constexpr (ASYNC) {
         if (tid == 0) {  // this item is done: its own pushes are already counted
             __threadfence();
+            async_release(a, fi, f.tile_off, t);
             atomicSub(&ctl->count[1], 1u);
         }
     }
@@ -772,9 +775,9 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
 
 // Asynchronous form: no rounds.  Every CTA pops items from one ticketed queue
 // and pushes the neighbours it improves; the launch ends when no item is
-// queued or in flight.  The label arena is +inf-initialised and written with
-// atomicMin, so a tile queued again while a CTA still holds it can be relaxed
-// by two CTAs at once without losing an improvement.
+// queued or in flight.  The label arena is +inf-initialised (every label is
+// valid from the start), and a tile is held by one CTA at a time: improvements
+// that reach a held tile mark it dirty and its holder queues it once more.
 template <int TH, int NT>
 __global__ void __launch_bounds__(NT) relax_async_kernel(RelaxArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

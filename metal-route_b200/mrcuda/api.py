@@ -304,7 +304,8 @@ def _take_result(L, res, n: int, fields: bool, layers: int = 1) -> IsolatedBatch
                  if total else np.zeros(0, np.uint32))
         costs = (np.ctypeslib.as_array(L.mrc_result_search_costs(res), shape=(n,)).copy()
                  if n else np.zeros(0, np.uint32))
-        paths = [cells[off[i]:off[i + 1]].tolist() if off[i + 1] > off[i] else None for i in range(n)]
+        cl, ol = cells.tolist(), off.tolist()
+        paths = [cl[ol[i]:ol[i + 1]] if ol[i + 1] > ol[i] else None for i in range(n)]
         out = IsolatedBatchResult(paths, [int(c) for c in costs], retried=int(L.mrc_result_retried(res)))
         wp = L.mrc_result_field_windows(res)
         if n and wp:

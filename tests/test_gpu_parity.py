@@ -223,7 +223,8 @@ def test_deterministic_across_calls_and_batches(engine):
         batch.launch()
         c = batch.finish()
         assert c.paths == a.paths and c.search_costs == a.search_costs
-    assert batch.kernel_launches == 3
+    # relax (+ the seed kernel of the queue schedule), path offsets, path walk
+    assert batch.kernel_launches == 3 + batch.config()["schedule"]
     # every tile height / CTA width the autotuner tries computes the same answer
     tuned = batch.autotune()
     assert tuned["tile_h"] in (8, 16, 32, 64) and tuned["threads"] in (128, 256)
