@@ -464,7 +464,7 @@ def _run_trace(eng, trace, slots, max_batch, boards):
     server's submit -> result-on-host time."""
     import threading
 
-    srv = eng.server(slots=slots, max_batch_requests=max_batch)
+    srv = eng.server(slots=slots, max_batch_requests=max_batch, max_batch_cells=64 << 20)
     for _, wl in trace[:3]:  # warm-up
         srv.wait(srv.submit_resident(boards[wl.meta["board_index"]], wl.nets, wl.windows))
     reqs = [(t, wl) for t, wl in trace]

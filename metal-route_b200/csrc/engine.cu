@@ -1800,6 +1800,7 @@ mrc_status server_launch(mrc_server *s, ServerBatch *b) {
     b->bt.reset(new mrc_batch());
     b->bt->force_tile_h = s->tile_h;
     b->bt->force_threads = s->threads;
+    b->bt->async_q = true;  // the queue schedule: no grid barrier, no co-residency needed
     b->bt->grid_num = (uint32_t)b->slots.size();
     b->bt->grid_div = s->p.slots;
     b->bt->smem_floor = s->smem_floor;
@@ -2012,8 +2013,8 @@ mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, 
         s->threads = kRelaxThreads;
         s->smem_floor = relax_smem_bytes(s->p.max_layers, s->tile_h, true);
         int per_sm = 0;
-        MRC_CUDA(relax_configure(s->tile_h, s->threads, s->smem_floor), "configure relax kernel");
-        MRC_CUDA(relax_occupancy(s->tile_h, s->threads, s->smem_floor, &per_sm), "relax occupancy");
+        MRC_CUDA(relax_configure(s->tile_h, s->threads, s->smem_floor, true), "configure relax kernel");
+        MRC_CUDA(relax_occupancy(s->tile_h, s->threads, s->smem_floor, &per_sm, true), "relax occupancy");
         if ((uint32_t)per_sm * (uint32_t)ctx->sms < s->p.slots) return fail(MRC_ERR_LIMIT, "too many slots");
         s->streams.resize(s->p.slots);
         s->staged.resize(s->p.slots);
