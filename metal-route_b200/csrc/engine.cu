@@ -747,6 +747,7 @@ PathArgs path_args(const mrc_batch *bt) {
     pa.lab = bt->d_lab.as<u64>();
     pa.tvisit = bt->d_tvisit.as<uint32_t>();
     pa.tile_h = bt->tile_h;
+    pa.arena_filled = bt->async_q ? 1u : 0u;
     pa.costs = bt->d_costs.as<uint32_t>();
     pa.lens = bt->d_lens.as<uint32_t>();
     pa.offsets = bt->d_offsets.as<unsigned long long>();
@@ -2248,6 +2249,7 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     pt.lab = in;
     pt.tvisit = d_vis.as<uint32_t>();
     pt.tile_h = kPlainTileH;
+    pt.arena_filled = 0;
     pt.costs = d_costs.as<uint32_t>();
     pt.lens = d_lens.as<uint32_t>();
     pt.offsets = d_off.as<unsigned long long>();
@@ -2542,6 +2544,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     pa.lab = ra.lab;
     pa.tvisit = ra.tvisit;
     pa.tile_h = tile_h;
+    pa.arena_filled = 0;
     pa.costs = reinterpret_cast<uint32_t *>(s + o_costs);
     pa.lens = reinterpret_cast<uint32_t *>(s + o_lens);
     pa.offsets = reinterpret_cast<unsigned long long *>(s + o_offsets);

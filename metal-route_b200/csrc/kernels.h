@@ -44,6 +44,7 @@ struct PathArgs {
     const u64 *lab;
     const uint32_t *tvisit;
     uint32_t tile_h;
+    uint32_t arena_filled;           // 1: the label arena was +inf-filled (queue schedule), tvisit not needed
     uint32_t *costs;                 // [n] by output slot
     uint32_t *lens;                  // [n] by output slot
     unsigned long long *offsets;     // [n+1] by output slot

@@ -817,7 +817,7 @@ __device__ __forceinline__ u64 field_label(const PathArgs &a, const DevField &f,
                                            uint32_t l) {
     const uint32_t ntx = (f.ww + kTW - 1) / kTW;
     const uint32_t t = (ly / a.tile_h) * ntx + lx / kTW;
-    if (!a.tvisit[f.tile_off + t]) return kInf;
+    if (!a.arena_filled && !a.tvisit[f.tile_off + t]) return kInf;
     return a.lab[f.lab_off + ((uint64_t)l * f.wh + ly) * f.ww + lx];
 }
 
