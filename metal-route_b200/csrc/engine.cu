@@ -304,53 +304,6 @@ mrc_status upload(mrc_context *ctx, DBuf &buf, const void *src, size_t bytes, co
     return MRC_OK;
 }
 
-// Host arrays to device buffers through the pinned stage: worker threads copy
-// 4 MB pieces into pinned memory, then one asynchronous copy per buffer.
-struct StagedCopy {
-    void *dst;
-    const void *src;
-    size_t bytes;
-};
-
-mrc_status staged_upload(mrc_context *ctx, const std::vector<StagedCopy> &copies, const char *what) {
-    std::vector<size_t> off(copies.size());
-    size_t total = 0;
-    for (size_t i = 0; i < copies.size(); ++i) {
-        off[i] = total;
-        total += (copies[i].bytes + 255) & ~(size_t)255;
-    }
-    if (!total) return MRC_OK;
-    MRC_CUDA(ctx->stage.reserve(total), "pinned staging buffer");
-    unsigned char *host = static_cast<unsigned char *>(ctx->stage.p);
-    struct Piece {
-        size_t i, at, n;
-    };
-    std::vector<Piece> pieces;
-    const size_t kPiece = 4u << 20;
-    for (size_t i = 0; i < copies.size(); ++i)
-        for (size_t at = 0; at < copies[i].bytes; at += kPiece)
-            pieces.push_back({i, at, std::min(kPiece, copies[i].bytes - at)});
-    std::atomic<size_t> next{0};
-    auto work = [&]() {
-        for (size_t k; (k = next.fetch_add(1)) < pieces.size();) {
-            const Piece &p = pieces[k];
-            std::memcpy(host + off[p.i] + p.at, static_cast<const unsigned char *>(copies[p.i].src) + p.at, p.n);
-        }
-    };
-    const uint32_t nthreads =
-        (uint32_t)std::min<size_t>(pieces.size(), std::max(1u, std::min(8u, std::thread::hardware_concurrency())));
-    std::vector<std::thread> workers;
-    for (uint32_t t = 1; t < nthreads; ++t) workers.emplace_back(work);
-    work();
-    for (auto &t : workers) t.join();
-    for (size_t i = 0; i < copies.size(); ++i)
-        if (copies[i].bytes)
-            MRC_CUDA(cudaMemcpyAsync(copies[i].dst, host + off[i], copies[i].bytes, cudaMemcpyHostToDevice, ctx->stream),
-                     what);
-    MRC_CUDA(cudaEventRecord(ctx->stage.done, ctx->stream), "stage event");
-    return MRC_OK;
-}
-
 // Upload the board and its edge prices; `keep_host` keeps the validation copies.
 mrc_status board_build(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *edges, bool keep_host,
                        mrc_board *b) {
@@ -374,40 +327,32 @@ mrc_status board_build(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *
         g.via_forbidden = g.via_forbidden ? b->viaf.data() : nullptr;
     }
     const size_t n = (size_t)g.n;
+    MRC_TRY(upload(ctx, b->d_cost, g.cost, n * 4, "upload cost"));
+    const bool has_flags = g.board || g.via_forbidden;
+    if (has_flags) {
+        if (g.board) {
+            MRC_TRY(upload(ctx, b->d_flags, g.board, n, "upload board mask"));
+        } else {
+            MRC_TRY(b->d_flags.get(ctx, std::max<size_t>(n, 4), "board flags"));
+            MRC_CUDA(cudaMemsetAsync(b->d_flags.p, 0, n, ctx->stream), "clear flags");
+        }
+        if (g.via_forbidden) {
+            DBuf tmp;
+            MRC_TRY(upload(ctx, tmp, g.via_forbidden, n, "upload via mask"));
+            MRC_CUDA(combine_flags_launch(b->d_flags.as<uint8_t>(), tmp.as<uint8_t>(), n, ctx->stream), "combine masks");
+            MRC_CUDA(cudaStreamSynchronize(ctx->stream), "combine masks");
+        }
+    }
     std::vector<uint32_t> vias(std::max<uint32_t>(ev, 1), 0);
     uint32_t via_mask = 0;
     for (uint32_t k = 0; k < ev; ++k) {
         vias[k] = edges->via_edge_costs[k];
         if (edges->via_allowed[k]) via_mask |= 1u << k;
     }
-    const bool has_flags = g.board || g.via_forbidden;
-    DBuf tmp;
-    MRC_TRY(b->d_cost.get(ctx, std::max<size_t>(n * 4, 4), "cost"));
-    MRC_TRY(b->d_x.get(ctx, std::max<size_t>((size_t)ex * 4, 4), "x edges"));
-    MRC_TRY(b->d_y.get(ctx, std::max<size_t>((size_t)ey * 4, 4), "y edges"));
-    MRC_TRY(b->d_via.get(ctx, vias.size() * 4, "via edges"));
-    std::vector<StagedCopy> copies = {{b->d_cost.p, g.cost, n * 4},
-                                      {b->d_x.p, edges->x_edge_costs, (size_t)ex * 4},
-                                      {b->d_y.p, edges->y_edge_costs, (size_t)ey * 4},
-                                      {b->d_via.p, vias.data(), vias.size() * 4}};
-    if (has_flags) {
-        MRC_TRY(b->d_flags.get(ctx, std::max<size_t>(n, 4), "board flags"));
-        if (g.board) copies.push_back({b->d_flags.p, g.board, n});
-        else MRC_CUDA(cudaMemsetAsync(b->d_flags.p, 0, n, ctx->stream), "clear flags");
-        if (g.via_forbidden) {
-            MRC_TRY(tmp.get(ctx, std::max<size_t>(n, 4), "via mask"));
-            copies.push_back({tmp.p, g.via_forbidden, n});
-        }
-    }
-    if (b->directed) {
-        MRC_TRY(b->d_dir.get(ctx, std::max<size_t>(n * 16, 16), "directed prices"));
-        copies.push_back({b->d_dir.p, edges->directed_in_costs, n * 16});
-    }
-    MRC_TRY(staged_upload(ctx, copies, "upload board"));
-    if (has_flags && g.via_forbidden) {
-        MRC_CUDA(combine_flags_launch(b->d_flags.as<uint8_t>(), tmp.as<uint8_t>(), n, ctx->stream), "combine masks");
-        MRC_CUDA(cudaStreamSynchronize(ctx->stream), "combine masks");
-    }
+    MRC_TRY(upload(ctx, b->d_x, edges->x_edge_costs, (size_t)ex * 4, "upload x edges"));
+    MRC_TRY(upload(ctx, b->d_y, edges->y_edge_costs, (size_t)ey * 4, "upload y edges"));
+    MRC_TRY(upload(ctx, b->d_via, vias.data(), vias.size() * 4, "upload via edges"));
+    if (b->directed) MRC_TRY(upload(ctx, b->d_dir, edges->directed_in_costs, n * 16, "upload directed prices"));
     b->dev.w = g.w;
     b->dev.h = g.h;
     b->dev.layers = g.layers;

@@ -235,6 +235,15 @@ __device__ __forceinline__ bool via_blocked(const DevField &f, const uint32_t *p
 template <int TH>
 __device__ __forceinline__ bool stack_pass(const Tile<TH> &t);
 
+// With 8-row tiles and 4 cells per lane, the row lanes of a layer (8 rows x 8
+// lanes) and its column lanes (32 columns x 2 lanes) fall on the same pair of
+// warps (2p, 2p+1), in every iteration of a pass.  Between the row and column
+// passes those 64 threads synchronise alone (named barrier 1 + p) instead of
+// the whole CTA.
+__device__ __forceinline__ void pair_barrier() {
+    asm volatile("bar.sync %0, 64;" ::"r"(1u + (threadIdx.x >> 6)) : "memory");
+}
+
 // One sweep of a staged tile: rows (4 lanes x 8 cells), columns (TH/8 lanes x
 // 8 cells), layer stacks (one thread each), each forward then backward, only
 // over lines whose dirty flag is set.
@@ -263,7 +272,12 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         },
         [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 33); },
         [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, 31 - pos); });
-    __syncthreads();
+    // rows -> columns: only the warps of the same layers exchange data
+    if constexpr (TH == 8 && kLaneCells == 4) {
+        pair_barrier();
+    } else {
+        __syncthreads();
+    }
     ch |= seg_pass<KC, SC>(
         t.lab, t.st, t.cold, L * 32, false,
         [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
