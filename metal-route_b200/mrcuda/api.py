@@ -283,6 +283,87 @@ class _Marshal:
         return e
 
 
+def _addr(a: Optional[np.ndarray]) -> int:
+    if a is None or a.size == 0:
+        return 0
+    try:
+        return C.addressof(C.c_char.from_buffer(a))
+    except (TypeError, ValueError):  # read-only buffer
+        return a.__array_interface__["data"][0]
+
+
+def _marshal_requests(m: _Marshal, requests: Sequence[IsolatedRouteRequest]):
+    """An array of C requests for many instances at once.  The structs are
+    written as 64-bit words from numpy columns (the layouts of _Grid, _Net,
+    _Window, _Edges and _Request on a 64-bit ABI), so the per-request Python work
+    is collecting a few buffer addresses."""
+    n = len(requests)
+    nets_all = [nt for rq in requests for nt in rq.nets]
+    nn = len(nets_all)
+    reqs = (_Request * max(n, 1))()
+    grids = np.zeros((max(n, 1), C.sizeof(_Grid) // 8), dtype=np.uint64)
+    nets = np.zeros((max(nn, 1), C.sizeof(_Net) // 8), dtype=np.uint64)
+    wins = np.zeros((max(nn, 1), 4), dtype=np.uint32)
+    # pads of every net in one array
+    pad_lists = [nt.passable_pads for nt in nets_all] + [nt.via_passable_pads for nt in nets_all]
+    lens = np.fromiter((len(p) for p in pad_lists), dtype=np.int64, count=len(pad_lists))
+    pads = np.fromiter((c for p in pad_lists for c in p), dtype=np.uint32, count=int(lens.sum()))
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]]) if len(lens) else np.zeros(0, np.int64)
+    m.keep += [reqs, grids, nets, wins, pads]
+    pbase = _addr(pads) if pads.size else 0
+    if nn:
+        nets[:, 0] = (np.fromiter((nt.src for nt in nets_all), np.uint64, nn)
+                      | (np.fromiter((nt.dst for nt in nets_all), np.uint64, nn) << np.uint64(32)))
+        lp, lv = lens[:nn], lens[nn:]
+        nets[:, 1] = np.where(lp > 0, pbase + 4 * starts[:nn], 0).astype(np.uint64)
+        nets[:, 2] = lp.astype(np.uint64)
+        nets[:, 3] = np.where(lv > 0, pbase + 4 * starts[nn:], 0).astype(np.uint64)
+        nets[:, 4] = lv.astype(np.uint64)
+        wins[:] = np.array([(w.x0, w.y0, w.x1, w.y1) for rq in requests for w in rq.windows],
+                           dtype=np.uint32).reshape(-1, 4)
+    rw = np.frombuffer(reqs, dtype=np.uint64).reshape(max(n, 1), C.sizeof(_Request) // 8)
+    gbase, nbase, wbase = _addr(grids), _addr(nets), _addr(wins)
+    # the small edge vectors of every request in one array each
+    xs = [_u32(rq.x_edge_costs) for rq in requests]
+    ys = [_u32(rq.y_edge_costs) for rq in requests]
+    vv = [_via_arrays(rq.via_edge_costs) for rq in requests]
+    xa = np.concatenate(xs) if n else np.zeros(0, np.uint32)
+    ya = np.concatenate(ys) if n else np.zeros(0, np.uint32)
+    vea = np.concatenate([v[0] for v in vv]) if n else np.zeros(0, np.uint32)
+    vaa = np.concatenate([v[1] for v in vv]) if n else np.zeros(0, np.uint8)
+    m.keep += [xa, ya, vea, vaa]
+    xb, yb, veb, vab = _addr(xa), _addr(ya), _addr(vea), _addr(vaa)
+    first = xo = yo = vo = 0
+    cols = [[] for _ in range(12)]
+    gcols = [[] for _ in range(5)]
+    for k, rq in enumerate(requests):
+        if len(rq.windows) != len(rq.nets):
+            raise BackendUnavailable("isolated request windows are not net-aligned")
+        g = rq.grid
+        nx, ny, nv = xs[k].size, ys[k].size, vv[k][0].size
+        d = None if rq.directed_in_costs is None else _u32(rq.directed_in_costs)
+        m.keep += [g.cost, g.board_constraint, g.via_forbidden, d]
+        gcols[0].append(g.dims.w | (g.dims.h << 32))
+        gcols[1].append(g.dims.layers)
+        gcols[2].append(_addr(g.cost))
+        gcols[3].append(_addr(g.board_constraint))
+        gcols[4].append(_addr(g.via_forbidden))
+        k_n = len(rq.nets)
+        for i, v in enumerate((gbase + k * C.sizeof(_Grid), nbase + first * C.sizeof(_Net) if k_n else 0, k_n,
+                               wbase + first * 16 if k_n else 0, xb + 4 * xo if nx else 0, nx,
+                               yb + 4 * yo if ny else 0, ny, veb + 4 * vo if nv else 0, vab + vo if nv else 0,
+                               nv, _addr(d))):
+            cols[i].append(v)
+        first += k_n
+        xo, yo, vo = xo + nx, yo + ny, vo + nv
+    if n:
+        for i in range(5):
+            grids[:n, i] = np.array(gcols[i], dtype=np.uint64)
+        for i in range(12):
+            rw[:n, i] = np.array(cols[i], dtype=np.uint64)
+    return reqs
+
+
 @dataclass
 class IsolatedBatchResult:
     """Per-net outputs, aligned with the request's nets."""
@@ -306,10 +387,11 @@ def _take_result(L, res, n: int, fields: bool, layers: int = 1) -> IsolatedBatch
                  if n else np.zeros(0, np.uint32))
         cl, ol = cells.tolist(), off.tolist()
         paths = [cl[ol[i]:ol[i + 1]] if ol[i + 1] > ol[i] else None for i in range(n)]
-        out = IsolatedBatchResult(paths, [int(c) for c in costs], retried=int(L.mrc_result_retried(res)))
+        out = IsolatedBatchResult(paths, costs.tolist(), retried=int(L.mrc_result_retried(res)))
         wp = L.mrc_result_field_windows(res)
         if n and wp:
-            out.field_windows = [IsolatedRouteWindow(wp[i].x0, wp[i].y0, wp[i].x1, wp[i].y1) for i in range(n)]
+            wa = np.ctypeslib.as_array(C.cast(wp, C.POINTER(C.c_uint32)), shape=(n * 4,)).tolist()
+            out.field_windows = [IsolatedRouteWindow(*wa[4 * i:4 * i + 4]) for i in range(n)]
         if fields:
             fo = np.ctypeslib.as_array(L.mrc_result_field_offsets(res), shape=(n + 1,)).copy()
             ft = int(fo[-1])
@@ -631,9 +713,7 @@ class Engine:
         """Solve many independent instances (own board, nets, windows) in one
         persistent launch; one result per instance."""
         m = _Marshal()
-        reqs = (_Request * max(len(requests), 1))()
-        for k, rq in enumerate(requests):
-            reqs[k] = self._request(m, rq)
+        reqs = _marshal_requests(m, requests)
         flags = (MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
         res = C.c_void_p()
         self._check(self.lib.mrc_route_instances(self.ctx, C.cast(reqs, C.c_void_p), len(requests), flags,

@@ -52,3 +52,48 @@ def test_no_device_is_an_error_not_a_fallback():
         pytest.skip("GPU present")
     with pytest.raises(mrcuda.BackendUnavailable):
         mrcuda.Engine(0)
+
+
+def test_many_request_marshalling_matches_the_struct_path():
+    """route_instances writes its C request array from numpy columns; every field
+    (grid, edge vectors, via prices and masks, nets, pads, windows) must equal
+    what the one-request struct path writes."""
+    import ctypes as C
+
+    import numpy as np
+
+    from mrcuda import api
+    from mrcuda import workloads as W
+    from mrcuda.types import Dims, Grid, IsolatedRouteRequest, IsolatedRouteWindow, NetEndpoints
+
+    reqs = W.uneven_instances(seed=21, n_instances=24).requests()
+    dims = Dims(6, 4, 3)
+    reqs.append(IsolatedRouteRequest(Grid.filled(dims, 2), [NetEndpoints("a", 1, 70, [5, 70], [70])],
+                                     [IsolatedRouteWindow(0, 0, 5, 3)], [3] * 5, [4] * 3, [None, 9],
+                                     np.arange(len(dims) * 4, dtype=np.uint32)))
+    reqs.append(IsolatedRouteRequest(Grid.filled(Dims(1, 1, 1), 1), [], [], [], [], []))
+
+    def dump(rq):
+        g = rq.grid.contents
+        e = rq.edges
+        out = [g.w, g.h, g.layers, g.cost, g.board_constraint, g.via_forbidden, rq.n_nets, e.n_x_edge_costs,
+               e.n_y_edge_costs, e.n_via_edge_costs, e.directed_in_costs]
+        for ptr, cnt, typ in ((e.x_edge_costs, e.n_x_edge_costs, C.c_uint32), (e.y_edge_costs, e.n_y_edge_costs, C.c_uint32),
+                              (e.via_edge_costs, e.n_via_edge_costs, C.c_uint32), (e.via_allowed, e.n_via_edge_costs, C.c_uint8)):
+            p = C.cast(ptr, C.POINTER(typ))
+            out.append(tuple(p[j] for j in range(cnt)))
+        nets = C.cast(rq.nets, C.POINTER(api._Net))
+        wins = C.cast(rq.windows, C.POINTER(api._Window))
+        for i in range(rq.n_nets):
+            nt = nets[i]
+            pp = C.cast(nt.passable_pads, C.POINTER(C.c_uint32))
+            vp = C.cast(nt.via_passable_pads, C.POINTER(C.c_uint32))
+            out += [nt.src, nt.dst, tuple(pp[j] for j in range(nt.n_passable_pads)),
+                    tuple(vp[j] for j in range(nt.n_via_passable_pads)), (wins[i].x0, wins[i].y0, wins[i].x1, wins[i].y1)]
+        return out
+
+    m = api._Marshal()
+    fast = api._marshal_requests(m, reqs)
+    m2 = api._Marshal()
+    for k, r in enumerate(reqs):
+        assert dump(fast[k]) == dump(api.Engine._request(None, m2, r)), k
