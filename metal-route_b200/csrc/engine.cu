@@ -56,8 +56,20 @@ mrc_status fail(mrc_status s, std::string msg) {
 class Pool {
    public:
     ~Pool() { trim(); }
-    cudaError_t alloc(size_t bytes, void **out) {
+    // Sizes above 1 MiB are rounded up to quarter-octave classes (2^k x 1,
+    // 1.25, 1.5, 1.75), so blocks freed by one batch fit the next batches of
+    // similar size and steady serving does not keep calling cudaMalloc (which
+    // can synchronise the device) or cudaFree.
+    static size_t size_class(size_t bytes) {
         bytes = std::max<size_t>((bytes + 255) & ~(size_t)255, 256);
+        if (bytes <= (1u << 20)) return bytes;
+        size_t p = 1u << 20;
+        while (p * 2 <= bytes) p *= 2;
+        const size_t q = p / 4;
+        return (bytes + q - 1) / q * q;
+    }
+    cudaError_t alloc(size_t bytes, void **out) {
+        bytes = size_class(bytes);
         auto it = free_.lower_bound(bytes);
         if (it != free_.end() && it->first <= 2 * bytes + (8u << 20)) {
             *out = it->second;
