@@ -45,6 +45,15 @@ constexpr int kStageUnroll = 4;    // cells whose loads one thread issues togeth
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
+// Asynchronous 4-byte global -> shared copy (cp.async, L1-allocating) and its
+// completion wait.
+__device__ __forceinline__ void cp_async4(uint32_t *smem, const uint32_t *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Label extended by a run of `h` steps whose prices sum to `d` (kMax = blocked or
 // saturated); a dist reaching 0xFFFFFFFF is unreachable.
 __device__ __forceinline__ u64 ext2(u64 t, uint32_t d, uint32_t h) {
@@ -475,6 +484,40 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     };
     __syncthreads();
 
+    // ---- step prices into every interior cell: phase 1 -----------------
+    // Per interior cell its cost (parked in the below-plane) and its four
+    // planar base prices go global -> shared with asynchronous copies issued
+    // first, so they overlap the label and flag loads below.  The board is
+    // read-only during the launch, so the L1-allocating cp.async is safe for it
+    // (labels, which other CTAs write, keep their L2-only loads).
+    const uint32_t ncell = L * TH * kTW;
+    for (uint32_t i = tid; i < ncell; i += blockDim.x) {
+        const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+        const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+        uint32_t *d0 = &tile.st[tile.si(kFromNegX, l, y, x)], *d1 = &tile.st[tile.si(kFromPosX, l, y, x)];
+        uint32_t *d2 = &tile.st[tile.si(kFromNegY, l, y, x)], *d3 = &tile.st[tile.si(kFromPosY, l, y, x)];
+        uint32_t *dc = &tile.st[tile.si(kFromBelow, l, y, x)];
+        if (gx < wx1 && gy < wy1) {
+            const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+            cp_async4(dc, b.cost + gc);
+            if (b.directed) {
+                const uint32_t *dp = reinterpret_cast<const uint32_t *>(b.directed + gc);
+                cp_async4(d0, dp + 1);  // from -x
+                cp_async4(d1, dp + 2);  // from +x
+                cp_async4(d2, dp + 0);  // from -y
+                cp_async4(d3, dp + 3);  // from +y
+            } else {
+                *d0 = gx > wx0 ? __ldg(b.x_edge + gx - 1) : kMax;
+                *d1 = gx + 1 < wx1 ? __ldg(b.x_edge + gx) : kMax;
+                *d2 = gy > wy0 ? __ldg(b.y_edge + gy - 1) : kMax;
+                *d3 = gy + 1 < wy1 ? __ldg(b.y_edge + gy) : kMax;
+            }
+        } else {
+            *d0 = *d1 = *d2 = *d3 = *dc = kMax;
+        }
+    }
+    cp_async_commit();
+
     // ---- stage labels and flag bytes (tile + halo ring) ---------------
     // Every thread issues the loads of kStageUnroll cells before it
     // stores any of them, so several L2 requests per thread are in
@@ -520,49 +563,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
         }
     }
-    // ---- step prices into every interior cell -------------------------
-    // Phase 1: independent loads only: per interior cell its cost
-    // (parked in the below-plane) and its four planar base prices
-    // (directed in-prices or axis gaps).
-    const uint32_t ncell = L * TH * kTW;
-    for (uint32_t i0 = tid; i0 < ncell; i0 += kStageUnroll * blockDim.x) {
-        uint32_t c[kStageUnroll], p0[kStageUnroll], p1[kStageUnroll], p2[kStageUnroll], p3[kStageUnroll];
-#pragma unroll
-        for (int k = 0; k < kStageUnroll; ++k) {
-            const uint32_t i = i0 + k * blockDim.x;
-            c[k] = p0[k] = p1[k] = p2[k] = p3[k] = kMax;
-            if (i >= ncell) continue;
-            const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-            const int gx = tx0 + (int)x, gy = ty0 + (int)y;
-            if (gx < wx1 && gy < wy1) {
-                const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-                c[k] = __ldg(b.cost + gc);
-                if (b.directed) {
-                    const uint4 d4 = __ldg(b.directed + gc);
-                    p0[k] = d4.y;  // from -x
-                    p1[k] = d4.z;  // from +x
-                    p2[k] = d4.x;  // from -y
-                    p3[k] = d4.w;  // from +y
-                } else {
-                    if (gx > wx0) p0[k] = __ldg(b.x_edge + gx - 1);
-                    if (gx + 1 < wx1) p1[k] = __ldg(b.x_edge + gx);
-                    if (gy > wy0) p2[k] = __ldg(b.y_edge + gy - 1);
-                    if (gy + 1 < wy1) p3[k] = __ldg(b.y_edge + gy);
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kStageUnroll; ++k) {
-            const uint32_t i = i0 + k * blockDim.x;
-            if (i >= ncell) continue;
-            const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-            tile.st[tile.si(kFromNegX, l, y, x)] = p0[k];
-            tile.st[tile.si(kFromPosX, l, y, x)] = p1[k];
-            tile.st[tile.si(kFromNegY, l, y, x)] = p2[k];
-            tile.st[tile.si(kFromPosY, l, y, x)] = p3[k];
-            tile.st[tile.si(kFromBelow, l, y, x)] = c[k];
-        }
-    }
+    cp_async_wait_all();  // the board words copied before the label loop
     __syncthreads();
     // Phase 2: every step price from the staged bytes (own pads and via
     // exemptions are the only global reads left).
