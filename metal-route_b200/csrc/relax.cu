@@ -934,6 +934,55 @@ __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevFiel
     return capmul(base, ec);
 }
 
+// global_step for the path walk with every load issued before any is used
+// (the flags of both cells, the enter cost and the base price), so a step costs
+// one memory round trip instead of a chain of dependent ones.
+__device__ __forceinline__ uint32_t walk_step(const DevBoard &b, const DevField &f, const uint32_t *pads,
+                                              uint32_t p, uint32_t cur, int kind) {
+    const uint32_t plane = b.w * b.h;
+    const uint32_t r = cur % plane, x = r % b.w, y = r / b.w, l = cur / plane;
+    const uint8_t fc = b.flags ? __ldg(b.flags + cur) : 0, fp = b.flags ? __ldg(b.flags + p) : 0;
+    const uint32_t cc = __ldg(b.cost + cur);
+    uint32_t base = 0;
+    if (kind == 0) base = __ldg(b.via_edge + l - 1);
+    else if (kind == 5) base = __ldg(b.via_edge + l);
+    else if (b.directed) base = __ldg(reinterpret_cast<const uint32_t *>(b.directed + cur) + (kind == 1 ? 0 : kind == 2 ? 1 : kind == 3 ? 2 : 3));
+    else if (kind == 1) base = __ldg(b.y_edge + y - 1);
+    else if (kind == 2) base = __ldg(b.x_edge + x - 1);
+    else if (kind == 3) base = __ldg(b.x_edge + x);
+    else base = __ldg(b.y_edge + y);
+    // cell_enter on the loaded values
+    uint32_t ec;
+    if (fc & kTraceNode) ec = kMax;
+    else if (cc != kMax) ec = cc;
+    else ec = (cur == f.src || cur == f.dst || sorted_has(pads + f.pad_off, f.n_pads, cur)) ? 1u : kMax;
+    if (ec == kMax) return kMax;
+    if (kind == 0 || kind == 5) {
+        const uint32_t k = kind == 0 ? l - 1 : l;
+        if (!((b.via_mask >> k) & 1u)) return kMax;
+        const uint8_t tc = cell_tile_flags(f, pads, cur, fc), tp = cell_tile_flags(f, pads, p, fp);
+        if ((tc | tp) & kViaBlocked) return kMax;
+        return capmul(base, ec);
+    }
+    uint8_t out_bit, in_bit;
+    if (kind == 1) {
+        out_bit = kEdgePosY;
+        in_bit = kEdgeNegY;
+    } else if (kind == 2) {
+        out_bit = kEdgePosX;
+        in_bit = kEdgeNegX;
+    } else if (kind == 3) {
+        out_bit = kEdgeNegX;
+        in_bit = kEdgePosX;
+    } else {
+        out_bit = kEdgeNegY;
+        in_bit = kEdgePosY;
+    }
+    if ((fp & out_bit) | (fc & in_bit)) return kMax;
+    if (b.directed && base == kMax) return kMax;
+    return capmul(base, ec);
+}
+
 // One warp per field: lanes 0..5 test the six neighbours (ascending CellIdx)
 // and the lowest qualifying one is the canonical predecessor.  Each step issues
 // all of its loads at once (the candidate's label and tile flag, and the step
@@ -979,7 +1028,7 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
                 const uint32_t lx = (uint32_t)px - f.x0, ly = (uint32_t)py - f.y0;
                 const uint32_t vis = a.tvisit[f.tile_off + (ly / a.tile_h) * ntx + lx / kTW];
                 const u64 raw = a.lab[f.lab_off + ((uint64_t)pl * f.wh + ly) * f.ww + lx];
-                const uint32_t st = global_step(b, f, a.pads, p, cur, (int)lane);
+                const uint32_t st = walk_step(b, f, a.pads, p, cur, (int)lane);
                 lp = vis ? raw : kInf;
                 ok = lp != kInf && extend(lp, st) == need;
             }
