@@ -482,6 +482,11 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         if (gf & kViaNode) return true;
         return (gf & kStaticVia) != 0 && !own_pad(s_vpads, kVPadCache, gvpads, f.n_vpads, c);
     };
+    // Dirty lines start clear; staging marks exactly the lines that hold a
+    // finite label (in the tile, or at their ends in the halo ring): a line of
+    // +inf labels with +inf ends cannot change until a crossing line lowers one
+    // of its cells, and that pass marks it.
+    for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 0;
     __syncthreads();
 
     // ---- step prices into every interior cell: phase 1 -----------------
@@ -561,6 +566,12 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
             tile.lab[tile.li(l, sy, sx)] = lv[k];
             tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
+            if (lv[k] != kInf) {
+                const bool row_in = sy >= 1 && sy <= TH, col_in = sx >= 1 && sx <= kTW;
+                if (row_in) tile.rowd[l * TH + sy - 1] = 1;
+                if (col_in) tile.cold[l * kTW + sx - 1] = 1;
+                if (row_in && col_in) tile.stackd[(sy - 1) * kTW + sx - 1] = 1;
+            }
         }
     }
     cp_async_wait_all();  // the board words copied before the label loop
@@ -613,7 +624,6 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         tile.st[tile.si(kFromBelow, l, y, x)] = s4;
         tile.st[tile.si(kFromAbove, l, y, x)] = s5;
     }
-    for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 1;
     __syncthreads();
 
     // ---- relax to local convergence ---------------------------------
