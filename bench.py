@@ -169,7 +169,7 @@ class ClockSampler:
 
 def _cpu_sample_rate(job, n_sample: int, threads: int = 0):
     """The oracle's A* alone-path search (window, then full board) on a sample of
-    nets, all host threads: nets/s.  Checker code only; never the measured GPU path."""
+    nets, all host threads: nets/s.  Oracle code, timed as the CPU baseline; never the measured GPU path."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     from mrcuda.types import IsolatedRouteRequest

@@ -1179,7 +1179,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
         }
         return cudaLaunchKernel(relax_fn(a.tile_h, threads, true), dim3(grid), dim3(threads), args, smem, st);
     }
-    // Cooperative (all CTAs co-resident, checked by the driver against occupancy);
+    // Cooperative (all CTAs co-resident, checked by the CUDA runtime against occupancy);
     // the attribute form is also what stream capture records as a graph node.
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);

@@ -1,7 +1,7 @@
 /*
  * oracle.h — CPU restatement of metalroute's canonical shortest-path semantics.
  *
- * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA engine in
+ * TEST INFRASTRUCTURE ONLY. This library is the test oracle of the CUDA engine in
  * metal-route_b200/: only tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline leg load it. Nothing in the product links, calls or falls back to it.
  *

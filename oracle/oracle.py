@@ -1,7 +1,7 @@
 """ctypes wrapper around the CPU oracle (oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, as the checker.  The product (the mr_cuda
+CPU-baseline leg of bench.py, as the oracle.  The product (the mr_cuda
 library and its Python binding) never imports this module.
 """
 from __future__ import annotations

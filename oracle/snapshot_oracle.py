@@ -1,7 +1,7 @@
-"""CPU restatement of one snapshot negotiation round (the checker of
-mrc_negotiation_round).
+"""CPU restatement of one snapshot negotiation round: the test oracle of
+mrc_negotiation_round.
 
-TEST INFRASTRUCTURE ONLY: imported by tests/ as the checker; the product never
+TEST INFRASTRUCTURE ONLY: imported by tests/ as the oracle; the product never
 imports it.
 
 The round is the reference's Jacobi negotiation iteration
