@@ -83,3 +83,25 @@ def test_full_size_negotiation_round_properties(engine, oracle):
             assert paths[i] == e_paths[0], (r, i)
         prev_hist = hist
     neg.close()
+
+
+def test_full_board_retry_at_full_size(engine, oracle):
+    """A window that cannot hold the path on the 2048x2048x6 board: the retry
+    solves the whole 25.2 M-cell board, and its path equals the oracle's."""
+    from mrcuda.types import COST_MAX, IsolatedRouteWindow, NetEndpoints
+
+    wl = W.snapshot_board(n_nets=1)
+    dims = wl.grid.dims
+    cost = wl.grid.cost.reshape(dims.layers, dims.h, dims.w).copy()
+    cost[:, 100:2048, 1024] = COST_MAX  # a wall on every layer with its gap at y < 100
+    src, dst = dims.idx3(1000, 1500, 0), dims.idx3(1050, 1500, 0)
+    cost.reshape(-1)[[src, dst]] = 1
+    grid = type(wl.grid)(dims, cost.reshape(-1))
+    net = NetEndpoints("r", src, dst)
+    req = IsolatedRouteRequest(grid, [net], [IsolatedRouteWindow(900, 1400, 1150, 1600)], wl.x, wl.y, wl.vias,
+                               wl.directed)
+    got = engine.route_isolated_batch(req, retry_full=True)
+    assert got.retried == 1 and got.paths[0] is not None
+    exp_paths, exp_costs = oracle.isolated_batch(req, retry_full=True, mode="field")
+    assert got.paths == exp_paths and got.search_costs == exp_costs
+    assert min(dims.xy(c)[1] for c in got.paths[0]) < 100  # it went around through the gap
