@@ -385,10 +385,11 @@ def run_snapshot(args):
     from mrcuda import workloads as W
 
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if rank != 0:  # one board per job: the rounds are not sharded here
-        return 0
+    if world > 1 or args.shards:
+        return run_snapshot_sharded(args, rank, world, local)
     wl = W.snapshot_board(n_nets=args.nets or 3000)
     req = wl.request()
     eng = mrcuda.Engine(local)
@@ -495,6 +496,70 @@ def _run_trace(eng, trace, slots, max_batch, boards):
     return lat, nets, makespan, st
 
 
+def run_snapshot_sharded(args, rank, world, local):
+    """The snapshot negotiation split across ranks: rank r routes the nets
+    i % world == r of the same board, and the occupancy is all-reduced (NCCL)
+    between the phases of every round.  Total work is fixed (strong scaling);
+    every rank runs the same rounds until no rank has a dirty net."""
+    import torch
+
+    import mrcuda
+    from mrcuda import workloads as W
+    from mrcuda.dist import init_from_env, max_over_ranks, sharded_negotiation_round
+
+    dist = init_from_env("nccl", timeout_s=300.0, device=torch.device("cuda", local))
+    reduce = None if dist else (lambda t: None)  # one rank: the global occupancy is its own
+    wl = W.snapshot_board(n_nets=args.nets or 3000)
+    req = wl.request()
+    owned = [i % world == rank for i in range(len(req.nets))]
+    eng = mrcuda.Engine(local)
+
+    def total(v):
+        t = torch.tensor([float(v)], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t)
+        return float(t.item())
+
+    warm = eng.negotiation(req, owned=owned)
+    for _ in range(max(args.warmup, 3)):
+        sharded_negotiation_round(warm, reduce)
+    warm.close()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    shard = eng.negotiation(req, owned=owned)
+    rounds = []
+    for _ in range(args.steps):
+        st = sharded_negotiation_round(shard, reduce)
+        rounds.append(st)
+        if total(st["next_dirty"]) == 0:
+            break
+    torch.cuda.synchronize()
+    wall = max_over_ranks(time.perf_counter() - t0, device="cuda")
+    clk = clocks.stop()
+    routed = total(sum(r["dirty"] for r in rounds))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": routed / wall, "unit": UNIT, "n_gpus": world, "steps": len(rounds),
+            "warmup": max(args.warmup, 3), "ms_per_step": 1000.0 * wall / max(len(rounds), 1),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": wl.meta["workload"] + f", sharded over {world} ranks", "rounds": len(rounds),
+                       "nets_routed": int(routed), "exchange": "all-reduce of the occupancy, twice per round",
+                       "timing": "wall clock of the synchronised round loop, max over ranks"},
+            "e2e": {"value": routed / wall, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+            "gpu_launches": None, "clocks": clk,
+        }
+        print(json.dumps(line))
+    shard.close()
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_serving(args):
     """Serving: Poisson arrivals of congestion-style boards (side log-uniform
     64-1024, 2-6 layers, 16-512 nets) at several rates through the
@@ -563,6 +628,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: seconds of arrivals per rate")
     ap.add_argument("--serve-max", type=int, default=600, help="serving: most requests per rate")
     ap.add_argument("--slots", type=int, default=2, help="serving: launches in flight")
+    ap.add_argument("--shards", action="store_true", help="snapshot: run the sharded rounds even on one rank")
     ap.add_argument("--nets", type=int, default=0, help="route only the first N nets (0 = all)")
     ap.add_argument("--cpu-sample", type=int, default=0, help="nets timed on the CPU (0 = workload default)")
     ap.add_argument("--plain-sample", type=int, default=0, help="nets timed one per launch (0 = workload default)")

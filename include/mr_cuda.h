@@ -331,6 +331,30 @@ mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *
                                   const mrc_negotiation_params *params, mrc_negotiation **out);
 /* Runs the next round.  A round with no dirty net does nothing (converged). */
 mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *neg, mrc_round_stats *stats);
+
+/* Sharded rounds (one shard per GPU, each routing its own nets of the same
+ * board).  A shard keeps the occupancy of its own paths ("local") and a global
+ * occupancy that the caller sets to the sum of every shard's local one (an
+ * all-reduce over NCCL, or a plain sum) between the phases of a round:
+ *   ripup  -> global = sum(local) -> route -> global = sum(local) -> settle.
+ * ripup takes this shard's dirty nets out of its local occupancy; route prices
+ * the snapshot from the global occupancy and history, routes this shard's dirty
+ * nets and merges them into the local occupancy; settle adds history on the
+ * edges the global occupancy overuses (the same on every shard) and finds this
+ * shard's next dirty nets.  The union of the shards' paths equals the paths of
+ * one unsharded negotiation over all nets.  The unsharded object runs the same
+ * three phases inside mrc_negotiation_round with its local occupancy as the
+ * global one.  No counterpart in the reference (its rounds run on one host). */
+mrc_status mrc_negotiation_create_shard(mrc_context *ctx, const mrc_isolated_request *req,
+                                        const mrc_negotiation_params *params, const uint8_t *owned,
+                                        mrc_negotiation **out);
+mrc_status mrc_negotiation_ripup(mrc_context *ctx, mrc_negotiation *neg);
+mrc_status mrc_negotiation_route(mrc_context *ctx, mrc_negotiation *neg, mrc_round_stats *stats);
+mrc_status mrc_negotiation_settle(mrc_context *ctx, mrc_negotiation *neg, mrc_round_stats *stats);
+/* Device addresses of the local and global occupancy (4 u32 per cell; the same
+ * buffer for an unsharded object) and their size in bytes. */
+mrc_status mrc_negotiation_buffers(mrc_negotiation *neg, void **local_present, void **global_present,
+                                   uint64_t *bytes);
 /* Current paths of every net (CSR, request order; an empty path = unrouted).
  * The pointers stay valid until the next round or destroy. */
 mrc_status mrc_negotiation_paths(const mrc_negotiation *neg, uint32_t *n_nets, const uint64_t **offsets,

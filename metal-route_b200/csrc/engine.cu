@@ -1373,8 +1373,14 @@ struct mrc_negotiation {
     std::vector<uint64_t> offsets;     // CSR of `paths` (host copy of d_off/d_cells)
     std::vector<uint32_t> cells;
     std::vector<uint32_t> dirty;       // nets of the next round
+    std::vector<uint8_t> owned;        // nets this object routes (a shard routes a subset)
+    bool sharded = false;              // occupancy of all shards arrives in d_global between phases
     uint32_t round = 0;
+    uint32_t phase = 0;                // 0 ready, 1 ripped up, 2 routed and merged
+    mrc_round_stats pending{};         // statistics of the round in progress
     DBuf d_present, d_history, d_snap, d_off, d_cells, d_list, d_flags, d_count;
+    DBuf d_global;                     // sharded: sum of every shard's d_present
+    const uint4 *global() const { return sharded ? d_global.as<uint4>() : d_present.as<uint4>(); }
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~mrc_negotiation() {
         if (ev0) cudaEventDestroy(ev0);
@@ -1419,8 +1425,25 @@ OccupancyArgs negotiation_occupancy(mrc_negotiation *ng, uint32_t n_list, bool a
 
 extern "C" {
 
+mrc_status negotiation_create(mrc_context *ctx, const mrc_isolated_request *req, const mrc_negotiation_params *params,
+                              const uint8_t *owned, mrc_negotiation **out);
+
 mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *req,
                                   const mrc_negotiation_params *params, mrc_negotiation **out) {
+    return negotiation_create(ctx, req, params, nullptr, out);
+}
+
+mrc_status mrc_negotiation_create_shard(mrc_context *ctx, const mrc_isolated_request *req,
+                                        const mrc_negotiation_params *params, const uint8_t *owned,
+                                        mrc_negotiation **out) {
+    if (!owned) return fail(MRC_ERR_INVALID_ARGUMENT, "owned mask is NULL");
+    return negotiation_create(ctx, req, params, owned, out);
+}
+
+}  // extern "C"
+
+mrc_status negotiation_create(mrc_context *ctx, const mrc_isolated_request *req, const mrc_negotiation_params *params,
+                              const uint8_t *owned, mrc_negotiation **out) {
     if (!ctx || !req || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
     *out = nullptr;
     Lock lock(ctx, 0);
@@ -1468,8 +1491,17 @@ mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *
     ng->snap->dev = ng->base->dev;
     ng->snap->dev.directed = ng->d_snap.as<uint4>();
     ng->paths.assign(n, {});
-    ng->dirty.resize(n);
-    std::iota(ng->dirty.begin(), ng->dirty.end(), 0u);
+    ng->sharded = owned != nullptr;
+    ng->owned.assign(n, 1);
+    if (owned)
+        for (uint32_t i = 0; i < n; ++i) ng->owned[i] = owned[i] ? 1 : 0;
+    if (ng->sharded) {
+        MRC_TRY(ng->d_global.get(ctx, std::max<size_t>(slots, 16), "global occupancy"));
+        MRC_CUDA(cudaMemsetAsync(ng->d_global.p, 0, slots, ctx->stream), "clear global occupancy");
+    }
+    ng->dirty.clear();
+    for (uint32_t i = 0; i < n; ++i)
+        if (ng->owned[i]) ng->dirty.push_back(i);
     MRC_TRY(negotiation_upload_paths(ng.get()));
     MRC_CUDA(cudaEventCreate(&ng->ev0), "create event");
     MRC_CUDA(cudaEventCreate(&ng->ev1), "create event");
@@ -1478,64 +1510,95 @@ mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *
     return MRC_OK;
 }
 
-mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *ng, mrc_round_stats *st) {
-    if (!ctx || !ng || !st) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+extern "C" {
+
+// Phase 1: the dirty nets this object owns leave its occupancy.
+mrc_status mrc_negotiation_ripup(mrc_context *ctx, mrc_negotiation *ng) {
+    if (!ctx || !ng) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ng->phase != 0) return fail(MRC_ERR_INVALID_ARGUMENT, "negotiation phase out of order (rip-up)");
     Lock lock(ctx, 0);
     MRC_TRY(set_device(ctx));
-    std::memset(st, 0, sizeof(*st));
-    st->round = ng->round;
-    st->pfac = 1 + ng->round;
+    std::memset(&ng->pending, 0, sizeof(ng->pending));
+    ng->pending.round = ng->round;
+    ng->pending.pfac = 1 + ng->round;
     const uint32_t n_dirty = (uint32_t)ng->dirty.size();
-    st->dirty = n_dirty;
-    if (!n_dirty) {
-        st->path_cells = ng->cells.size();
-        return MRC_OK;
-    }
-    const GridView &g = ng->base->view;
+    ng->pending.dirty = n_dirty;
     cudaStream_t s = ctx->stream;
     MRC_CUDA(cudaEventRecord(ng->ev0, s), "record event");
-    // 2. rip-up of the dirty nets' current paths
-    MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
-    MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, false), s), "rip-up");
-    // 3. the frozen snapshot
+    if (n_dirty) {
+        MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
+        MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, false), s), "rip-up");
+    }
+    MRC_CUDA(cudaStreamSynchronize(s), "rip-up");
+    ng->phase = 1;
+    return MRC_OK;
+}
+
+// Phase 2: the frozen snapshot from the global occupancy (after every shard's
+// rip-up) and history, the owned dirty nets routed alone on it, and merged
+// into this object's occupancy.
+mrc_status mrc_negotiation_route(mrc_context *ctx, mrc_negotiation *ng, mrc_round_stats *out) {
+    if (!ctx || !ng) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ng->phase != 1) return fail(MRC_ERR_INVALID_ARGUMENT, "negotiation phase out of order (route)");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    mrc_round_stats *st = &ng->pending;
+    const GridView &g = ng->base->view;
+    cudaStream_t s = ctx->stream;
+    const uint32_t n_dirty = (uint32_t)ng->dirty.size();
     SnapshotArgs sa;
     sa.base = ng->base->dev.directed;
-    sa.present = ng->d_present.as<uint4>();
+    sa.present = ng->global();
     sa.history = ng->d_history.as<uint4>();
     sa.out = ng->d_snap.as<uint4>();
     sa.n = g.n;
     sa.pfac = st->pfac;
     sa.weight = ng->params.present_weight;
     MRC_CUDA(snapshot_launch(sa, s), "price snapshot");
-    // 4. the dirty nets, alone on the snapshot (window, then full-board retry)
-    std::vector<NetCopy> nets;
-    std::vector<mrc_window> wins;
-    nets.reserve(n_dirty);
-    for (uint32_t i : ng->dirty) {
-        nets.push_back(ng->nets[i]);
-        wins.push_back(ng->windows[i]);
+    if (n_dirty) {
+        std::vector<NetCopy> nets;
+        std::vector<mrc_window> wins;
+        nets.reserve(n_dirty);
+        for (uint32_t i : ng->dirty) {
+            nets.push_back(ng->nets[i]);
+            wins.push_back(ng->windows[i]);
+        }
+        mrc_result *raw = nullptr;
+        MRC_TRY(solve(ctx, {ng->snap.get()}, std::move(nets), std::move(wins), MRC_FLAG_RETRY_FULL, &raw, nullptr));
+        std::unique_ptr<mrc_result> res(raw);
+        for (uint32_t k = 0; k < n_dirty; ++k) {
+            const uint32_t i = ng->dirty[k];
+            ng->paths[i].assign(res->cells.begin() + res->offsets[k], res->cells.begin() + res->offsets[k + 1]);
+            if (!ng->paths[i].empty()) st->routed++;
+            const mrc_window &w0 = ng->windows[i], &w1 = res->field_windows[k];
+            const uint64_t c0 = (uint64_t)(w0.x1 - w0.x0 + 1) * (w0.y1 - w0.y0 + 1) * g.layers;
+            const bool retried = w1.x0 != w0.x0 || w1.y0 != w0.y0 || w1.x1 != w0.x1 || w1.y1 != w0.y1;
+            st->window_cells += c0 + (retried ? g.n : 0);
+            st->retried += retried;
+        }
+        MRC_TRY(negotiation_upload_paths(ng));
+        MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
+        MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, true), s), "merge paths");
     }
-    mrc_result *raw = nullptr;
-    MRC_TRY(solve(ctx, {ng->snap.get()}, std::move(nets), std::move(wins), MRC_FLAG_RETRY_FULL, &raw, nullptr));
-    std::unique_ptr<mrc_result> res(raw);
-    for (uint32_t k = 0; k < n_dirty; ++k) {
-        const uint32_t i = ng->dirty[k];
-        ng->paths[i].assign(res->cells.begin() + res->offsets[k], res->cells.begin() + res->offsets[k + 1]);
-        if (!ng->paths[i].empty()) st->routed++;
-        const mrc_window &w0 = ng->windows[i], &w1 = res->field_windows[k];
-        const uint64_t c0 = (uint64_t)(w0.x1 - w0.x0 + 1) * (w0.y1 - w0.y0 + 1) * g.layers;
-        const bool retried = w1.x0 != w0.x0 || w1.y0 != w0.y0 || w1.x1 != w0.x1 || w1.y1 != w0.y1;
-        st->window_cells += c0 + (retried ? g.n : 0);
-        st->retried += retried;
-    }
-    // 5. merge: the new paths enter the occupancy
-    MRC_TRY(negotiation_upload_paths(ng));
-    MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
-    MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, true), s), "merge paths");
-    // 6. history on overused edges, then the next dirty set
+    MRC_CUDA(cudaStreamSynchronize(s), "route");
+    ng->phase = 2;
+    if (out) *out = *st;
+    return MRC_OK;
+}
+
+// Phase 3: history on the edges the global occupancy overuses, then the owned
+// nets the next round routes.
+mrc_status mrc_negotiation_settle(mrc_context *ctx, mrc_negotiation *ng, mrc_round_stats *out) {
+    if (!ctx || !ng) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ng->phase != 2) return fail(MRC_ERR_INVALID_ARGUMENT, "negotiation phase out of order (settle)");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    mrc_round_stats *st = &ng->pending;
+    const GridView &g = ng->base->view;
+    cudaStream_t s = ctx->stream;
     MRC_CUDA(cudaMemsetAsync(ng->d_count.p, 0, 8, s), "clear count");
     OveruseArgs oa;
-    oa.present = ng->d_present.as<uint4>();
+    oa.present = ng->global();
     oa.history = ng->d_history.as<uint4>();
     oa.n = g.n;
     oa.step = ng->params.history_step;
@@ -1548,7 +1611,7 @@ mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *ng, mrc_roun
     da.n_nets = n;
     da.w = g.w;
     da.plane = g.w * g.h;
-    da.present = ng->d_present.as<uint32_t>();
+    da.present = reinterpret_cast<const uint32_t *>(ng->global());
     da.flags = ng->d_flags.as<uint8_t>();
     MRC_CUDA(dirty_launch(da, s), "dirty scan");
     MRC_CUDA(cudaEventRecord(ng->ev1, s), "record event");
@@ -1560,12 +1623,39 @@ mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *ng, mrc_roun
     MRC_CUDA(cudaEventElapsedTime(&st->round_ms, ng->ev0, ng->ev1), "round time");
     ng->dirty.clear();
     for (uint32_t i = 0; i < n; ++i)
-        if (flags[i]) ng->dirty.push_back(i);
+        if (flags[i] && ng->owned[i]) ng->dirty.push_back(i);  // the dirty scan marks unrouted nets too
     st->overused_edges = slots / 2;
     st->next_dirty = (uint32_t)ng->dirty.size();
     st->path_cells = ng->cells.size();
     ng->round++;
+    ng->phase = 0;
+    if (out) *out = *st;
     return MRC_OK;
+}
+
+mrc_status mrc_negotiation_buffers(mrc_negotiation *ng, void **local_present, void **global_present,
+                                   uint64_t *bytes) {
+    if (!ng || !local_present || !global_present || !bytes) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *local_present = ng->d_present.p;
+    *global_present = const_cast<uint4 *>(ng->global());
+    *bytes = (uint64_t)ng->base->view.n * 16;
+    return MRC_OK;
+}
+
+// One whole round of an unsharded negotiation (its occupancy is the global one).
+mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *ng, mrc_round_stats *st) {
+    if (!ctx || !ng || !st) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ng->sharded) return fail(MRC_ERR_INVALID_ARGUMENT, "a shard runs its rounds phase by phase");
+    if (ng->dirty.empty()) {  // converged: nothing to do
+        std::memset(st, 0, sizeof(*st));
+        st->round = ng->round;
+        st->pfac = 1 + ng->round;
+        st->path_cells = ng->cells.size();
+        return MRC_OK;
+    }
+    MRC_TRY(mrc_negotiation_ripup(ctx, ng));
+    MRC_TRY(mrc_negotiation_route(ctx, ng, nullptr));
+    return mrc_negotiation_settle(ctx, ng, st);
 }
 
 mrc_status mrc_negotiation_paths(const mrc_negotiation *ng, uint32_t *n_nets, const uint64_t **offsets,

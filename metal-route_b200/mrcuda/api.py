@@ -189,6 +189,12 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_negotiation_read": (C.c_int, [vp, vp, vp, vp, vp]),
             "mrc_negotiation_dirty": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32p)]),
             "mrc_negotiation_destroy": (None, [vp]),
+            "mrc_negotiation_create_shard": (C.c_int, [vp, C.POINTER(_Request), C.POINTER(_NegParams), vp,
+                                                       C.POINTER(vp)]),
+            "mrc_negotiation_ripup": (C.c_int, [vp, vp]),
+            "mrc_negotiation_route": (C.c_int, [vp, vp, C.POINTER(_RoundStats)]),
+            "mrc_negotiation_settle": (C.c_int, [vp, vp, C.POINTER(_RoundStats)]),
+            "mrc_negotiation_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_uint64)]),
             "mrc_server_create": (C.c_int, [vp, C.POINTER(_ServerParams), C.POINTER(vp)]),
             "mrc_server_submit": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(C.c_uint64)]),
             "mrc_server_submit_resident": (C.c_int, [vp, vp, vp, u32, vp, u32, C.POINTER(C.c_uint64)]),
@@ -537,23 +543,64 @@ class Negotiation:
     history_step to every edge two or more nets use."""
 
     def __init__(self, engine: "Engine", req: IsolatedRouteRequest, present_weight: int = 16,
-                 history_step: int = 1):
+                 history_step: int = 1, owned: Optional[Sequence[bool]] = None):
         self.engine = engine
         self.n = len(req.nets)
         self.dims = req.grid.dims
         m = _Marshal()
         r = engine._request(m, req)
         h = C.c_void_p()
-        engine._check(engine.lib.mrc_negotiation_create(engine.ctx, C.byref(r),
-                                                        C.byref(_NegParams(present_weight, history_step)),
-                                                        C.byref(h)))
+        prm = C.byref(_NegParams(present_weight, history_step))
+        if owned is None:
+            engine._check(engine.lib.mrc_negotiation_create(engine.ctx, C.byref(r), prm, C.byref(h)))
+        else:
+            mask = np.ascontiguousarray(np.asarray(owned, dtype=np.uint8))
+            if mask.size != self.n:
+                raise InvalidArgument("owned mask must have one entry per net")
+            engine._check(engine.lib.mrc_negotiation_create_shard(engine.ctx, C.byref(r), prm, m.arr(mask),
+                                                                  C.byref(h)))
         self.handle = h
+
+    @staticmethod
+    def _stats(st) -> dict:
+        return {f: getattr(st, f) for f, _ in _RoundStats._fields_}
 
     def round(self) -> dict:
         st = _RoundStats()
         e = self.engine
         e._check(e.lib.mrc_negotiation_round(e.ctx, self.handle, C.byref(st)))
-        return {f: getattr(st, f) for f, _ in _RoundStats._fields_}
+        return self._stats(st)
+
+    # -- the phases of a sharded round ----------------------------------------
+    def ripup(self) -> None:
+        self.engine._check(self.engine.lib.mrc_negotiation_ripup(self.engine.ctx, self.handle))
+
+    def route(self) -> dict:
+        st = _RoundStats()
+        self.engine._check(self.engine.lib.mrc_negotiation_route(self.engine.ctx, self.handle, C.byref(st)))
+        return self._stats(st)
+
+    def settle(self) -> dict:
+        st = _RoundStats()
+        self.engine._check(self.engine.lib.mrc_negotiation_settle(self.engine.ctx, self.handle, C.byref(st)))
+        return self._stats(st)
+
+    def occupancy(self):
+        """(local, global) occupancy as int32 CUDA tensors of 4 slots per cell,
+        sharing the engine's device memory (for an all-reduce between phases)."""
+        import torch
+
+        loc, glo, nbytes = C.c_void_p(), C.c_void_p(), C.c_uint64()
+        self.engine._check(self.engine.lib.mrc_negotiation_buffers(self.handle, C.byref(loc), C.byref(glo),
+                                                                   C.byref(nbytes)))
+        n = int(nbytes.value) // 4
+
+        class _Dev:
+            def __init__(self, ptr):
+                self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False),
+                                                 "version": 3}
+
+        return (torch.as_tensor(_Dev(loc.value), device="cuda"), torch.as_tensor(_Dev(glo.value), device="cuda"))
 
     def paths(self) -> List[Optional[List[int]]]:
         n, off, cells = C.c_uint32(), C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
@@ -770,8 +817,10 @@ class Engine:
     def server(self, **kw) -> Server:
         return Server(self, **kw)
 
-    def negotiation(self, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1) -> Negotiation:
-        return Negotiation(self, req, present_weight, history_step)
+    def negotiation(self, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1,
+                    owned: Optional[Sequence[bool]] = None) -> Negotiation:
+        """An unsharded negotiation, or (with `owned`) this GPU's shard of one."""
+        return Negotiation(self, req, present_weight, history_step, owned)
 
 
 def net_windows(dims, nets: Sequence[NetEndpoints]) -> List[IsolatedRouteWindow]:

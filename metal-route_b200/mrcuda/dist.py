@@ -84,3 +84,28 @@ def init_from_env(backend: str, timeout_s: float = 120.0, device=None) -> Option
         kw["device_id"] = device
     dist.init_process_group(backend, **kw)
     return dist
+
+
+def sharded_negotiation_round(shard, all_reduce=None) -> dict:
+    """One negotiation round of this rank's shard (Engine.negotiation(...,
+    owned=...)): rip-up, exchange, route, exchange, settle.  The exchange sets the
+    global occupancy to the sum of every rank's local occupancy; `all_reduce`
+    (default: torch.distributed SUM over the process group, NCCL on GPUs) is
+    called on the global tensor after the local one is copied into it."""
+    import torch.distributed as dist
+
+    if all_reduce is None:
+        def all_reduce(t):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+
+    local, glob = shard.occupancy()
+
+    def exchange():
+        glob.copy_(local)
+        all_reduce(glob)
+
+    shard.ripup()
+    exchange()
+    shard.route()
+    exchange()
+    return shard.settle()

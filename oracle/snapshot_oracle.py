@@ -133,3 +133,67 @@ class SnapshotNegotiation:
                      next_dirty=len(nxt))
         self.round_no += 1
         return stats
+
+
+class SnapshotShard:
+    """One shard of the sharded round (the protocol of mrc_negotiation_create_shard):
+    it routes only the nets in `owned`, keeps the occupancy of its own paths in
+    `local`, and reads the `glob` occupancy that the caller sets to the sum of
+    every shard's local occupancy between the phases ripup / route / settle."""
+
+    def __init__(self, oracle, req: IsolatedRouteRequest, owned, present_weight: int = 16, history_step: int = 1):
+        self.o = oracle
+        self.req = req
+        self.dims = req.grid.dims
+        self.weight, self.step = int(present_weight), int(history_step)
+        n = len(self.dims)
+        self.base = base_prices(req)
+        self.local = np.zeros((n, 4), dtype=np.uint32)
+        self.glob = np.zeros((n, 4), dtype=np.uint32)
+        self.history = np.zeros((n, 4), dtype=np.uint32)
+        self.owned = [bool(x) for x in owned]
+        self.paths: List[Optional[List[int]]] = [None] * len(req.nets)
+        self.dirty = [i for i in range(len(req.nets)) if self.owned[i]]
+        self.round_no = 0
+
+    def _apply(self, path, delta: int):
+        c, s = edge_slots(path or [], self.dims.w, self.dims.plane)
+        if c.size:
+            (np.add if delta > 0 else np.subtract).at(self.local, (c, s), np.uint32(1))
+
+    def ripup(self):
+        for i in self.dirty:
+            self._apply(self.paths[i], -1)
+
+    def route(self):
+        pfac = 1 + self.round_no
+        price = (self.base.astype(np.uint64) + self.history.astype(np.uint64)
+                 + np.uint64(pfac * self.weight) * self.glob.astype(np.uint64))
+        snap = np.minimum(price, np.uint64(CAP)).astype(np.uint32)
+        snap[self.base == COST_MAX] = COST_MAX
+        r = self.req
+        if self.dirty:
+            sub = IsolatedRouteRequest(r.grid, [r.nets[i] for i in self.dirty], [r.windows[i] for i in self.dirty],
+                                       r.x_edge_costs, r.y_edge_costs, r.via_edge_costs, snap.reshape(-1))
+            new_paths, _ = self.o.isolated_batch(sub, retry_full=True, mode="astar")
+            for i, p in zip(self.dirty, new_paths):
+                self.paths[i] = p
+                self._apply(p, +1)
+
+    def settle(self):
+        over = self.glob >= 2
+        h = self.history.astype(np.uint64) + over.astype(np.uint64) * np.uint64(self.step)
+        self.history = np.minimum(h, np.uint64(COST_MAX)).astype(np.uint32)
+        nxt = []
+        for i, p in enumerate(self.paths):
+            if not self.owned[i]:
+                continue
+            if not p:
+                nxt.append(i)
+                continue
+            c, s = edge_slots(p, self.dims.w, self.dims.plane)
+            if c.size and bool((self.glob[c, s] >= 2).any()):
+                nxt.append(i)
+        self.dirty = nxt
+        self.round_no += 1
+        return int(over.sum()) // 2

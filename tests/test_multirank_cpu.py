@@ -8,6 +8,7 @@ import socket
 import sys
 import time
 
+import numpy as np
 import pytest
 
 from mrcuda.dist import Heartbeat, RankFailure, max_over_ranks, shard
@@ -109,3 +110,77 @@ def test_a_dead_rank_is_detected_within_the_timeout():
 
 def test_max_over_ranks_without_a_group():
     assert max_over_ranks(3.5) == 3.5
+
+
+def _shard_worker(rank, world, port, q):
+    try:
+        import torch
+        import torch.distributed as dist
+
+        root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        for p in (os.path.join(root, "metal-route_b200"), os.path.join(root, "oracle")):
+            sys.path.insert(0, p)
+        import oracle as orc
+        from mrcuda import workloads as W
+        from snapshot_oracle import SnapshotShard
+
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        wl = W.snapshot_board(w=96, h=80, layers=2, n_nets=40, median=30)
+        req = wl.request()
+        owned = [i % world == rank for i in range(len(req.nets))]
+        sh = SnapshotShard(orc.get(), req, owned)
+
+        def exchange():
+            t = torch.from_numpy(sh.local.astype(np.int64))
+            dist.all_reduce(t)
+            sh.glob = t.numpy().astype(np.uint32)
+
+        over = []
+        for _ in range(4):
+            sh.ripup()
+            exchange()
+            sh.route()
+            exchange()
+            over.append(sh.settle())
+        q.put((rank, [sh.paths[i] for i in range(len(req.nets)) if owned[i]], over, sh.history.sum().item()))
+        dist.destroy_process_group()
+    except Exception as err:
+        q.put((rank, "error", repr(err), None))
+
+
+
+def test_sharded_round_protocol_with_two_gloo_ranks(oracle):
+    """The sharded round run by two gloo ranks (the oracle as each rank's
+    router, occupancy all-reduced between the phases) equals one unsharded
+    snapshot negotiation over all nets."""
+    from mrcuda import workloads as W
+    from snapshot_oracle import SnapshotNegotiation
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_shard_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = {}
+    deadline = time.monotonic() + 120
+    while len(out) < 2 and time.monotonic() < deadline:
+        try:
+            r = q.get(timeout=1.0)
+            out[r[0]] = r
+        except Exception:
+            pass
+    for p in ps:
+        p.join(timeout=5)
+        if p.is_alive():
+            p.kill()
+    assert len(out) == 2 and all(v[1] != "error" for v in out.values()), out
+    wl = W.snapshot_board(w=96, h=80, layers=2, n_nets=40, median=30)
+    whole = SnapshotNegotiation(oracle, wl.request())
+    over = [whole.round().get("overused_edges", 0) for _ in range(4)]
+    assert out[0][2] == over and out[1][2] == over
+    assert out[0][3] == out[1][3] == int(whole.history.sum())
+    for rank in (0, 1):
+        mine = [whole.paths[i] for i in range(40) if i % 2 == rank]
+        assert out[rank][1] == mine
