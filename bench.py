@@ -46,17 +46,23 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _traffic_per_launch(kernel_profile: str):
-    """Bytes per relax launch from the committed ncu summary, when present."""
+def _profile_value(kernel_profile: str, key: str):
+    """A `key: value` figure from the committed ncu summary, when present."""
     path = os.path.join(ROOT, "profiles", kernel_profile)
     try:
         with open(path) as f:
             for line in f:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
-                    return int(float(line.split(":", 1)[1].strip().split()[0]))
+                if line.strip().startswith(key + ":"):
+                    return float(line.split(":", 1)[1].strip().split()[0])
     except OSError:
         pass
     return None
+
+
+def _traffic_per_launch(kernel_profile: str):
+    """DRAM bytes per relax launch from the committed ncu summary, when present."""
+    v = _profile_value(kernel_profile, "traffic_bytes_per_launch")
+    return None if v is None else int(v)
 
 
 def _workload(name: str, rank: int, nets: int = 0):
@@ -322,7 +328,9 @@ def run_engine(args):
     sched = batch.config()
     kname = "relax_async_kernel" if sched["schedule"] == 1 else "relax_rounds_kernel"
     # DRAM bytes per launch from the committed ncu summary of this kernel and workload
-    traffic = _traffic_per_launch(f"{kname.replace('_kernel', '')}_{args.workload}.md")
+    prof = f"{kname.replace('_kernel', '')}_{args.workload}.md"
+    traffic = _traffic_per_launch(prof)
+    ipc = _profile_value(prof, "ipc_per_sm")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -338,7 +346,10 @@ def run_engine(args):
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": f"{kname}<{sched['tile_h']},{sched['threads']}>",
                      "kernel_ms": relax_avg, "algorithmic_bytes_per_launch": int(alg_bytes),
                      "bytes_per_cell": round(wl.bytes_per_cell(), 3), "tile_activations": work["activations"],
-                     "in_tile_sweeps": work["sweeps"], "rounds": work["rounds"], "tiles": work["tiles"]},
+                     "in_tile_sweeps": work["sweeps"], "rounds": work["rounds"], "tiles": work["tiles"],
+                     # what does bind the kernel: instruction issue (ncu, small case of the same kernel)
+                     "issue": None if ipc is None else {"ipc_per_sm": ipc, "peak_ipc_per_sm": 4.0,
+                                                        "frac": ipc / 4.0, "source": f"profiles/{prof}"}},
         "clocks": clk,
     }
 
