@@ -179,22 +179,6 @@ __device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *
     return changed;
 }
 
-// Step price of the planar move p -> c read from HBM (staging and push checks).
-// out_bit / in_bit are the Grid::BOARD_EDGE_* bits of the move; dir is the
-// directed in-price slot of c (0 = from -y, 1 = -x, 2 = +x, 3 = +y).
-__device__ __forceinline__ uint32_t planar_step_g(const DevBoard &b, uint32_t ec, uint8_t fp, uint8_t fc,
-                                                  uint8_t out_bit, uint8_t in_bit, uint32_t gcell_c, uint32_t dir,
-                                                  uint32_t gap) {
-    if (ec == kMax) return kMax;
-    if ((fp & out_bit) | (fc & in_bit)) return kMax;
-    uint32_t base = gap;
-    if (b.directed) {
-        const uint4 d4 = __ldg(b.directed + gcell_c);
-        base = dir == 0 ? d4.x : dir == 1 ? d4.y : dir == 2 ? d4.z : d4.w;
-        if (base == kMax) return kMax;
-    }
-    return capmul(base, ec);
-}
 
 // Grid-wide barrier for a cooperative launch.  The wait is bounded: after
 // kBarrierSpinLimit polls it records kStatusBarrier and returns, and every CTA
@@ -690,19 +674,21 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
         const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
         const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
-        uint32_t en = kMax;  // cell_enter of the neighbour
-        if (!(fn & kTraceNode)) {
-            const uint32_t cn = __ldg(b.cost + gn);
-            en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
-        }
-        if (en == kMax) continue;
+        // the neighbour's enter cost and in-price, both loaded before either is used
         const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
-        uint32_t gap;
-        if (side == 0) gap = __ldg(b.x_edge + gx_n);
-        else if (side == 1) gap = __ldg(b.x_edge + gx_n - 1);
-        else if (side == 2) gap = __ldg(b.y_edge + gy_n);
-        else gap = __ldg(b.y_edge + gy_n - 1);
-        const u64 cand = ext2(lb, planar_step_g(b, en, fb, fn, out_bit, in_bit, gn, dir, gap), 1);
+        const uint32_t cn = __ldg(b.cost + gn);
+        uint32_t base;
+        if (b.directed) base = __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
+        else if (side == 0) base = __ldg(b.x_edge + gx_n);
+        else if (side == 1) base = __ldg(b.x_edge + gx_n - 1);
+        else if (side == 2) base = __ldg(b.y_edge + gy_n);
+        else base = __ldg(b.y_edge + gy_n - 1);
+        uint32_t en = kMax;  // cell_enter of the neighbour
+        if (!(fn & kTraceNode)) en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
+        if (en == kMax) continue;
+        uint32_t step = kMax;  // planar_step_g on the loaded values
+        if (!((fb & out_bit) | (fn & in_bit)) && !(b.directed && base == kMax)) step = capmul(base, en);
+        const u64 cand = ext2(lb, step, 1);
         if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
     }
     __syncthreads();
