@@ -108,7 +108,8 @@ struct Tile {
 // One directional pass over lines of K*S cells, S consecutive lanes per line
 // (K cells each), skipping lines whose dirty flag is clear.  Each lane runs its
 // segment's local chain, the S lanes combine their transfer functions
-// f(t) = min(A, t (+) (D, H)) with a Kogge-Stone scan, and every cell takes
+// f(t) = min(A, t (+) (D, H)) with a Kogge-Stone scan (H, the hop count, is the
+// group's cell count), and every cell takes
 // min(local, incoming (+) prefix).  `cell(line, pos, &lab, &step)` maps the
 // pos-th cell of a line in traversal order; `halo(line)` is the label index
 // before the first cell; `touch(line, pos)` marks the crossing lines of a cell
@@ -142,17 +143,18 @@ __device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *
             u[i] = umin64(v[i], ext2(u[i - 1], sp[i], 1));
             P[i] = dsum(P[i - 1], sp[i]);
         }
+        // The hop counts need no shuffles: before step o a participating lane's
+        // group spans o segments (K*o cells), and after the scan the group of
+        // lane seg-1 spans segments 0..seg-1 (K*seg cells).
         u64 A = u[K - 1];
-        uint32_t D = P[K - 1], H = K;
+        uint32_t D = P[K - 1];
 #pragma unroll
         for (int o = 1; o < S; o <<= 1) {
             const u64 Ap = __shfl_up_sync(mask, A, o, S);
             const uint32_t Dp = __shfl_up_sync(mask, D, o, S);
-            const uint32_t Hp = __shfl_up_sync(mask, H, o, S);
             if (seg >= (uint32_t)o) {
-                A = umin64(A, ext2(Ap, D, H));
+                A = umin64(A, ext2(Ap, D, (uint32_t)(K * o)));
                 D = dsum(Dp, D);
-                H = Hp + H;
             }
         }
         const u64 hl = lab[halo(line)];
@@ -160,8 +162,7 @@ __device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *
         if (S > 1) {
             const u64 Fa = __shfl_up_sync(mask, A, 1, S);
             const uint32_t Fd = __shfl_up_sync(mask, D, 1, S);
-            const uint32_t Fh = __shfl_up_sync(mask, H, 1, S);
-            if (seg > 0) C = umin64(Fa, ext2(hl, Fd, Fh));
+            if (seg > 0) C = umin64(Fa, ext2(hl, Fd, K * seg));
         }
         if (C != kInf) {
 #pragma unroll
