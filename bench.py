@@ -246,6 +246,7 @@ def run_engine(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     from mrcuda.dist import init_from_env, max_over_ranks
+    from mrcuda.workloads import pin_boards
 
     dist = init_from_env("nccl", timeout_s=120.0, device=torch.device("cuda", local))
 
@@ -306,16 +307,25 @@ def run_engine(args):
     ms_max = max_over_ranks(ms, device="cuda")
     value = len(wl.nets) * world / (ms_max / 1000.0)
 
-    # end to end through the public call with host buffers
+    # end to end through the public call with host buffers: first the caller's
+    # ordinary (pageable) arrays, then the same boards in page-locked memory
     e2e_steps = max(1, min(args.steps, 5))
-    wl.route(eng)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        out_paths = wl.route(eng)
-    torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
+
+    def e2e_time():
+        wl.route(eng)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            paths = wl.route(eng)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / e2e_steps, paths
+
+    e2e_pageable_s, out_pageable = e2e_time()
+    pin_boards(eng, wl.boards)
+    e2e_s, out_paths = e2e_time()
+    assert out_pageable == out_paths, "page-locked inputs changed the answer"
     e2e_value = len(wl.nets) * world / max_over_ranks(e2e_s, device="cuda")
+    e2e_pageable = len(wl.nets) * world / max_over_ranks(e2e_pageable_s, device="cuda")
     h2d = wl.h2d_bytes()
     d2h = 8 * (len(wl.nets) + 1) + 4 * len(wl.nets) + 4 * sum(len(p) for p in out_paths if p) + 4
     assert out_paths == first.paths, "end-to-end call disagrees with the resident batch"
@@ -340,7 +350,8 @@ def run_engine(args):
                    "routed": routed, "retried": first.retried, "l2": "flushed between steps (512 MiB write)",
                    "windows": wl.meta.get("windows"), "autotuned": tuned, "graph": not args.no_graph,
                    "instances": len(wl.boards)},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "inputs": "page-locked host arrays", "pageable_value": e2e_pageable},
         "gpu_launches": batch.kernel_launches * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": f"{kname}<{sched['tile_h']},{sched['threads']}>",

@@ -124,6 +124,17 @@ void mrc_context_destroy(mrc_context *ctx);
 const char *mrc_last_error(const mrc_context *ctx);
 uint32_t mrc_abi_version(void);
 
+/* Page-locked host memory, mapped into every device's address space.  Board
+ * arrays (cost, masks, directed prices) held here are read in place by one
+ * gather launch in mrc_route_instances instead of being staged, and reach HBM
+ * at full link rate in the single-board calls.  Ordinary (pageable) arrays
+ * stay accepted everywhere. */
+mrc_status mrc_host_alloc(mrc_context *ctx, size_t bytes, void **out);
+void mrc_host_free(void *p);
+/* Board bytes (cost, masks, directed prices) moved to HBM by this context so
+ * far: through a staging copy, and read in place from page-locked arrays. */
+mrc_status mrc_upload_stats(mrc_context *ctx, uint64_t *staged_bytes, uint64_t *in_place_bytes);
+
 /* ---- the provider seam ------------------------------------------------------ */
 
 /* Solve an isolated batch: per net, the canonical path inside its window and,

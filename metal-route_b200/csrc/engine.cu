@@ -13,6 +13,8 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -113,6 +115,45 @@ class Pool {
 
 namespace {
 
+// Phase trace: with MRC_TRACE set in the environment, the instance and batch
+// calls print the host time of each phase to stderr.  The stream is
+// synchronised at every mark so device work is charged to the phase that
+// queued it (tracing therefore removes the overlap it measures around).
+struct Trace {
+    const char *call;
+    cudaStream_t stream;
+    std::chrono::steady_clock::time_point t0, t;
+    static bool enabled() {
+        static const bool on = std::getenv("MRC_TRACE") != nullptr;
+        return on;
+    }
+    Trace(const char *c, cudaStream_t s) : call(c), stream(s), t0(std::chrono::steady_clock::now()), t(t0) {}
+    void mark(const char *phase) {
+        cudaStreamSynchronize(stream);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "mrc trace %s %-14s %8.3f ms (at %8.3f)\n", call, phase,
+                     std::chrono::duration<double, std::milli>(now - t).count(),
+                     std::chrono::duration<double, std::milli>(now - t0).count());
+        t = now;
+    }
+};
+thread_local Trace *g_trace = nullptr;
+void trace_mark(const char *phase) {
+    if (g_trace) g_trace->mark(phase);
+}
+struct TraceScope {
+    std::unique_ptr<Trace> tr;
+    TraceScope(const char *call, cudaStream_t s) {
+        if (Trace::enabled()) {
+            tr.reset(new Trace(call, s));
+            g_trace = tr.get();
+        }
+    }
+    ~TraceScope() {
+        if (tr) g_trace = nullptr;
+    }
+};
+
 // Pinned host staging reused across calls: host inputs are gathered here by
 // several threads and reach HBM with full-rate asynchronous copies.
 struct HostStage {
@@ -135,7 +176,7 @@ struct HostStage {
         p = nullptr;
         bytes = 0;
         const size_t want = std::max(n + n / 4, (size_t)64 << 20);
-        e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        e = cudaHostAlloc(&p, want, cudaHostAllocMapped);
         if (e != cudaSuccess) return e;
         bytes = want;
         return cudaSuccess;
@@ -155,6 +196,9 @@ struct mrc_context {
     // autotuned relax configuration per (layers, directed): tile height, CTA
     // width, schedule (0 = bulk-synchronous rounds, 1 = asynchronous queue)
     std::map<uint32_t, std::array<uint32_t, 3>> tuned;
+    // board bytes moved to HBM since creation: through the pinned stage or a
+    // pageable copy, and straight from the caller's page-locked arrays
+    uint64_t staged_bytes = 0, in_place_bytes = 0;
 };
 
 namespace {
@@ -310,6 +354,18 @@ struct mrc_board {
 
 namespace {
 
+// The device-readable address of page-locked, mapped host memory; null for
+// pageable memory.
+const void *mapped_host(const void *p) {
+    if (!p) return nullptr;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 mrc_status upload(mrc_context *ctx, DBuf &buf, const void *src, size_t bytes, const char *what) {
     MRC_TRY(buf.get(ctx, std::max<size_t>(bytes, 4), what));
     if (bytes) MRC_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream), what);
@@ -330,6 +386,9 @@ mrc_status board_build(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *
         return fail(MRC_ERR_INVALID_ARGUMENT, "edge price pointer is NULL");
     b->ctx = ctx;
     b->directed = edges->directed_in_costs != nullptr;
+    // uploads read the caller's arrays (page-locked ones at full link rate)
+    const uint32_t *src_cost = g.cost;
+    const uint8_t *src_board = g.board, *src_viaf = g.via_forbidden;
     if (keep_host) {
         b->cost.assign(g.cost, g.cost + g.n);
         if (g.board) b->board.assign(g.board, g.board + g.n);
@@ -339,18 +398,25 @@ mrc_status board_build(mrc_context *ctx, const mrc_grid *grid, const mrc_edges *
         g.via_forbidden = g.via_forbidden ? b->viaf.data() : nullptr;
     }
     const size_t n = (size_t)g.n;
-    MRC_TRY(upload(ctx, b->d_cost, g.cost, n * 4, "upload cost"));
+    {
+        const size_t big = n * 4 + ((g.board || g.via_forbidden) ? n : 0) + (b->directed ? n * 16 : 0);
+        const bool pinned = mapped_host(src_cost) && (!src_board || mapped_host(src_board)) &&
+                            (!src_viaf || mapped_host(src_viaf)) &&
+                            (!b->directed || mapped_host(edges->directed_in_costs));
+        (pinned ? ctx->in_place_bytes : ctx->staged_bytes) += big;
+    }
+    MRC_TRY(upload(ctx, b->d_cost, src_cost, n * 4, "upload cost"));
     const bool has_flags = g.board || g.via_forbidden;
     if (has_flags) {
         if (g.board) {
-            MRC_TRY(upload(ctx, b->d_flags, g.board, n, "upload board mask"));
+            MRC_TRY(upload(ctx, b->d_flags, src_board, n, "upload board mask"));
         } else {
             MRC_TRY(b->d_flags.get(ctx, std::max<size_t>(n, 4), "board flags"));
             MRC_CUDA(cudaMemsetAsync(b->d_flags.p, 0, n, ctx->stream), "clear flags");
         }
         if (g.via_forbidden) {
             DBuf tmp;
-            MRC_TRY(upload(ctx, tmp, g.via_forbidden, n, "upload via mask"));
+            MRC_TRY(upload(ctx, tmp, src_viaf, n, "upload via mask"));
             MRC_CUDA(combine_flags_launch(b->d_flags.as<uint8_t>(), tmp.as<uint8_t>(), n, ctx->stream), "combine masks");
             MRC_CUDA(cudaStreamSynchronize(ctx->stream), "combine masks");
         }
@@ -387,13 +453,106 @@ namespace {
 // their views point at the caller's arrays for the duration of the call.
 struct BoardPack {
     DBuf data;
+    DBuf spans;  // gather list of the page-locked upload
     std::vector<std::unique_ptr<mrc_board>> boards;
 };
 
-mrc_status board_pack_build(mrc_context *ctx, const mrc_isolated_request *inst, uint32_t n, BoardPack *pk) {
-    struct Off {
-        size_t cost, flags, x, y, via, dir;
+struct PackOff {
+    size_t cost, flags, x, y, via, dir;
+};
+
+void pack_views(BoardPack *pk, const std::vector<PackOff> &offs) {
+    unsigned char *base = pk->data.as<unsigned char>();
+    for (size_t k = 0; k < offs.size(); ++k) {
+        mrc_board &b = *pk->boards[k];
+        const PackOff &o = offs[k];
+        b.dev.w = b.view.w;
+        b.dev.h = b.view.h;
+        b.dev.layers = b.view.layers;
+        b.dev.cost = reinterpret_cast<const uint32_t *>(base + o.cost);
+        b.dev.flags = o.flags != SIZE_MAX ? base + o.flags : nullptr;
+        b.dev.x_edge = reinterpret_cast<const uint32_t *>(base + o.x);
+        b.dev.y_edge = reinterpret_cast<const uint32_t *>(base + o.y);
+        b.dev.via_edge = reinterpret_cast<const uint32_t *>(base + o.via);
+        b.dev.directed = o.dir != SIZE_MAX ? reinterpret_cast<const uint4 *>(base + o.dir) : nullptr;
+    }
+}
+
+// Page-locked instances: the cost, mask and directed arrays are read in place by
+// one gather launch; only the small edge vectors and the gather list pass
+// through the stage.  `src[k]` holds the mapped addresses of instance k's cost,
+// board mask, via mask and directed prices.
+mrc_status board_pack_direct(mrc_context *ctx, const mrc_isolated_request *inst, uint32_t n, BoardPack *pk,
+                             const std::vector<PackOff> &offs, size_t total,
+                             const std::vector<std::array<const void *, 4>> &src) {
+    MRC_TRY(pk->data.get(ctx, std::max<size_t>(total, 256), "instance boards"));
+    auto up16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    // stage layout: per instance the device bytes from o.x to the end of the via
+    // prices (same padding as on the device), then the spans, then chunk starts
+    std::vector<size_t> small(n);
+    size_t sb = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        small[k] = sb;
+        sb += up16(offs[k].via + (size_t)std::max(inst[k].edges.n_via_edge_costs, 1u) * 4 - offs[k].x);
+    }
+    const size_t max_spans = (size_t)4 * n;
+    const size_t o_spans = sb, o_chunks = up16(o_spans + max_spans * sizeof(HostSpan));
+    const size_t stage_bytes = o_chunks + max_spans * 8;
+    MRC_CUDA(ctx->stage.reserve(stage_bytes), "pinned staging buffer");
+    unsigned char *host = static_cast<unsigned char *>(ctx->stage.p);
+    const unsigned char *host_dev = static_cast<const unsigned char *>(mapped_host(host));
+    if (!host_dev) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "pinned staging buffer is not mapped into the device");
+    HostSpan *spans = reinterpret_cast<HostSpan *>(host + o_spans);
+    uint64_t *chunk = reinterpret_cast<uint64_t *>(host + o_chunks);
+    unsigned char *base = pk->data.as<unsigned char>();
+    uint32_t ns = 0;
+    uint64_t nc = 0;
+    auto add = [&](const void *a, const void *b, size_t off, size_t bytes, uint32_t kind) {
+        if (!bytes) return;
+        spans[ns] = HostSpan{a, b, base + off, bytes, kind};
+        chunk[ns++] = nc;
+        nc += host_gather_chunks(bytes);
     };
+    for (uint32_t k = 0; k < n; ++k) {
+        const GridView &g = pk->boards[k]->view;
+        const mrc_edges &e = inst[k].edges;
+        const PackOff &o = offs[k];
+        unsigned char *sm = host + small[k];
+        if (e.n_x_edge_costs) std::memcpy(sm, e.x_edge_costs, (size_t)e.n_x_edge_costs * 4);
+        if (e.n_y_edge_costs) std::memcpy(sm + (o.y - o.x), e.y_edge_costs, (size_t)e.n_y_edge_costs * 4);
+        uint32_t *via = reinterpret_cast<uint32_t *>(sm + (o.via - o.x));
+        uint32_t mask = 0;
+        via[0] = 0;
+        for (uint32_t i = 0; i < e.n_via_edge_costs; ++i) {
+            via[i] = e.via_edge_costs[i];
+            if (e.via_allowed[i]) mask |= 1u << i;
+        }
+        pk->boards[k]->dev.via_mask = mask;
+        ctx->in_place_bytes += (size_t)g.n * 4 + (o.flags != SIZE_MAX ? g.n : 0) + (o.dir != SIZE_MAX ? (size_t)g.n * 16 : 0);
+        add(src[k][0], nullptr, o.cost, (size_t)g.n * 4, 0);
+        if (o.flags != SIZE_MAX) add(src[k][1], src[k][2], o.flags, g.n, g.via_forbidden ? 1 : 0);
+        if (o.dir != SIZE_MAX) add(src[k][3], nullptr, o.dir, (size_t)g.n * 16, 0);
+        add(host_dev + small[k], nullptr, o.x, o.via + (size_t)std::max(e.n_via_edge_costs, 1u) * 4 - o.x, 0);
+    }
+    // the gather list itself goes over in one copy (the kernel searches it per chunk)
+    const size_t list_bytes = up16((size_t)ns * sizeof(HostSpan)) + (size_t)ns * 8;
+    MRC_TRY(pk->spans.get(ctx, std::max<size_t>(list_bytes, 256), "gather list"));
+    unsigned char *dl = pk->spans.as<unsigned char>();
+    MRC_CUDA(cudaMemcpyAsync(dl, spans, (size_t)ns * sizeof(HostSpan), cudaMemcpyHostToDevice, ctx->stream),
+             "upload gather list");
+    const size_t dchunk = up16((size_t)ns * sizeof(HostSpan));
+    MRC_CUDA(cudaMemcpyAsync(dl + dchunk, chunk, (size_t)ns * 8, cudaMemcpyHostToDevice, ctx->stream),
+             "upload gather list");
+    MRC_CUDA(host_gather_launch(reinterpret_cast<const HostSpan *>(dl), reinterpret_cast<const uint64_t *>(dl + dchunk),
+                                ns, nc, (uint32_t)ctx->sms, ctx->stream),
+             "gather instance boards");
+    MRC_CUDA(cudaEventRecord(ctx->stage.done, ctx->stream), "stage event");
+    pack_views(pk, offs);
+    return MRC_OK;
+}
+
+mrc_status board_pack_build(mrc_context *ctx, const mrc_isolated_request *inst, uint32_t n, BoardPack *pk) {
+    using Off = PackOff;
     std::vector<Off> offs(n);
     size_t total = 0;
     auto take = [&](size_t bytes) {
@@ -423,8 +582,21 @@ mrc_status board_pack_build(mrc_context *ctx, const mrc_isolated_request *inst, 
         o.dir = b->directed ? take(g.n * 16) : SIZE_MAX;
         pk->boards.push_back(std::move(b));
     }
+    // page-locked inputs (every large array of every instance mapped) are read in place
+    if (n && mapped_host(pk->boards[0]->view.cost)) {
+        std::vector<std::array<const void *, 4>> src(n);
+        bool all = true;
+        for (uint32_t k = 0; k < n && all; ++k) {
+            const GridView &g = pk->boards[k]->view;
+            const void *dir = inst[k].edges.directed_in_costs;
+            src[k] = {mapped_host(g.cost), mapped_host(g.board), mapped_host(g.via_forbidden), mapped_host(dir)};
+            all = src[k][0] && (!g.board || src[k][1]) && (!g.via_forbidden || src[k][2]) && (!dir || src[k][3]);
+        }
+        if (all) return board_pack_direct(ctx, inst, n, pk, offs, total, src);
+    }
     MRC_TRY(pk->data.get(ctx, std::max<size_t>(total, 256), "instance boards"));
     MRC_CUDA(ctx->stage.reserve(total), "pinned staging buffer");
+    ctx->staged_bytes += total;
     unsigned char *host = static_cast<unsigned char *>(ctx->stage.p);
     auto fill = [&](uint32_t k) {
         const GridView &g = pk->boards[k]->view;
@@ -484,20 +656,7 @@ mrc_status board_pack_build(mrc_context *ctx, const mrc_isolated_request *inst, 
     for (auto &t : workers) t.join();
     MRC_CUDA(ce, "upload instance boards");
     MRC_CUDA(cudaEventRecord(ctx->stage.done, ctx->stream), "stage event");
-    unsigned char *base = pk->data.as<unsigned char>();
-    for (uint32_t k = 0; k < n; ++k) {
-        mrc_board &b = *pk->boards[k];
-        const Off &o = offs[k];
-        b.dev.w = b.view.w;
-        b.dev.h = b.view.h;
-        b.dev.layers = b.view.layers;
-        b.dev.cost = reinterpret_cast<const uint32_t *>(base + o.cost);
-        b.dev.flags = o.flags != SIZE_MAX ? base + o.flags : nullptr;
-        b.dev.x_edge = reinterpret_cast<const uint32_t *>(base + o.x);
-        b.dev.y_edge = reinterpret_cast<const uint32_t *>(base + o.y);
-        b.dev.via_edge = reinterpret_cast<const uint32_t *>(base + o.via);
-        b.dev.directed = o.dir != SIZE_MAX ? reinterpret_cast<const uint4 *>(base + o.dir) : nullptr;
-    }
+    pack_views(pk, offs);
     return MRC_OK;
 }
 
@@ -819,9 +978,13 @@ mrc_status solve(mrc_context *ctx, std::vector<const mrc_board *> boards, std::v
         own.reset(new mrc_batch());
         bt = own.get();
         MRC_TRY(batch_build(ctx, std::move(boards), std::move(nets), std::move(wins), flags, bt));
+        trace_mark("batch build");
         MRC_TRY(batch_launch(bt, ctx->stream));
+        trace_mark("kernels");
     }
-    return finish_batch(ctx, bt, flags, out);
+    MRC_TRY(finish_batch(ctx, bt, flags, out));
+    trace_mark("results");
+    return MRC_OK;
 }
 
 // Results of a launched batch (waits for it), with the full-board retry.
@@ -966,6 +1129,31 @@ void mrc_context_destroy(mrc_context *ctx) {
     delete ctx;
 }
 
+mrc_status mrc_host_alloc(mrc_context *ctx, size_t bytes, void **out) {
+    if (!ctx || !out) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    MRC_TRY(set_device(ctx));
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, std::max<size_t>(bytes, 16), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(MRC_ERR_OUT_OF_MEMORY, "page-locked host allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    *out = p;
+    return MRC_OK;
+}
+
+void mrc_host_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
+mrc_status mrc_upload_stats(mrc_context *ctx, uint64_t *staged_bytes, uint64_t *in_place_bytes) {
+    if (!ctx || !staged_bytes || !in_place_bytes) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    Lock lock(ctx, 0);
+    *staged_bytes = ctx->staged_bytes;
+    *in_place_bytes = ctx->in_place_bytes;
+    return MRC_OK;
+}
+
 mrc_status mrc_net_windows(uint32_t w, uint32_t h, uint32_t layers, const mrc_net *nets, uint32_t n_nets,
                            mrc_window *out) {
     if ((n_nets && (!nets || !out))) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -989,6 +1177,7 @@ mrc_status mrc_route_isolated_batch(mrc_context *ctx, const mrc_isolated_request
     Lock lock(ctx, flags);
     if (lock.st != MRC_OK) return lock.st;
     MRC_TRY(set_device(ctx));
+    TraceScope trace("route_isolated_batch", ctx->stream);
     GridView g;
     MRC_TRY(view_grid(req->grid, &g));
     if (req->n_nets && !req->windows) return fail(MRC_ERR_INVALID_ARGUMENT, "windows is NULL");
@@ -996,8 +1185,10 @@ mrc_status mrc_route_isolated_batch(mrc_context *ctx, const mrc_isolated_request
     MRC_TRY(validate_nets(g, req->nets, req->n_nets, &nets));
     std::vector<mrc_window> wins;
     MRC_TRY(collect_windows(g, nets, req->windows, &wins));
+    trace_mark("validate");
     mrc_board board;
     MRC_TRY(board_build(ctx, req->grid, &req->edges, false, &board));
+    trace_mark("board upload");
     if (nets.empty()) {
         *out = new mrc_result();
         (*out)->offsets.assign(1, 0);
@@ -1079,6 +1270,7 @@ mrc_status mrc_route_instances(mrc_context *ctx, const mrc_isolated_request *ins
     Lock lock(ctx, flags);
     if (lock.st != MRC_OK) return lock.st;
     MRC_TRY(set_device(ctx));
+    TraceScope trace("route_instances", ctx->stream);
     std::vector<NetCopy> nets;
     std::vector<mrc_window> wins;
     for (uint32_t k = 0; k < n_instances; ++k) {
@@ -1101,8 +1293,10 @@ mrc_status mrc_route_instances(mrc_context *ctx, const mrc_isolated_request *ins
         (*out)->field_offsets.assign(1, 0);
         return MRC_OK;
     }
+    trace_mark("validate");
     BoardPack pk;
     MRC_TRY(board_pack_build(ctx, instances, n_instances, &pk));
+    trace_mark("board upload");
     std::vector<const mrc_board *> boards;
     for (auto &b : pk.boards) boards.push_back(b.get());
     return solve(ctx, std::move(boards), std::move(nets), std::move(wins), flags, out, nullptr);

@@ -118,4 +118,19 @@ cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t
 cudaError_t wait_selftest_launch(Ctl *c, uint32_t spins, cudaStream_t st);
 cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, uint64_t n, cudaStream_t st);
 
+// A span of page-locked host memory (device-mapped address) copied into HBM.
+// kind 0: dst = src (src may be null: zeros); kind 1: flag bytes, dst[i] =
+// src[i] | (src2[i] ? kStaticVia : 0), either source may be null.
+struct HostSpan {
+    const void *src;
+    const void *src2;
+    void *dst;
+    uint64_t bytes;
+    uint32_t kind;
+};
+// chunk_start[s] = the first chunk of span s (prefix sum of host_gather_chunks)
+cudaError_t host_gather_launch(const HostSpan *spans, const uint64_t *chunk_start, uint32_t n_spans, uint64_t n_chunks,
+                               uint32_t sms, cudaStream_t st);
+uint64_t host_gather_chunks(uint64_t bytes);
+
 }  // namespace mrc

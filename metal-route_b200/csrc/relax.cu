@@ -1100,7 +1100,104 @@ __global__ void combine_flags_kernel(uint8_t *flags, const uint8_t *via_forbidde
         if (via_forbidden[i]) flags[i] |= kStaticVia;
 }
 
+// ---- gather of page-locked host buffers into HBM ---------------------------
+// One launch moves many host spans of one instance set to their places in a
+// device block: the SMs read the host memory through its device mapping (PCIe
+// reads, 16 bytes a thread, several in flight), so thousands of small and large
+// spans cost one launch instead of one copy call each.  The spans are cut into
+// 64 KiB chunks and the blocks stride over the chunks.
+
+constexpr uint64_t kGatherChunk = 64u << 10;
+
+// 0x80 in each nonzero byte of w, 0 elsewhere
+__device__ __forceinline__ uint32_t nonzero_bytes(uint32_t w) {
+    return (((w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | w) & 0x80808080u;
+}
+static_assert(kStaticVia == 0x40, "the via-mask bit is the nonzero mark shifted by one");
+
+__device__ __forceinline__ uint32_t flag_word(uint32_t board, uint32_t via) { return board | (nonzero_bytes(via) >> 1); }
+
+__global__ void __launch_bounds__(256) host_gather_kernel(const HostSpan *spans, const uint64_t *chunk_start,
+                                                          uint32_t n_spans, uint64_t n_chunks) {
+    for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+        // the span holding chunk c: the last s with chunk_start[s] <= c
+        uint32_t lo = 0, hi = n_spans - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (chunk_start[mid] <= c) lo = mid; else hi = mid - 1;
+        }
+        const HostSpan sp = spans[lo];
+        const uint64_t off = (c - chunk_start[lo]) * kGatherChunk;
+        const uint64_t len = min(kGatherChunk, sp.bytes - off);
+        const unsigned char *src = static_cast<const unsigned char *>(sp.src) + off;
+        const unsigned char *src2 = static_cast<const unsigned char *>(sp.src2) + off;
+        unsigned char *dst = static_cast<unsigned char *>(sp.dst) + off;
+        const bool have_src = sp.src != nullptr, have_src2 = sp.src2 != nullptr;
+        const uintptr_t align = (uintptr_t)dst | (have_src ? (uintptr_t)src : 0) | (have_src2 ? (uintptr_t)src2 : 0);
+        uint64_t done = 0;
+        if ((align & 15) == 0) {
+            const uint64_t n16 = len / 16;
+            constexpr int U = 4;
+            for (uint64_t i0 = 0; i0 < n16; i0 += (uint64_t)U * blockDim.x) {
+                uint4 a[U], b[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t i = i0 + (uint64_t)u * blockDim.x + threadIdx.x;
+                    a[u] = make_uint4(0, 0, 0, 0);
+                    b[u] = make_uint4(0, 0, 0, 0);
+                    if (i < n16) {
+                        if (have_src) a[u] = reinterpret_cast<const uint4 *>(src)[i];
+                        if (sp.kind == 1 && have_src2) b[u] = reinterpret_cast<const uint4 *>(src2)[i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t i = i0 + (uint64_t)u * blockDim.x + threadIdx.x;
+                    if (i >= n16) continue;
+                    if (sp.kind == 1)
+                        a[u] = make_uint4(flag_word(a[u].x, b[u].x), flag_word(a[u].y, b[u].y), flag_word(a[u].z, b[u].z),
+                                          flag_word(a[u].w, b[u].w));
+                    reinterpret_cast<uint4 *>(dst)[i] = a[u];
+                }
+            }
+            done = n16 * 16;
+        } else if ((align & 3) == 0 && sp.kind == 0) {
+            const uint64_t n4 = len / 4;
+            constexpr int U = 8;
+            for (uint64_t i0 = 0; i0 < n4; i0 += (uint64_t)U * blockDim.x) {
+                uint32_t a[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t i = i0 + (uint64_t)u * blockDim.x + threadIdx.x;
+                    a[u] = (i < n4 && have_src) ? reinterpret_cast<const uint32_t *>(src)[i] : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t i = i0 + (uint64_t)u * blockDim.x + threadIdx.x;
+                    if (i < n4) reinterpret_cast<uint32_t *>(dst)[i] = a[u];
+                }
+            }
+            done = n4 * 4;
+        }
+        for (uint64_t i = done + threadIdx.x; i < len; i += blockDim.x) {
+            uint8_t v = have_src ? src[i] : 0;
+            if (sp.kind == 1 && have_src2 && src2[i]) v |= kStaticVia;
+            dst[i] = v;
+        }
+    }
+}
+
 // ---- host-side launch helpers ---------------------------------------------
+
+cudaError_t host_gather_launch(const HostSpan *spans, const uint64_t *chunk_start, uint32_t n_spans, uint64_t n_chunks,
+                               uint32_t sms, cudaStream_t st) {
+    if (!n_spans || !n_chunks) return cudaSuccess;
+    const uint64_t blocks = std::min<uint64_t>(n_chunks, (uint64_t)sms * 8);
+    host_gather_kernel<<<(uint32_t)blocks, 256, 0, st>>>(spans, chunk_start, n_spans, n_chunks);
+    return cudaGetLastError();
+}
+
+uint64_t host_gather_chunks(uint64_t bytes) { return (bytes + kGatherChunk - 1) / kGatherChunk; }
 
 cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, uint64_t n, cudaStream_t st) {
     if (n == 0) return cudaSuccess;

@@ -17,6 +17,7 @@ unavailable every call raises ``BackendUnavailable`` and the caller decides.
 """
 from __future__ import annotations
 
+import array
 import ctypes as C
 import os
 import threading
@@ -150,6 +151,9 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_last_error": (C.c_char_p, [vp]),
             "mrc_context_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
             "mrc_context_destroy": (None, [vp]),
+            "mrc_host_alloc": (C.c_int, [vp, C.c_size_t, C.POINTER(vp)]),
+            "mrc_host_free": (None, [vp]),
+            "mrc_upload_stats": (C.c_int, [vp, u64p, u64p]),
             "mrc_route_isolated_batch": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(vp)]),
             "mrc_route_isolated_plain": (C.c_int, [vp, C.POINTER(_Request), u32, C.POINTER(vp)]),
             "mrc_route_lee": (C.c_int, [vp, C.POINTER(_Grid), vp, u32, C.POINTER(vp)]),
@@ -298,6 +302,14 @@ def _addr(a: Optional[np.ndarray]) -> int:
         return a.__array_interface__["data"][0]
 
 
+def _flat_u32(lists) -> np.ndarray:
+    """Concatenation of many short integer sequences as one u32 array."""
+    a = array.array("I")
+    for p in lists:
+        a.extend(p)
+    return np.frombuffer(a, dtype=np.uint32) if len(a) else np.zeros(0, np.uint32)
+
+
 def _marshal_requests(m: _Marshal, requests: Sequence[IsolatedRouteRequest]):
     """An array of C requests for many instances at once.  The structs are
     written as 64-bit words from numpy columns (the layouts of _Grid, _Net,
@@ -312,11 +324,12 @@ def _marshal_requests(m: _Marshal, requests: Sequence[IsolatedRouteRequest]):
     wins = np.zeros((max(nn, 1), 4), dtype=np.uint32)
     # pads of every net in one array
     pad_lists = [nt.passable_pads for nt in nets_all] + [nt.via_passable_pads for nt in nets_all]
-    lens = np.fromiter((len(p) for p in pad_lists), dtype=np.int64, count=len(pad_lists))
-    pads = np.fromiter((c for p in pad_lists for c in p), dtype=np.uint32, count=int(lens.sum()))
-    starts = np.concatenate([[0], np.cumsum(lens)[:-1]]) if len(lens) else np.zeros(0, np.int64)
-    m.keep += [reqs, grids, nets, wins, pads]
-    pbase = _addr(pads) if pads.size else 0
+    lens = np.fromiter(map(len, pad_lists), dtype=np.int64, count=len(pad_lists))
+    pads = _flat_u32(pad_lists)
+    starts = np.cumsum(lens) - lens
+    # the caller's arrays stay referenced by the requests themselves
+    m.keep += [requests, reqs, grids, nets, wins, pads]
+    pbase = _addr(pads)
     if nn:
         nets[:, 0] = (np.fromiter((nt.src for nt in nets_all), np.uint64, nn)
                       | (np.fromiter((nt.dst for nt in nets_all), np.uint64, nn) << np.uint64(32)))
@@ -325,48 +338,46 @@ def _marshal_requests(m: _Marshal, requests: Sequence[IsolatedRouteRequest]):
         nets[:, 2] = lp.astype(np.uint64)
         nets[:, 3] = np.where(lv > 0, pbase + 4 * starts[nn:], 0).astype(np.uint64)
         nets[:, 4] = lv.astype(np.uint64)
-        wins[:] = np.array([(w.x0, w.y0, w.x1, w.y1) for rq in requests for w in rq.windows],
-                           dtype=np.uint32).reshape(-1, 4)
-    rw = np.frombuffer(reqs, dtype=np.uint64).reshape(max(n, 1), C.sizeof(_Request) // 8)
+        wins.reshape(-1)[:] = np.fromiter((c for rq in requests for w in rq.windows for c in (w.x0, w.y0, w.x1, w.y1)),
+                                          np.uint32, 4 * nn)
+    if not n:
+        return reqs
+    if any(len(rq.windows) != len(rq.nets) for rq in requests):
+        raise BackendUnavailable("isolated request windows are not net-aligned")
+    rw = np.frombuffer(reqs, dtype=np.uint64).reshape(n, C.sizeof(_Request) // 8)
     gbase, nbase, wbase = _addr(grids), _addr(nets), _addr(wins)
     # the small edge vectors of every request in one array each
     xs = [_u32(rq.x_edge_costs) for rq in requests]
     ys = [_u32(rq.y_edge_costs) for rq in requests]
     vv = [_via_arrays(rq.via_edge_costs) for rq in requests]
-    xa = np.concatenate(xs) if n else np.zeros(0, np.uint32)
-    ya = np.concatenate(ys) if n else np.zeros(0, np.uint32)
-    vea = np.concatenate([v[0] for v in vv]) if n else np.zeros(0, np.uint32)
-    vaa = np.concatenate([v[1] for v in vv]) if n else np.zeros(0, np.uint8)
-    m.keep += [xa, ya, vea, vaa]
-    xb, yb, veb, vab = _addr(xa), _addr(ya), _addr(vea), _addr(vaa)
-    first = xo = yo = vo = 0
-    cols = [[] for _ in range(12)]
-    gcols = [[] for _ in range(5)]
-    for k, rq in enumerate(requests):
-        if len(rq.windows) != len(rq.nets):
-            raise BackendUnavailable("isolated request windows are not net-aligned")
-        g = rq.grid
-        nx, ny, nv = xs[k].size, ys[k].size, vv[k][0].size
-        d = None if rq.directed_in_costs is None else _u32(rq.directed_in_costs)
-        m.keep += [g.cost, g.board_constraint, g.via_forbidden, d]
-        gcols[0].append(g.dims.w | (g.dims.h << 32))
-        gcols[1].append(g.dims.layers)
-        gcols[2].append(_addr(g.cost))
-        gcols[3].append(_addr(g.board_constraint))
-        gcols[4].append(_addr(g.via_forbidden))
-        k_n = len(rq.nets)
-        for i, v in enumerate((gbase + k * C.sizeof(_Grid), nbase + first * C.sizeof(_Net) if k_n else 0, k_n,
-                               wbase + first * 16 if k_n else 0, xb + 4 * xo if nx else 0, nx,
-                               yb + 4 * yo if ny else 0, ny, veb + 4 * vo if nv else 0, vab + vo if nv else 0,
-                               nv, _addr(d))):
-            cols[i].append(v)
-        first += k_n
-        xo, yo, vo = xo + nx, yo + ny, vo + nv
-    if n:
-        for i in range(5):
-            grids[:n, i] = np.array(gcols[i], dtype=np.uint64)
-        for i in range(12):
-            rw[:n, i] = np.array(cols[i], dtype=np.uint64)
+    ds = [None if rq.directed_in_costs is None else _u32(rq.directed_in_costs) for rq in requests]
+    xa, ya = np.concatenate(xs), np.concatenate(ys)
+    vea, vaa = np.concatenate([v[0] for v in vv]), np.concatenate([v[1] for v in vv])
+    m.keep += [xa, ya, vea, vaa, ds]
+    kn = np.fromiter((len(rq.nets) for rq in requests), np.int64, n)
+    nx = np.fromiter((a.size for a in xs), np.int64, n)
+    ny = np.fromiter((a.size for a in ys), np.int64, n)
+    nv = np.fromiter((v[0].size for v in vv), np.int64, n)
+    first, xo, yo, vo = (np.cumsum(c) - c for c in (kn, nx, ny, nv))
+    gl = [rq.grid for rq in requests]
+    grids[:n, 0] = np.fromiter((g.dims.w | (g.dims.h << 32) for g in gl), np.uint64, n)
+    grids[:n, 1] = np.fromiter((g.dims.layers for g in gl), np.uint64, n)
+    grids[:n, 2] = np.fromiter((_addr(g.cost) for g in gl), np.uint64, n)
+    grids[:n, 3] = np.fromiter((_addr(g.board_constraint) for g in gl), np.uint64, n)
+    grids[:n, 4] = np.fromiter((_addr(g.via_forbidden) for g in gl), np.uint64, n)
+    at = lambda cnt, base, off, size: np.where(cnt > 0, base + size * off, 0).astype(np.uint64)
+    rw[:, 0] = gbase + C.sizeof(_Grid) * np.arange(n, dtype=np.uint64)
+    rw[:, 1] = at(kn, nbase, first, C.sizeof(_Net))
+    rw[:, 2] = kn
+    rw[:, 3] = at(kn, wbase, first, 16)
+    rw[:, 4] = at(nx, _addr(xa), xo, 4)
+    rw[:, 5] = nx
+    rw[:, 6] = at(ny, _addr(ya), yo, 4)
+    rw[:, 7] = ny
+    rw[:, 8] = at(nv, _addr(vea), vo, 4)
+    rw[:, 9] = at(nv, _addr(vaa), vo, 1)
+    rw[:, 10] = nv
+    rw[:, 11] = np.fromiter((_addr(d) for d in ds), np.uint64, n)
     return reqs
 
 
@@ -394,7 +405,7 @@ def _take_result(L, res, n: int, fields: bool, layers: int = 1) -> IsolatedBatch
         cl, ol = cells.tolist(), off.tolist()
         paths = [cl[ol[i]:ol[i + 1]] if ol[i + 1] > ol[i] else None for i in range(n)]
         out = IsolatedBatchResult(paths, costs.tolist(), retried=int(L.mrc_result_retried(res)))
-        wp = L.mrc_result_field_windows(res)
+        wp = L.mrc_result_field_windows(res) if fields else None
         if n and wp:
             wa = np.ctypeslib.as_array(C.cast(wp, C.POINTER(C.c_uint32)), shape=(n * 4,)).tolist()
             out.field_windows = [IsolatedRouteWindow(*wa[4 * i:4 * i + 4]) for i in range(n)]
@@ -709,6 +720,18 @@ class Server:
             pass
 
 
+class _HostBlock:
+    """Frees one mrc_host_alloc block when the buffer that owns it goes away."""
+
+    def __init__(self, lib, ptr: int):
+        self.lib, self.ptr = lib, ptr
+
+    def __del__(self):
+        if self.ptr:
+            self.lib.mrc_host_free(C.c_void_p(self.ptr))
+            self.ptr = 0
+
+
 class Engine:
     """One CUDA context of the engine (one per process per device)."""
 
@@ -735,6 +758,36 @@ class Engine:
             msg = self.lib.mrc_last_error(self.ctx)
             msg = msg.decode() if msg else ""
             raise _ERRORS.get(status, RouterError)(msg)
+
+    # -- page-locked host arrays --------------------------------------------
+    def pinned_empty(self, shape, dtype) -> np.ndarray:
+        """An uninitialised numpy array in page-locked, device-mapped host
+        memory (freed when the last view of it goes away).  Board arrays held
+        here are read in place by route_instances and reach HBM at full link
+        rate in the single-board calls."""
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+        p = C.c_void_p()
+        self._check(self.lib.mrc_host_alloc(self.ctx, max(nbytes, 1), C.byref(p)))
+        buf = (C.c_char * max(nbytes, 1)).from_address(p.value)
+        buf._block = _HostBlock(self.lib, p.value)
+        return np.frombuffer(buf, dtype=dtype, count=nbytes // dtype.itemsize).reshape(shape)
+
+    def upload_stats(self) -> dict:
+        """Board bytes moved to HBM so far: staged, and read in place from
+        page-locked arrays."""
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.mrc_upload_stats(self.ctx, C.byref(a), C.byref(b)))
+        return {"staged_bytes": a.value, "in_place_bytes": b.value}
+
+    def pin(self, a):
+        """A page-locked copy of `a` (None stays None)."""
+        if a is None:
+            return None
+        a = np.asarray(a)
+        out = self.pinned_empty(a.shape, a.dtype)
+        out[...] = a
+        return out
 
     # -- the provider seam ---------------------------------------------------
     def _request(self, m: _Marshal, req: IsolatedRouteRequest) -> _Request:

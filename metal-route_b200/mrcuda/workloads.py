@@ -20,7 +20,7 @@ fixed seed and every distribution choice is recorded in ``Workload.meta``.
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -64,6 +64,32 @@ class Workload:
         if self.grid.board_constraint is not None or self.grid.via_forbidden is not None:
             b_in += 1
         return b_in + 4
+
+
+def pin_boards(engine, boards: Sequence["Workload"]) -> None:
+    """Moves every workload's board arrays (cost, masks, directed prices) into
+    one page-locked block of `engine` (64-byte aligned views), in place."""
+    arrays = []
+    for wl in boards:
+        g = wl.grid
+        arrays += [g.cost, g.board_constraint, g.via_forbidden, wl.directed]
+    offs, tot = [], 0
+    for a in arrays:
+        offs.append(tot)
+        tot += 0 if a is None else (a.nbytes + 63) & ~63
+    blk = engine.pinned_empty(max(tot, 1), np.uint8)
+
+    def view(a, o):
+        if a is None:
+            return None
+        v = blk[o:o + a.nbytes].view(a.dtype).reshape(a.shape)
+        v[...] = a
+        return v
+
+    for k, wl in enumerate(boards):
+        c, b, vf, d = (view(arrays[4 * k + i], offs[4 * k + i]) for i in range(4))
+        wl.grid = Grid(wl.grid.dims, c, b, vf)
+        wl.directed = d
 
 
 _FREE_CACHE: Dict[int, tuple] = {}

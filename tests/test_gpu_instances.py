@@ -143,3 +143,90 @@ def test_graph_replay_matches_stream_launch(engine, oracle):
     batch.capture_graph()
     batch.launch()
     assert batch.finish().paths == ref.paths
+
+
+def _pinned_request(engine, r, shifts=(0, 0, 0)):
+    """`r` with its cost, masks and directed prices copied into page-locked
+    memory, each array starting `shifts` bytes past a 16-byte boundary (cost,
+    masks, directed)."""
+    def pin(a, dtype, shift):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+        blk = engine.pinned_empty(a.nbytes + 32, np.uint8)
+        v = blk[shift:shift + a.nbytes].view(dtype)
+        v[:] = a
+        return v
+    g = r.grid
+    grid = Grid(g.dims, pin(g.cost, np.uint32, shifts[0]), pin(g.board_constraint, np.uint8, shifts[1]),
+                pin(g.via_forbidden, np.uint8, shifts[1]))
+    assert grid.cost.ctypes.data % 16 == shifts[0]  # no copy was made
+    d = pin(r.directed_in_costs, np.uint32, shifts[2])
+    return IsolatedRouteRequest(grid, r.nets, r.windows, r.x_edge_costs, r.y_edge_costs, r.via_edge_costs, d)
+
+
+def _big_bytes(reqs):
+    b = 0
+    for r in reqs:
+        n = len(r.grid.dims)
+        b += 4 * n + (n if r.grid.board_constraint is not None or r.grid.via_forbidden is not None else 0)
+        b += 16 * n if r.directed_in_costs is not None else 0
+    return b
+
+
+@pytest.mark.parametrize("shifts", [(0, 0, 0), (4, 1, 8)], ids=["aligned", "unaligned"])
+def test_page_locked_instances_are_read_in_place(engine, oracle, shifts):
+    """Instances whose board arrays are page-locked are gathered straight from
+    host memory by one launch (16-byte, word and byte paths; flag bytes built
+    from both masks); the answers equal the staged upload's and the oracle's.
+    A set that mixes page-locked and pageable instances takes the staged path."""
+    rng = np.random.default_rng(78)
+    reqs = []
+    for trial in range(40):
+        r = _random_case(rng, trial, directed=trial % 3 == 0, max_side=70, max_layers=12 if trial % 5 == 0 else 4)
+        if r is not None:
+            reqs.append(r)
+    pinned = [_pinned_request(engine, r, shifts) for r in reqs]
+    before = engine.upload_stats()
+    got = engine.route_instances(pinned, keep_fields=True)
+    after = engine.upload_stats()
+    assert after["in_place_bytes"] - before["in_place_bytes"] == _big_bytes(reqs)
+    assert after["staged_bytes"] == before["staged_bytes"]
+    exp = _oracle_each(oracle, reqs, mode="field")
+    staged = engine.route_instances(reqs, keep_fields=True)
+    for k, (g, s, e) in enumerate(zip(got, staged, exp)):
+        assert (g.paths, g.search_costs) == e, k
+        assert all(np.array_equal(a, b) for a, b in zip(g.fields, s.fields)), k
+    mixed = [p if k % 2 else r for k, (p, r) in enumerate(zip(pinned, reqs))]
+    before = engine.upload_stats()
+    got = engine.route_instances(mixed)
+    assert engine.upload_stats()["in_place_bytes"] == before["in_place_bytes"]
+    assert [(g.paths, g.search_costs) for g in got] == exp
+
+
+def test_page_locked_uneven_instances_span_many_chunks(engine, oracle):
+    """256 uneven instances (boards up to 1024x1024x8, spans of many 64 KiB
+    gather chunks) read in place equal the staged upload and the oracle."""
+    s = W.uneven_instances(seed=12, n_instances=256)
+    reqs = s.requests()
+    pinned = [_pinned_request(engine, r) for r in reqs]
+    got = engine.route_instances(pinned)
+    staged = engine.route_instances(reqs)
+    assert [(g.paths, g.search_costs) for g in got] == [(g.paths, g.search_costs) for g in staged]
+    for k in range(0, 256, 16):
+        assert (got[k].paths, got[k].search_costs) == oracle.isolated_batch(reqs[k], retry_full=True, mode="astar"), k
+
+
+def test_page_locked_single_board_upload(engine, oracle):
+    """A single-board call with page-locked arrays copies them in place."""
+    rng = np.random.default_rng(79)
+    r = None
+    trial = 0
+    while r is None:
+        r = _random_case(rng, trial, directed=True, max_side=60, max_layers=4)
+        trial += 1
+    p = _pinned_request(engine, r)
+    before = engine.upload_stats()
+    got = engine.route_isolated_batch(p)
+    assert engine.upload_stats()["in_place_bytes"] - before["in_place_bytes"] == _big_bytes([r])
+    assert (got.paths, got.search_costs) == oracle.isolated_batch(r, retry_full=True, mode="field")
