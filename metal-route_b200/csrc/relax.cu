@@ -105,68 +105,107 @@ struct Tile {
     }
 };
 
-// One directional pass over lines of K*S cells, S consecutive lanes per line
-// (K cells each), skipping lines whose dirty flag is clear.  Each lane runs its
+// Line passes over lines of K*S cells, S consecutive lanes per line (K cells
+// each), skipping lines whose dirty flag is clear.  Each lane runs its
 // segment's local chain, the S lanes combine their transfer functions
 // f(t) = min(A, t (+) (D, H)) with a Kogge-Stone scan (H, the hop count, is the
-// group's cell count), and every cell takes
-// min(local, incoming (+) prefix).  `cell(line, pos, &lab, &step)` maps the
-// pos-th cell of a line in traversal order; `halo(line)` is the label index
-// before the first cell; `touch(line, pos)` marks the crossing lines of a cell
-// whose label fell; `clear` resets the line's dirty flag (last pass of a pair).
+// group's cell count), and every cell takes min(local, incoming (+) prefix).
+// `halo(line, &before, &after)` gives the label indices outside both ends;
+// `touch(line, pos)` marks the crossing lines of a cell whose label fell.
+// Both directions of a line run in one pass: the forward scan, then, on its
+// results still in registers, the backward scan (mirror image: shuffles down,
+// the halo after the last cell).  A 1-D line is closed by one forward and one
+// backward scan, so one load and one store of each label serve both.  `cell(line, pos, &lab,
+// &step_fwd, &step_bwd)`: step_fwd prices the move into the cell from its
+// predecessor in traversal order, step_bwd the move from its successor.
 template <int K, int S, class CellFn, class HaloFn, class TouchFn>
-__device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *dirty, uint32_t nlines, bool clear,
-                                         CellFn cell, HaloFn halo, TouchFn touch) {
+__device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *dirty, uint32_t nlines, CellFn cell,
+                                          HaloFn halo, TouchFn touch) {
     bool changed = false;
-    const uint32_t lanes_total = nlines * S;  // a multiple of 32: whole warps are active or idle
+    const uint32_t lanes_total = nlines * S;
     for (uint32_t base = 0; base < lanes_total; base += blockDim.x) {
         if (base + (threadIdx.x & ~31u) >= lanes_total) break;
         const uint32_t tl = base + threadIdx.x;
         const uint32_t line = tl / S, seg = tl % S;
         const bool mine = dirty[line] != 0;
         const uint32_t mask = __ballot_sync(0xFFFFFFFFu, mine);
-        if (!mine) continue;  // whole S-lane groups drop out together
-        if (clear && seg == 0) dirty[line] = 0;
+        if (!mine) continue;
+        if (seg == 0) dirty[line] = 0;
         u64 v[K], u[K];
-        uint32_t sp[K], P[K], li[K];
+        uint32_t spf[K], spb[K], P[K], li[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            uint32_t sidx;
-            cell(line, seg * K + i, &li[i], &sidx);
+            uint32_t sf, sb;
+            cell(line, seg * K + i, &li[i], &sf, &sb);
             v[i] = lab[li[i]];
-            sp[i] = st[sidx];
+            spf[i] = st[sf];
+            spb[i] = st[sb];
         }
+        uint32_t hf, hb;
+        halo(line, &hf, &hb);
+        // forward
         u[0] = v[0];
-        P[0] = sp[0];
+        P[0] = spf[0];
 #pragma unroll
         for (int i = 1; i < K; ++i) {
-            u[i] = umin64(v[i], ext2(u[i - 1], sp[i], 1));
-            P[i] = dsum(P[i - 1], sp[i]);
+            u[i] = umin64(v[i], ext2(u[i - 1], spf[i], 1));
+            P[i] = dsum(P[i - 1], spf[i]);
         }
-        // The hop counts need no shuffles: before step o a participating lane's
-        // group spans o segments (K*o cells), and after the scan the group of
-        // lane seg-1 spans segments 0..seg-1 (K*seg cells).
-        u64 A = u[K - 1];
-        uint32_t D = P[K - 1];
+        {
+            u64 A = u[K - 1];
+            uint32_t D = P[K - 1];
 #pragma unroll
-        for (int o = 1; o < S; o <<= 1) {
-            const u64 Ap = __shfl_up_sync(mask, A, o, S);
-            const uint32_t Dp = __shfl_up_sync(mask, D, o, S);
-            if (seg >= (uint32_t)o) {
-                A = umin64(A, ext2(Ap, D, (uint32_t)(K * o)));
-                D = dsum(Dp, D);
+            for (int o = 1; o < S; o <<= 1) {
+                const u64 Ap = __shfl_up_sync(mask, A, o, S);
+                const uint32_t Dp = __shfl_up_sync(mask, D, o, S);
+                if (seg >= (uint32_t)o) {
+                    A = umin64(A, ext2(Ap, D, (uint32_t)(K * o)));
+                    D = dsum(Dp, D);
+                }
+            }
+            const u64 hl = lab[hf];
+            u64 C = hl;
+            if (S > 1) {
+                const u64 Fa = __shfl_up_sync(mask, A, 1, S);
+                const uint32_t Fd = __shfl_up_sync(mask, D, 1, S);
+                if (seg > 0) C = umin64(Fa, ext2(hl, Fd, K * seg));
+            }
+            if (C != kInf) {
+#pragma unroll
+                for (int i = 0; i < K; ++i) u[i] = umin64(u[i], ext2(C, P[i], (uint32_t)i + 1u));
             }
         }
-        const u64 hl = lab[halo(line)];
-        u64 C = hl;
-        if (S > 1) {
-            const u64 Fa = __shfl_up_sync(mask, A, 1, S);
-            const uint32_t Fd = __shfl_up_sync(mask, D, 1, S);
-            if (seg > 0) C = umin64(Fa, ext2(hl, Fd, K * seg));
-        }
-        if (C != kInf) {
+        // backward over the forward results; segment sb = S-1-seg counts from the far end
+        {
+            const uint32_t sbk = (uint32_t)(S - 1) - seg;
+            P[K - 1] = spb[K - 1];
 #pragma unroll
-            for (int i = 0; i < K; ++i) u[i] = umin64(u[i], ext2(C, P[i], (uint32_t)i + 1u));
+            for (int i = K - 2; i >= 0; --i) {
+                u[i] = umin64(u[i], ext2(u[i + 1], spb[i], 1));
+                P[i] = dsum(P[i + 1], spb[i]);
+            }
+            u64 A = u[0];
+            uint32_t D = P[0];
+#pragma unroll
+            for (int o = 1; o < S; o <<= 1) {
+                const u64 Ap = __shfl_down_sync(mask, A, o, S);
+                const uint32_t Dp = __shfl_down_sync(mask, D, o, S);
+                if (sbk >= (uint32_t)o) {
+                    A = umin64(A, ext2(Ap, D, (uint32_t)(K * o)));
+                    D = dsum(Dp, D);
+                }
+            }
+            const u64 hr = lab[hb];
+            u64 C = hr;
+            if (S > 1) {
+                const u64 Fa = __shfl_down_sync(mask, A, 1, S);
+                const uint32_t Fd = __shfl_down_sync(mask, D, 1, S);
+                if (sbk > 0) C = umin64(Fa, ext2(hr, Fd, K * sbk));
+            }
+            if (C != kInf) {
+#pragma unroll
+                for (int i = 0; i < K; ++i) u[i] = umin64(u[i], ext2(C, P[i], (uint32_t)(K - i)));
+            }
         }
 #pragma unroll
         for (int i = 0; i < K; ++i) {
@@ -179,7 +218,6 @@ __device__ __forceinline__ bool seg_pass(u64 *lab, const uint32_t *st, uint8_t *
     }
     return changed;
 }
-
 
 // Grid-wide barrier for a cooperative launch.  The wait is bounded: after
 // kBarrierSpinLimit polls it records kStatusBarrier and returns, and every CTA
@@ -248,24 +286,18 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
     const uint32_t L = t.L;
     bool ch = false;
     ch |= seg_pass<KC, SR>(
-        t.lab, t.st, t.rowd, L * TH, false,
-        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
+        t.lab, t.st, t.rowd, L * TH,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *sf, uint32_t *sb) {
             const uint32_t l = line / TH, y = line % TH;
             *li = t.li(l, y + 1, pos + 1);
-            *si = t.si(kFromNegX, l, y, pos);
+            *sf = t.si(kFromNegX, l, y, pos);
+            *sb = t.si(kFromPosX, l, y, pos);
         },
-        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 0); },
+        [&](uint32_t line, uint32_t *hf, uint32_t *hb) {
+            *hf = t.li(line / TH, line % TH + 1, 0);
+            *hb = t.li(line / TH, line % TH + 1, 33);
+        },
         [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, pos); });
-    __syncwarp();
-    ch |= seg_pass<KC, SR>(
-        t.lab, t.st, t.rowd, L * TH, true,
-        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
-            const uint32_t l = line / TH, y = line % TH, x = 31 - pos;
-            *li = t.li(l, y + 1, x + 1);
-            *si = t.si(kFromPosX, l, y, x);
-        },
-        [&](uint32_t line) { return t.li(line / TH, line % TH + 1, 33); },
-        [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, 31 - pos); });
     // rows -> columns: only the warps of the same layers exchange data
     if constexpr (TH == 8 && kLaneCells == 4) {
         pair_barrier();
@@ -273,24 +305,18 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         __syncthreads();
     }
     ch |= seg_pass<KC, SC>(
-        t.lab, t.st, t.cold, L * 32, false,
-        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
+        t.lab, t.st, t.cold, L * 32,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *sf, uint32_t *sb) {
             const uint32_t l = line / 32, x = line % 32;
             *li = t.li(l, pos + 1, x + 1);
-            *si = t.si(kFromNegY, l, pos, x);
+            *sf = t.si(kFromNegY, l, pos, x);
+            *sb = t.si(kFromPosY, l, pos, x);
         },
-        [&](uint32_t line) { return t.li(line / 32, 0, line % 32 + 1); },
+        [&](uint32_t line, uint32_t *hf, uint32_t *hb) {
+            *hf = t.li(line / 32, 0, line % 32 + 1);
+            *hb = t.li(line / 32, TH + 1, line % 32 + 1);
+        },
         [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, pos, line % 32); });
-    __syncwarp();
-    ch |= seg_pass<KC, SC>(
-        t.lab, t.st, t.cold, L * 32, true,
-        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *si) {
-            const uint32_t l = line / 32, x = line % 32, y = TH - 1 - pos;
-            *li = t.li(l, y + 1, x + 1);
-            *si = t.si(kFromPosY, l, y, x);
-        },
-        [&](uint32_t line) { return t.li(line / 32, TH + 1, line % 32 + 1); },
-        [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, TH - 1 - pos, line % 32); });
     if (L > 1) {
         __syncthreads();
         ch |= stack_pass<TH>(t);
