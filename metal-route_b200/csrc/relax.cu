@@ -325,40 +325,83 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
 }
 
 // Layer stacks: one thread per (y, x) column of the tile, upward then downward.
+// Stacks of up to kStackRegs layers are held in registers between the two
+// directions (one load and at most one store per label); taller ones run from
+// shared memory.
+constexpr uint32_t kStackRegs = 4;
+
 template <int TH>
 __device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
     const uint32_t L = t.L;
     bool ch = false;
-    {
-        for (uint32_t r = threadIdx.x; r < TH * 32; r += blockDim.x) {
-            if (!t.stackd[r]) continue;
-            t.stackd[r] = 0;
-            const uint32_t y = r / 32, x = r % 32;
+    for (uint32_t r = threadIdx.x; r < TH * 32; r += blockDim.x) {
+        if (!t.stackd[r]) continue;
+        t.stackd[r] = 0;
+        const uint32_t y = r / 32, x = r % 32;
+        if (L <= kStackRegs) {
+            u64 v[kStackRegs];
+            uint32_t fell = 0;  // bit l: the label of layer l fell
+#pragma unroll
+            for (uint32_t l = 0; l < kStackRegs; ++l)
+                if (l < L) v[l] = t.lab[t.li(l, y + 1, x + 1)];
             u64 prev = kInf;
-            for (uint32_t l = 0; l < L; ++l) {
-                const uint32_t c = t.li(l, y + 1, x + 1);
-                const u64 cur = t.lab[c];
-                const u64 w = umin64(cur, ext2(prev, l ? t.st[t.si(kFromBelow, l, y, x)] : kMax, 1));
-                if (w < cur) {
-                    t.lab[c] = w;
+#pragma unroll
+            for (uint32_t l = 0; l < kStackRegs; ++l) {
+                if (l < L) {
+                    const u64 w = ext2(prev, l ? t.st[t.si(kFromBelow, l, y, x)] : kMax, 1);
+                    if (w < v[l]) {
+                        v[l] = w;
+                        fell |= 1u << l;
+                    }
+                    prev = v[l];
+                }
+            }
+            prev = kInf;
+#pragma unroll
+            for (int l = (int)kStackRegs - 1; l >= 0; --l) {
+                if ((uint32_t)l < L) {
+                    const u64 w = ext2(prev, (uint32_t)l + 1 < L ? t.st[t.si(kFromAbove, (uint32_t)l, y, x)] : kMax, 1);
+                    if (w < v[l]) {
+                        v[l] = w;
+                        fell |= 1u << l;
+                    }
+                    prev = v[l];
+                }
+            }
+#pragma unroll
+            for (uint32_t l = 0; l < kStackRegs; ++l) {
+                if ((fell >> l) & 1u) {
+                    t.lab[t.li(l, y + 1, x + 1)] = v[l];
                     t.touched_by_stack(l, y, x);
                     ch = true;
                 }
-                prev = w;
             }
-            prev = kInf;
-            for (int l = (int)L - 1; l >= 0; --l) {
-                const uint32_t c = t.li((uint32_t)l, y + 1, x + 1);
-                const u64 cur = t.lab[c];
-                const u64 w =
-                    umin64(cur, ext2(prev, (uint32_t)l + 1 < L ? t.st[t.si(kFromAbove, (uint32_t)l, y, x)] : kMax, 1));
-                if (w < cur) {
-                    t.lab[c] = w;
-                    t.touched_by_stack((uint32_t)l, y, x);
-                    ch = true;
-                }
-                prev = w;
+            continue;
+        }
+        u64 prev = kInf;
+        for (uint32_t l = 0; l < L; ++l) {
+            const uint32_t c = t.li(l, y + 1, x + 1);
+            const u64 cur = t.lab[c];
+            const u64 w = umin64(cur, ext2(prev, l ? t.st[t.si(kFromBelow, l, y, x)] : kMax, 1));
+            if (w < cur) {
+                t.lab[c] = w;
+                t.touched_by_stack(l, y, x);
+                ch = true;
             }
+            prev = w;
+        }
+        prev = kInf;
+        for (int l = (int)L - 1; l >= 0; --l) {
+            const uint32_t c = t.li((uint32_t)l, y + 1, x + 1);
+            const u64 cur = t.lab[c];
+            const u64 w =
+                umin64(cur, ext2(prev, (uint32_t)l + 1 < L ? t.st[t.si(kFromAbove, (uint32_t)l, y, x)] : kMax, 1));
+            if (w < cur) {
+                t.lab[c] = w;
+                t.touched_by_stack((uint32_t)l, y, x);
+                ch = true;
+            }
+            prev = w;
         }
     }
     return ch;
