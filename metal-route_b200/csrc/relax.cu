@@ -55,18 +55,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Label extended by a run of `h` steps whose prices sum to `d` (kMax = blocked or
-// saturated); a dist reaching 0xFFFFFFFF is unreachable.
+// saturated); a dist reaching 0xFFFFFFFF is unreachable.  With 32-bit wrapping
+// addition, td or d equal to kMax always gives nd < td or nd == kMax, so those
+// two tests cover the blocked operands too.
 __device__ __forceinline__ u64 ext2(u64 t, uint32_t d, uint32_t h) {
     const uint32_t td = (uint32_t)(t >> 32);
     const uint32_t nd = td + d;
-    const bool bad = (td == kMax) | (d == kMax) | (nd < td) | (nd == kMax);
+    const bool bad = (nd < td) | (nd == kMax);
     return bad ? kInf : (((u64)nd << 32) | (uint32_t)((uint32_t)t + h));
 }
 
-// Saturating sum of step prices; kMax absorbs.
+// Saturating sum of step prices; kMax absorbs (an operand equal to kMax gives
+// s == kMax or s < a under wrapping addition).
 __device__ __forceinline__ uint32_t dsum(uint32_t a, uint32_t b) {
     const uint32_t s = a + b;
-    return (a == kMax) | (b == kMax) | (s < a) ? kMax : s;
+    return s < a ? kMax : s;
 }
 
 __device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
@@ -696,27 +699,33 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
 
     // ---- write back and find neighbours this tile can improve -------
     u64 *labw = a.lab + f.lab_off;
-    // the tile is held by this CTA alone (both schedules), so plain stores
-    for (uint32_t i = tid; i < L * th * tw; i += blockDim.x) {
-        const uint32_t tx = i % tw, r = i / tw, ty = r % th, l = r / th;
+    // the tile is held by this CTA alone (both schedules), so plain stores;
+    // indices are split by the compile-time tile shape (cells past a ragged
+    // window edge are skipped)
+    for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
+        const uint32_t tx = i % kTW, r = i / kTW, ty = r % TH, l = r / TH;
+        if (tx >= tw || ty >= th) continue;
         const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
         labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
     }
     // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
-    const uint32_t nb = 2 * L * th + 2 * L * tw;
+    const uint32_t nb = 2 * L * TH + 2 * L * kTW;
     for (uint32_t i = tid; i < nb; i += blockDim.x) {
         uint32_t side, l, k;
-        if (i < 2 * L * th) {
-            side = i / (L * th);
-            const uint32_t r = i % (L * th);
-            l = r / th;
-            k = r % th;
+        if (i < 2 * L * TH) {
+            side = i >= L * TH;
+            const uint32_t r = i - side * L * TH;
+            l = r / TH;
+            k = r % TH;
+            if (k >= th) continue;
         } else {
-            const uint32_t j = i - 2 * L * th;
-            side = 2 + j / (L * tw);
-            const uint32_t r = j % (L * tw);
-            l = r / tw;
-            k = r % tw;
+            const uint32_t j = i - 2 * L * TH;
+            const uint32_t hi = j >= L * kTW;
+            side = 2 + hi;
+            const uint32_t r = j - hi * L * kTW;
+            l = r / kTW;
+            k = r % kTW;
+            if (k >= tw) continue;
         }
         bool exists;
         uint32_t bsx, bsy, nsx, nsy, dir;
