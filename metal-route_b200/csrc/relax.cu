@@ -1013,9 +1013,7 @@ __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevFiel
 // (the flags of both cells, the enter cost and the base price), so a step costs
 // one memory round trip instead of a chain of dependent ones.
 __device__ __forceinline__ uint32_t walk_step(const DevBoard &b, const DevField &f, const uint32_t *pads,
-                                              uint32_t p, uint32_t cur, int kind) {
-    const uint32_t plane = b.w * b.h;
-    const uint32_t r = cur % plane, x = r % b.w, y = r / b.w, l = cur / plane;
+                                              uint32_t p, uint32_t cur, uint32_t x, uint32_t y, uint32_t l, int kind) {
     const uint8_t fc = b.flags ? __ldg(b.flags + cur) : 0, fp = b.flags ? __ldg(b.flags + p) : 0;
     const uint32_t cc = __ldg(b.cost + cur);
     uint32_t base = 0;
@@ -1058,10 +1056,52 @@ __device__ __forceinline__ uint32_t walk_step(const DevBoard &b, const DevField 
     return capmul(base, ec);
 }
 
-// One warp per field: lanes 0..5 test the six neighbours (ascending CellIdx)
-// and the lowest qualifying one is the canonical predecessor.  Each step issues
-// all of its loads at once (the candidate's label and tile flag, and the step
-// inputs) and carries the winner's label forward as the next target.
+// Neighbour `kind` of (x, y, l): 0 the layer below, 1 -y, 2 -x, 3 +x, 4 +y,
+// 5 the layer above (ascending CellIdx); kind 5 - k is the opposite of k.
+__device__ __forceinline__ void walk_offset(int kind, int &x, int &y, int &l) {
+    if (kind == 0) l -= 1;
+    else if (kind == 1) y -= 1;
+    else if (kind == 2) x -= 1;
+    else if (kind == 3) x += 1;
+    else if (kind == 4) y += 1;
+    else l += 1;
+}
+
+// Label of window cell (x, y, l) (absolute coordinates inside the window), or
+// +inf when its tile was never visited.
+__device__ __forceinline__ u64 walk_label(const PathArgs &a, const DevField &f, uint32_t ntx, uint32_t tile_shift,
+                                          int x, int y, int l) {
+    const uint32_t lx = (uint32_t)x - f.x0, ly = (uint32_t)y - f.y0;
+    const u64 raw = a.lab[f.lab_off + ((uint64_t)(uint32_t)l * f.wh + ly) * f.ww + lx];
+    if (a.arena_filled) return raw;
+    return a.tvisit[f.tile_off + (ly >> tile_shift) * ntx + lx / kTW] ? raw : kInf;
+}
+
+__device__ __forceinline__ bool walk_inside(const DevField &f, const DevBoard &b, int x, int y, int l) {
+    return l >= 0 && l < (int)b.layers && x >= (int)f.x0 && x < (int)(f.x0 + f.ww) && y >= (int)f.y0 &&
+           y < (int)(f.y0 + f.wh);
+}
+
+// Is the neighbour `kind` of target t = (tx, ty, tl) a predecessor of t, i.e.
+// its label extended by the step into t equals `need`?  Its cell and label are
+// returned for the caller to carry forward.
+__device__ __forceinline__ bool walk_try(const PathArgs &a, const DevField &f, const DevBoard &b, uint32_t ntx,
+                                         uint32_t tile_shift, int tx, int ty, int tl, uint32_t t, u64 need, int kind,
+                                         uint32_t *q, u64 *lq) {
+    int px = tx, py = ty, pl = tl;
+    walk_offset(kind, px, py, pl);
+    if (!walk_inside(f, b, px, py, pl)) return false;
+    *q = ((uint32_t)pl * b.h + (uint32_t)py) * b.w + (uint32_t)px;
+    *lq = walk_label(a, f, ntx, tile_shift, px, py, pl);
+    const uint32_t st = walk_step(b, f, a.pads, *q, t, (uint32_t)tx, (uint32_t)ty, (uint32_t)tl, kind);
+    return *lq != kInf && extend(*lq, st) == need;
+}
+
+// One warp per field: lanes 0..5 test the six neighbours of the current cell
+// (ascending CellIdx) and the lowest qualifying one is the canonical
+// predecessor.  Each step issues all of its loads at once (the candidate's
+// label and tile flag, and the step inputs) and carries the winner's label and
+// coordinates forward, so no step divides a cell index.
 __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
@@ -1072,41 +1112,28 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
     const DevBoard b = a.boards[f.board];
     const uint32_t plane = b.w * b.h;
     const uint32_t ntx = (f.ww + kTW - 1) / kTW;
+    const uint32_t tile_shift = (uint32_t)(__ffs((int)a.tile_h) - 1);  // tile heights are powers of two
     uint32_t *out = a.cells + a.offsets[f.out];
     uint32_t cur = f.dst;
-    u64 need;
+    int cx, cy, cl;
     {
         const uint32_t r = cur % plane;
-        need = field_label(a, f, r % b.w - f.x0, r / b.w - f.y0, cur / plane);
+        cx = (int)(r % b.w);
+        cy = (int)(r / b.w);
+        cl = (int)(cur / plane);
     }
+    u64 need = walk_label(a, f, ntx, tile_shift, cx, cy, cl);
     for (uint32_t pos = len - 1;; --pos) {
         if (lane == 0) out[pos] = cur;
         if (pos == 0) {
             if (lane == 0 && cur != f.src) atomicOr(a.status, kStatusPathBroken);
-            break;
+            return;
         }
-        const uint32_t r = cur % plane, x = r % b.w, y = r / b.w, l = cur / plane;
         bool ok = false;
         uint32_t p = 0;
         u64 lp = kInf;
         if (lane < 6) {
-            int px = (int)x, py = (int)y, pl = (int)l;
-            if (lane == 0) pl -= 1;
-            else if (lane == 1) py -= 1;
-            else if (lane == 2) px -= 1;
-            else if (lane == 3) px += 1;
-            else if (lane == 4) py += 1;
-            else pl += 1;
-            if (pl >= 0 && pl < (int)b.layers && px >= (int)f.x0 && px < (int)(f.x0 + f.ww) && py >= (int)f.y0 &&
-                py < (int)(f.y0 + f.wh)) {
-                p = ((uint32_t)pl * b.h + (uint32_t)py) * b.w + (uint32_t)px;
-                const uint32_t lx = (uint32_t)px - f.x0, ly = (uint32_t)py - f.y0;
-                const uint32_t vis = a.tvisit[f.tile_off + (ly / a.tile_h) * ntx + lx / kTW];
-                const u64 raw = a.lab[f.lab_off + ((uint64_t)pl * f.wh + ly) * f.ww + lx];
-                const uint32_t st = walk_step(b, f, a.pads, p, cur, (int)lane);
-                lp = vis ? raw : kInf;
-                ok = lp != kInf && extend(lp, st) == need;
-            }
+            ok = walk_try(a, f, b, ntx, tile_shift, cx, cy, cl, cur, need, (int)lane, &p, &lp);
         }
         const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
         if (m == 0) {
@@ -1116,6 +1143,7 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
         const uint32_t win = __ffs(m) - 1;
         cur = __shfl_sync(0xFFFFFFFFu, p, win);
         need = __shfl_sync(0xFFFFFFFFu, lp, win);
+        walk_offset((int)win, cx, cy, cl);
     }
 }
 
