@@ -420,11 +420,19 @@ def run_snapshot(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1 or args.shards:
+        if args.groups:
+            raise SystemExit("--groups: connection groups need every path, so they do not run sharded")
         return run_snapshot_sharded(args, rank, world, local)
     wl = W.snapshot_board(n_nets=args.nets or 3000)
+    groups = None
+    if args.groups:
+        # nets renamed into '#'-sibling connection groups of args.groups nets
+        wl.nets = [mrcuda.NetEndpoints(f"s{i // args.groups}#{i % args.groups}", nt.src, nt.dst,
+                                       nt.passable_pads, nt.via_passable_pads) for i, nt in enumerate(wl.nets)]
+        groups = "connections"
     req = wl.request()
     eng = mrcuda.Engine(local)
-    warm = eng.negotiation(req)
+    warm = eng.negotiation(req, groups=groups)
     for _ in range(max(args.warmup, 3)):
         warm.round()
     warm.close()
@@ -432,7 +440,7 @@ def run_snapshot(args):
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
-    neg = eng.negotiation(req)
+    neg = eng.negotiation(req, groups=groups)
     rounds = []
     for _ in range(args.steps):
         st = neg.round()
@@ -456,6 +464,8 @@ def run_snapshot(args):
         "warmup": max(args.warmup, 3), "ms_per_step": dev_ms / max(len(rounds), 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl.meta["workload"], "rounds": len(rounds), "nets_routed": routed,
+                   "groups": (f"connection groups: '#'-siblings of {args.groups} nets, plus shared endpoints"
+                              if args.groups else "every net its own group"),
                    "window_cells": cells, "l2": "inputs larger than L2 (25M-cell board, 400 MB price planes)",
                    "per_round": [{k: r[k] for k in ("round", "dirty", "routed", "retried", "overused_edges",
                                                      "round_ms")} for r in rounds]},
@@ -482,7 +492,7 @@ def run_snapshot(args):
                                 "sample": f"{ns} nets of round 0 (snapshot = base prices), search with h = 0 "
                                           f"(directed prices), {cores} host threads, {dt:.2f} s"}
     # gpu launches: per round 4 negotiation kernels + the batch sequence (+ a retry batch)
-    line["gpu_launches"] = sum(4 + 4 + (4 if r["retried"] else 0) for r in rounds)
+    line["gpu_launches"] = sum(4 + 4 + (4 if r["retried"] else 0) + (1 if groups else 0) for r in rounds)
     print(json.dumps(line))
     neg.close()
     eng.close()
@@ -660,6 +670,8 @@ def main():
     ap.add_argument("--serve-max", type=int, default=600, help="serving: most requests per rate")
     ap.add_argument("--slots", type=int, default=2, help="serving: launches in flight")
     ap.add_argument("--shards", action="store_true", help="snapshot: run the sharded rounds even on one rank")
+    ap.add_argument("--groups", type=int, default=0,
+                    help="snapshot: group nets into '#'-sibling connection groups of this size (0 = none)")
     ap.add_argument("--nets", type=int, default=0, help="route only the first N nets (0 = all)")
     ap.add_argument("--cpu-sample", type=int, default=0, help="nets timed on the CPU (0 = workload default)")
     ap.add_argument("--plain-sample", type=int, default=0, help="nets timed one per launch (0 = workload default)")

@@ -343,6 +343,18 @@ mrc_status mrc_negotiation_create(mrc_context *ctx, const mrc_isolated_request *
 /* Runs the next round.  A round with no dirty net does nothing (converged). */
 mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *neg, mrc_round_stats *stats);
 
+/* Connection groups (the reference's connection_group_ids,
+ * crates/mr-cpu/src/negotiated.rs:929-989, and its group-aware overuse scan,
+ * :1923-1943): nets of one group may share edges.  With groups set, an edge is
+ * overused when nets of two or more distinct groups use it; history, the
+ * overused count and the next dirty set follow that test (occupancy prices are
+ * unchanged: every net still pays for every other net's presence, as in
+ * route_negotiated).  groups[i] is net i's group id (any value but 0xFFFFFFFF;
+ * the reference's are dense first-appearance ids).  Called before the first
+ * round; not on a shard, whose nets see only part of the paths.  Without this
+ * call every net is its own group. */
+mrc_status mrc_negotiation_set_groups(mrc_context *ctx, mrc_negotiation *neg, const uint32_t *groups);
+
 /* Sharded rounds (one shard per GPU, each routing its own nets of the same
  * board).  A shard keeps the occupancy of its own paths ("local") and a global
  * occupancy that the caller sets to the sum of every shard's local one (an

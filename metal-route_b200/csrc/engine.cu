@@ -1575,6 +1575,8 @@ struct mrc_negotiation {
     mrc_round_stats pending{};         // statistics of the round in progress
     DBuf d_present, d_history, d_snap, d_off, d_cells, d_list, d_flags, d_count;
     DBuf d_global;                     // sharded: sum of every shard's d_present
+    bool grouped = false;              // overuse counts connection groups, not nets
+    DBuf d_group, d_first, d_over;     // group of every net; per slot: first group seen, overused flag
     const uint4 *global() const { return sharded ? d_global.as<uint4>() : d_present.as<uint4>(); }
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~mrc_negotiation() {
@@ -1792,14 +1794,31 @@ mrc_status mrc_negotiation_settle(mrc_context *ctx, mrc_negotiation *ng, mrc_rou
     const GridView &g = ng->base->view;
     cudaStream_t s = ctx->stream;
     MRC_CUDA(cudaMemsetAsync(ng->d_count.p, 0, 8, s), "clear count");
+    const uint32_t n = (uint32_t)ng->nets.size();
+    if (ng->grouped) {
+        // group-aware overuse of the current paths of every net
+        MRC_CUDA(cudaMemsetAsync(ng->d_first.p, 0xFF, (size_t)g.n * 16, s), "clear group claims");
+        MRC_CUDA(cudaMemsetAsync(ng->d_over.p, 0, (size_t)g.n * 4, s), "clear overuse flags");
+        GroupArgs ga;
+        ga.offsets = ng->d_off.as<unsigned long long>();
+        ga.cells = ng->d_cells.as<uint32_t>();
+        ga.group = ng->d_group.as<uint32_t>();
+        ga.n_nets = n;
+        ga.w = g.w;
+        ga.plane = g.w * g.h;
+        ga.first = ng->d_first.as<uint32_t>();
+        ga.over = ng->d_over.as<uint8_t>();
+        MRC_CUDA(group_overuse_launch(ga, s), "group overuse scan");
+    }
+    const uint8_t *over = ng->grouped ? ng->d_over.as<uint8_t>() : nullptr;
     OveruseArgs oa;
     oa.present = ng->global();
+    oa.over = over;
     oa.history = ng->d_history.as<uint4>();
     oa.n = g.n;
     oa.step = ng->params.history_step;
     oa.count = ng->d_count.as<unsigned long long>();
     MRC_CUDA(overuse_launch(oa, s), "overuse scan");
-    const uint32_t n = (uint32_t)ng->nets.size();
     DirtyArgs da;
     da.offsets = ng->d_off.as<unsigned long long>();
     da.cells = ng->d_cells.as<uint32_t>();
@@ -1807,6 +1826,7 @@ mrc_status mrc_negotiation_settle(mrc_context *ctx, mrc_negotiation *ng, mrc_rou
     da.w = g.w;
     da.plane = g.w * g.h;
     da.present = reinterpret_cast<const uint32_t *>(ng->global());
+    da.over = over;
     da.flags = ng->d_flags.as<uint8_t>();
     MRC_CUDA(dirty_launch(da, s), "dirty scan");
     MRC_CUDA(cudaEventRecord(ng->ev1, s), "record event");
@@ -1825,6 +1845,25 @@ mrc_status mrc_negotiation_settle(mrc_context *ctx, mrc_negotiation *ng, mrc_rou
     ng->round++;
     ng->phase = 0;
     if (out) *out = *st;
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_set_groups(mrc_context *ctx, mrc_negotiation *ng, const uint32_t *groups) {
+    if (!ctx || !ng || !groups) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ng->sharded) return fail(MRC_ERR_INVALID_ARGUMENT, "connection groups need every path: not on a shard");
+    if (ng->round != 0 || ng->phase != 0)
+        return fail(MRC_ERR_INVALID_ARGUMENT, "connection groups are set before the first round");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    const uint32_t n = (uint32_t)ng->nets.size();
+    for (uint32_t i = 0; i < n; ++i)
+        if (groups[i] == kNoGroup) return fail(MRC_ERR_INVALID_ARGUMENT, "group id 0xFFFFFFFF is reserved");
+    const size_t cells = (size_t)ng->base->view.n;
+    MRC_TRY(upload(ctx, ng->d_group, groups, (size_t)n * 4, "upload connection groups"));
+    MRC_TRY(ng->d_first.get(ctx, std::max<size_t>(cells * 16, 16), "group claims"));
+    MRC_TRY(ng->d_over.get(ctx, std::max<size_t>(cells * 4, 16), "overuse flags"));
+    MRC_CUDA(cudaStreamSynchronize(ctx->stream), "upload connection groups");
+    ng->grouped = true;
     return MRC_OK;
 }
 

@@ -82,6 +82,7 @@ struct SnapshotArgs {
 
 struct OveruseArgs {
     const uint4 *present;
+    const uint8_t *over;                // nullable: group-aware overuse flags, 4 per cell
     uint4 *history;
     uint64_t n;
     uint32_t step;
@@ -94,13 +95,27 @@ struct DirtyArgs {
     uint32_t n_nets;
     uint32_t w, plane;
     const uint32_t *present;
+    const uint8_t *over;                // nullable: group-aware overuse flags (else present >= 2)
     uint8_t *flags;                     // 1 = route again next round
+};
+
+constexpr uint32_t kNoGroup = 0xFFFFFFFFu;
+
+struct GroupArgs {
+    const unsigned long long *offsets;  // path CSR of every net
+    const uint32_t *cells;
+    const uint32_t *group;              // connection group of every net
+    uint32_t n_nets;
+    uint32_t w, plane;
+    uint32_t *first;                    // 4 per cell: first group seen, kNoGroup before any
+    uint8_t *over;                      // 4 per cell: 1 = used by two or more groups
 };
 
 cudaError_t occupancy_launch(const OccupancyArgs &a, cudaStream_t st);
 cudaError_t snapshot_launch(const SnapshotArgs &a, cudaStream_t st);
 cudaError_t overuse_launch(const OveruseArgs &a, cudaStream_t st);
 cudaError_t dirty_launch(const DirtyArgs &a, cudaStream_t st);
+cudaError_t group_overuse_launch(const GroupArgs &a, cudaStream_t st);
 
 // Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);

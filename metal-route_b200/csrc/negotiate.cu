@@ -85,6 +85,30 @@ __global__ void snapshot_kernel(SnapshotArgs a) {
     }
 }
 
+// Group-aware overuse (the reference's scan, negotiated.rs:1923-1943, on edge
+// slots): every planar step of every current path claims both of its slots for
+// its net's connection group; a slot already claimed by another group is
+// overused.  The outcome does not depend on the order of the claims: a slot is
+// flagged exactly when two or more distinct groups use it.
+__global__ void group_overuse_kernel(GroupArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t net = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; net < a.n_nets; net += warps) {
+        const uint32_t g = a.group[net];
+        const u64 p0 = a.offsets[net], p1 = a.offsets[net + 1];
+        for (u64 k = p0 + lane; k + 1 < p1; k += 32) {
+            const uint32_t u = a.cells[k], v = a.cells[k + 1];
+            int su, sv;
+            if (!planar_slots(u, v, a.w, a.plane, &su, &sv)) continue;
+            const u64 iu = 4ull * u + su, iv = 4ull * v + sv;
+            const uint32_t ou = atomicCAS(a.first + iu, kNoGroup, g);
+            if (ou != kNoGroup && ou != g) a.over[iu] = 1;
+            const uint32_t ov = atomicCAS(a.first + iv, kNoGroup, g);
+            if (ov != kNoGroup && ov != g) a.over[iv] = 1;
+        }
+    }
+}
+
 __device__ __forceinline__ uint32_t bump(uint32_t h, bool over, uint32_t step, uint32_t *count) {
     if (!over) return h;
     ++*count;
@@ -96,13 +120,20 @@ __global__ void overuse_kernel(OveruseArgs a) {
     uint32_t count = 0;
     const u64 stride = (u64)gridDim.x * blockDim.x;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
-        const uint4 p = a.present[i];
-        if (p.x < 2 && p.y < 2 && p.z < 2 && p.w < 2) continue;
+        bool ox, oy, oz, ow;
+        if (a.over) {  // group-aware flags
+            const uchar4 o = reinterpret_cast<const uchar4 *>(a.over)[i];
+            ox = o.x, oy = o.y, oz = o.z, ow = o.w;
+        } else {
+            const uint4 p = a.present[i];
+            ox = p.x >= 2, oy = p.y >= 2, oz = p.z >= 2, ow = p.w >= 2;
+        }
+        if (!(ox | oy | oz | ow)) continue;
         uint4 h = a.history[i];
-        h.x = bump(h.x, p.x >= 2, a.step, &count);
-        h.y = bump(h.y, p.y >= 2, a.step, &count);
-        h.z = bump(h.z, p.z >= 2, a.step, &count);
-        h.w = bump(h.w, p.w >= 2, a.step, &count);
+        h.x = bump(h.x, ox, a.step, &count);
+        h.y = bump(h.y, oy, a.step, &count);
+        h.z = bump(h.z, oz, a.step, &count);
+        h.w = bump(h.w, ow, a.step, &count);
         a.history[i] = h;
     }
     // every undirected edge owns two slots: the host halves the slot count
@@ -119,7 +150,9 @@ __global__ void dirty_kernel(DirtyArgs a) {
         for (u64 k = p0 + lane; !hit && k + 1 < p1; k += 32) {
             const uint32_t u = a.cells[k], v = a.cells[k + 1];
             int su, sv;
-            if (planar_slots(u, v, a.w, a.plane, &su, &sv) && __ldg(a.present + 4ull * v + sv) >= 2) hit = true;
+            if (planar_slots(u, v, a.w, a.plane, &su, &sv) &&
+                (a.over ? __ldg(a.over + 4ull * v + sv) != 0 : __ldg(a.present + 4ull * v + sv) >= 2))
+                hit = true;
         }
         hit = __any_sync(0xffffffffu, hit);
         if (lane == 0) a.flags[net] = hit ? 1 : 0;
@@ -148,6 +181,12 @@ cudaError_t snapshot_launch(const SnapshotArgs &a, cudaStream_t st) {
 cudaError_t overuse_launch(const OveruseArgs &a, cudaStream_t st) {
     if (!a.n) return cudaSuccess;
     overuse_kernel<<<grid_for(a.n, 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t group_overuse_launch(const GroupArgs &a, cudaStream_t st) {
+    if (!a.n_nets) return cudaSuccess;
+    group_overuse_kernel<<<grid_for((u64)a.n_nets * 32, 256), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -17,6 +17,8 @@ from .types import (  # noqa: F401
     Grid,
     IsolatedRouteRequest,
     IsolatedRouteWindow,
+    connection_group_ids,
+    group_of,
     NetEndpoints,
 )
 from .api import (  # noqa: F401

@@ -29,6 +29,7 @@ import numpy as np
 from .types import (
     COST_MAX,
     Grid,
+    connection_group_ids,
     IsolatedRouteRequest,
     IsolatedRouteWindow,
     NetEndpoints,
@@ -193,6 +194,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_negotiation_read": (C.c_int, [vp, vp, vp, vp, vp]),
             "mrc_negotiation_dirty": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32p)]),
             "mrc_negotiation_destroy": (None, [vp]),
+            "mrc_negotiation_set_groups": (C.c_int, [vp, vp, vp]),
             "mrc_negotiation_create_shard": (C.c_int, [vp, C.POINTER(_Request), C.POINTER(_NegParams), vp,
                                                        C.POINTER(vp)]),
             "mrc_negotiation_ripup": (C.c_int, [vp, vp]),
@@ -554,7 +556,11 @@ class Negotiation:
     history_step to every edge two or more nets use."""
 
     def __init__(self, engine: "Engine", req: IsolatedRouteRequest, present_weight: int = 16,
-                 history_step: int = 1, owned: Optional[Sequence[bool]] = None):
+                 history_step: int = 1, owned: Optional[Sequence[bool]] = None, groups=None):
+        """`groups`: None (every net its own group), "connections" (the
+        reference's connection groups from the net names and shared endpoints),
+        or one group id per net; with groups an edge is overused only when nets
+        of two or more groups use it."""
         self.engine = engine
         self.n = len(req.nets)
         self.dims = req.grid.dims
@@ -571,6 +577,24 @@ class Negotiation:
             engine._check(engine.lib.mrc_negotiation_create_shard(engine.ctx, C.byref(r), prm, m.arr(mask),
                                                                   C.byref(h)))
         self.handle = h
+        try:
+            self._set_groups(req, groups)
+        except Exception:
+            self.close()
+            raise
+
+    def _set_groups(self, req: IsolatedRouteRequest, groups) -> None:
+        engine = self.engine
+        if groups is not None:
+            if isinstance(groups, str):
+                if groups != "connections":
+                    raise InvalidArgument("groups must be None, 'connections' or one id per net")
+                groups = connection_group_ids(req.nets)
+            g = np.ascontiguousarray(np.asarray(groups, dtype=np.uint32))
+            if g.size != self.n:
+                raise InvalidArgument("groups must have one entry per net")
+            engine._check(engine.lib.mrc_negotiation_set_groups(engine.ctx, self.handle,
+                                                                g.ctypes.data if g.size else None))
 
     @staticmethod
     def _stats(st) -> dict:
@@ -871,9 +895,10 @@ class Engine:
         return Server(self, **kw)
 
     def negotiation(self, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1,
-                    owned: Optional[Sequence[bool]] = None) -> Negotiation:
-        """An unsharded negotiation, or (with `owned`) this GPU's shard of one."""
-        return Negotiation(self, req, present_weight, history_step, owned)
+                    owned: Optional[Sequence[bool]] = None, groups=None) -> Negotiation:
+        """An unsharded negotiation, or (with `owned`) this GPU's shard of one;
+        `groups` as in Negotiation."""
+        return Negotiation(self, req, present_weight, history_step, owned, groups)
 
 
 def net_windows(dims, nets: Sequence[NetEndpoints]) -> List[IsolatedRouteWindow]:

@@ -12,7 +12,7 @@ carry no routing logic.  Field names and meanings follow the reference:
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import List, Optional, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -125,3 +125,49 @@ class IsolatedRouteRequest:
     y_edge_costs: Sequence[int]
     via_edge_costs: Sequence[Optional[int]]
     directed_in_costs: Optional[np.ndarray] = None
+
+
+def group_of(name: str) -> str:
+    """A net's connection-group name: the prefix before the first '#'
+    (negotiated.rs:915-922)."""
+    i = name.find("#")
+    return name if i < 0 else name[:i]
+
+
+def connection_group_ids(nets: Sequence[NetEndpoints]) -> List[int]:
+    """Dense connection-group ids, the reference's connection_group_ids
+    (negotiated.rs:929-989): nets whose names share a group_of prefix, or that
+    share an endpoint cell, are one group (union toward the lower index); ids
+    are numbered by the first appearance of each group's root."""
+    n = len(nets)
+    parent = list(range(n))
+
+    def find(x: int) -> int:
+        root = x
+        while parent[root] != root:
+            root = parent[root]
+        while parent[x] != root:
+            parent[x], x = root, parent[x]
+        return root
+
+    def union(a: int, b: int) -> None:
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            if ra < rb:
+                parent[rb] = ra
+            else:
+                parent[ra] = rb
+
+    by_name: Dict[str, int] = {}
+    for i, nt in enumerate(nets):
+        j = by_name.setdefault(group_of(nt.net), i)
+        if j != i:
+            union(i, j)
+    by_cell: Dict[int, int] = {}
+    for i, nt in enumerate(nets):
+        for c in (nt.src, nt.dst):
+            j = by_cell.setdefault(c, i)
+            if j != i:
+                union(i, j)
+    ids: Dict[int, int] = {}
+    return [ids.setdefault(find(i), len(ids)) for i in range(n)]

@@ -24,6 +24,11 @@ reference counts cells):
 
 Slots per cell are (-y, -x, +x, +y) in-edges; an undirected edge {a, b} counts
 at b's slot "from a" and at a's slot "from b".
+
+With connection groups (`groups`, one id per net) the overuse test is the
+reference's group-aware scan (:1923-1943): a slot is overused when nets of two
+or more distinct groups use it; history, the overused count and the next dirty
+set follow it, while prices still count every net's presence.
 """
 from __future__ import annotations
 
@@ -76,8 +81,9 @@ def base_prices(req: IsolatedRouteRequest) -> np.ndarray:
 
 class SnapshotNegotiation:
     def __init__(self, oracle, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1,
-                 threads: int = 0):
+                 threads: int = 0, groups=None):
         self.o = oracle
+        self.groups = None if groups is None else [int(g) for g in groups]
         self.req = req
         self.dims = req.grid.dims
         self.weight = int(present_weight)
@@ -117,7 +123,7 @@ class SnapshotNegotiation:
         for i, p in zip(dirty, new_paths):  # merge in net-index order
             self.paths[i] = p
             self._apply(p, +1)
-        over = self.present >= 2
+        over = self.present >= 2 if self.groups is None else self._group_overuse()
         h = self.history.astype(np.uint64) + over.astype(np.uint64) * np.uint64(self.step)
         self.history = np.minimum(h, np.uint64(COST_MAX)).astype(np.uint32)
         nxt = []
@@ -126,13 +132,28 @@ class SnapshotNegotiation:
                 nxt.append(i)
                 continue
             c, s = edge_slots(p, self.dims.w, self.dims.plane)
-            if c.size and bool((self.present[c, s] >= 2).any()):
+            if c.size and bool(over[c, s].any()):
                 nxt.append(i)
         self.dirty = nxt
         stats.update(routed=sum(1 for i in dirty if self.paths[i]), overused_edges=int(over.sum()) // 2,
                      next_dirty=len(nxt))
         self.round_no += 1
         return stats
+
+    def _group_overuse(self) -> np.ndarray:
+        """(cells, 4) flags: slots used by nets of two or more distinct groups."""
+        keys, grp = [], []
+        for i, p in enumerate(self.paths):
+            c, s = edge_slots(p or [], self.dims.w, self.dims.plane)
+            keys.append(c * 4 + s)
+            grp.append(np.full(c.size, self.groups[i], dtype=np.int64))
+        over = np.zeros(self.present.shape, dtype=bool)
+        if keys:
+            k, g = np.concatenate(keys), np.concatenate(grp)
+            pairs = np.unique(np.stack([k, g], axis=1), axis=0) if k.size else np.zeros((0, 2), np.int64)
+            uk, cnt = np.unique(pairs[:, 0], return_counts=True)
+            over.reshape(-1)[uk[cnt >= 2]] = True
+        return over
 
 
 class SnapshotShard:

@@ -22,9 +22,10 @@ def engine():
     e.close()
 
 
-def _run_both(engine, oracle, req, rounds, weight=16, step=1, check_arrays=True):
-    dev = engine.negotiation(req, present_weight=weight, history_step=step)
-    cpu = SnapshotNegotiation(oracle, req, present_weight=weight, history_step=step)
+def _run_both(engine, oracle, req, rounds, weight=16, step=1, check_arrays=True, groups=None):
+    dev = engine.negotiation(req, present_weight=weight, history_step=step, groups=groups)
+    cpu_groups = mrcuda.connection_group_ids(req.nets) if groups == "connections" else groups
+    cpu = SnapshotNegotiation(oracle, req, present_weight=weight, history_step=step, groups=cpu_groups)
     history = []
     for r in range(rounds):
         a = dev.round()
@@ -101,3 +102,40 @@ def test_medium_board_rounds(engine, oracle):
     """512x512x4, 300 nets, 4 rounds: paths, statistics and arrays."""
     wl = W.snapshot_board(seed=8, w=512, h=512, layers=4, n_nets=300, median=120)
     _run_both(engine, oracle, wl.request(), rounds=4)
+
+
+def test_connection_groups_on_a_congested_board(engine, oracle):
+    """Group-aware overuse: nets renamed into "#"-sibling groups of eight (and
+    groups by shared endpoints), every round against the oracle; then explicit
+    ids.  Same-group sharing adds no history, so the rounds differ from the
+    ungrouped ones."""
+    wl = W.snapshot_board(w=160, h=128, layers=3, n_nets=80, median=60)
+    req = wl.request()
+    nets = [NetEndpoints(f"g{i // 8}#{i % 8}", nt.src, nt.dst, nt.passable_pads, nt.via_passable_pads)
+            for i, nt in enumerate(req.nets)]
+    req = IsolatedRouteRequest(req.grid, nets, req.windows, req.x_edge_costs, req.y_edge_costs, req.via_edge_costs,
+                               req.directed_in_costs)
+    grouped = _run_both(engine, oracle, req, rounds=6, groups="connections")
+    plain = _run_both(engine, oracle, req, rounds=6)
+    assert grouped[0]["overused_edges"] < plain[0]["overused_edges"]  # same-group sharing is free
+    _run_both(engine, oracle, req, rounds=4, groups=[i % 5 for i in range(len(nets))])
+
+
+def test_connection_groups_are_checked(engine):
+    wl = W.snapshot_board(w=64, h=48, layers=2, n_nets=6, median=20)
+    req = wl.request()
+    with pytest.raises(mrcuda.InvalidArgument):
+        engine.negotiation(req, groups=[0] * 5)
+    with pytest.raises(mrcuda.InvalidArgument):
+        engine.negotiation(req, groups=[0xFFFFFFFF] * 6)
+    neg = engine.negotiation(req)
+    neg.round()
+    g = np.zeros(6, np.uint32)
+    with pytest.raises(mrcuda.InvalidArgument):  # only before the first round
+        neg.engine._check(neg.engine.lib.mrc_negotiation_set_groups(neg.engine.ctx, neg.handle, g.ctypes.data))
+    neg.close()
+    shard = engine.negotiation(req, owned=[True] * 6)
+    with pytest.raises(mrcuda.InvalidArgument):  # a shard sees only part of the paths
+        shard.engine._check(shard.engine.lib.mrc_negotiation_set_groups(shard.engine.ctx, shard.handle,
+                                                                        g.ctypes.data))
+    shard.close()

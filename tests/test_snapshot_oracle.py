@@ -76,3 +76,54 @@ def test_negotiation_spreads_nets_and_keeps_the_invariant(oracle):
     assert st.get("overused_edges", 0) < first["overused_edges"]
     # the snapshot never prices a blocked base edge
     assert (neg.snapshot[neg.base == COST_MAX] == COST_MAX).all()
+
+
+def _corridor_request(names):
+    dims = Dims(9, 5, 1)
+    cost = np.full((5, 9), COST_MAX, np.uint32)
+    cost[:, 0] = 1
+    cost[:, 8] = 1
+    cost[2, :] = 1  # corridor along y = 2
+    grid = Grid(dims, cost.reshape(-1))
+    nets = [NetEndpoints(names[0], dims.idx(0, 0), dims.idx(8, 0)),
+            NetEndpoints(names[1], dims.idx(0, 4), dims.idx(8, 4))]
+    return dims, IsolatedRouteRequest(grid, nets, [IsolatedRouteWindow.full(dims)] * 2, [10] * 8, [10] * 4, [])
+
+
+def test_connection_groups_follow_the_reference_rule():
+    """The reference's grouping (negotiated.rs:929-989, pinned by its test
+    route_exports_aligned_group_ids): '#'-siblings share a group, a foreign
+    net is its own; nets that share an endpoint cell are one group too; ids are
+    dense in order of first appearance."""
+    from mrcuda import connection_group_ids, group_of
+
+    assert group_of("g#0") == "g" and group_of("plain") == "plain" and group_of("a#b#c") == "a"
+    nets = [NetEndpoints("g#0", 0, 7), NetEndpoints("g#1", 16, 23), NetEndpoints("foreign", 40, 47)]
+    assert connection_group_ids(nets) == [0, 0, 1]
+    nets = [NetEndpoints("a", 0, 5), NetEndpoints("b", 5, 9), NetEndpoints("c", 10, 11), NetEndpoints("d#x", 12, 13),
+            NetEndpoints("d#y", 14, 15), NetEndpoints("e", 11, 20), NetEndpoints("f", 30, 30)]
+    assert connection_group_ids(nets) == [0, 0, 1, 2, 2, 1, 3]
+    assert connection_group_ids([]) == []
+
+
+def test_same_group_nets_share_a_corridor_without_overuse(oracle):
+    """Two nets of one connection group through a one-cell corridor: the edges
+    are not overused, so no history accrues and no net is dirty after round 0
+    (prices still count both nets, as in route_negotiated).  Nets of two groups
+    on the same board overuse all 8 corridor edges every round."""
+    dims, req = _corridor_request(["n#0", "n#1"])
+    neg = SnapshotNegotiation(oracle, req, history_step=3, groups=[0, 0])
+    st = neg.round()
+    assert st["routed"] == 2 and st["overused_edges"] == 0 and st["next_dirty"] == 0
+    assert (neg.history == 0).all()
+    assert (neg.present[[dims.idx(x, 2) for x in range(1, 9)], 1] == 2).all()
+    _, req2 = _corridor_request(["a", "b"])
+    neg2 = SnapshotNegotiation(oracle, req2, history_step=3, groups=[0, 1])
+    for r in range(3):
+        st = neg2.round()
+        assert st["overused_edges"] == 8 and st["next_dirty"] == 2
+    # every net its own group is the default test (count >= 2)
+    neg3 = SnapshotNegotiation(oracle, req2, history_step=3)
+    for r in range(3):
+        neg3.round()
+    np.testing.assert_array_equal(neg3.history, neg2.history)
