@@ -905,9 +905,11 @@ __global__ void async_seed_kernel(RelaxArgs a) {
 // Label of a window cell after the relax launch (unvisited tiles are unreached).
 __device__ __forceinline__ u64 field_label(const PathArgs &a, const DevField &f, uint32_t lx, uint32_t ly,
                                            uint32_t l) {
-    const uint32_t ntx = (f.ww + kTW - 1) / kTW;
-    const uint32_t t = (ly / a.tile_h) * ntx + lx / kTW;
-    if (!a.arena_filled && !a.tvisit[f.tile_off + t]) return kInf;
+    if (!a.arena_filled) {
+        const uint32_t ntx = (f.ww + kTW - 1) / kTW;
+        const uint32_t t = (ly >> (__ffs((int)a.tile_h) - 1)) * ntx + lx / kTW;  // tile heights are powers of two
+        if (!a.tvisit[f.tile_off + t]) return kInf;
+    }
     return a.lab[f.lab_off + ((uint64_t)l * f.wh + ly) * f.ww + lx];
 }
 
@@ -1159,10 +1161,10 @@ __global__ void emit_fields_kernel(PathArgs a, uint32_t *out, uint64_t total) {
             else hi = mid;
         }
         const DevField f = a.fields[lo];
-        const uint64_t li = i - f.lab_off;
-        const uint32_t lx = (uint32_t)(li % f.ww);
-        const uint64_t rr = li / f.ww;
-        const uint32_t ly = (uint32_t)(rr % f.wh), l = (uint32_t)(rr / f.wh);
+        // a window has at most 2^32 cells (the CellIdx domain): 32-bit index math
+        const uint32_t li = (uint32_t)(i - f.lab_off);
+        const uint32_t rr = li / f.ww, lx = li - rr * f.ww;
+        const uint32_t l = rr / f.wh, ly = rr - l * f.wh;
         out[i] = (uint32_t)(field_label(a, f, lx, ly, l) >> 32);
     }
 }
