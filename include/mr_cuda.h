@@ -221,9 +221,17 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
 mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t tile_h, uint32_t threads);
 /* The relax schedule: 0 = bulk-synchronous rounds over a shared tile list
  * (cooperative launch, grid barrier between rounds); 1 = one asynchronous
- * work queue (no rounds; a tile held by one CTA at a time).  Both give the
- * same labels and paths.  The autotuner tries both. */
+ * work queue (no rounds; a tile held by one CTA at a time); 2 = the same queue
+ * with one warp per tile (tiles of 4 S x 8 cells over every layer, S = 32 /
+ * next_pow2(layers), labels held in registers; boards of at most 16 layers,
+ * else MRC_ERR_LIMIT).  All give the same labels and paths.  The autotuner
+ * tries every one.  These replace the per-round dispatch loop of
+ * crates/mr-metal/src/gpu.rs:1630-2039. */
 mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule);
+/* Schedule of batches built on this context while it holds no autotuned
+ * configuration for their layer count and price form: 1 (the default) or 2
+ * (see mrc_batch_set_schedule); batches with more than 16 layers keep 1. */
+mrc_status mrc_context_set_schedule(mrc_context *ctx, uint32_t schedule);
 /* The batch's current tile height, CTA width and schedule. */
 mrc_status mrc_batch_config(const mrc_batch *batch, uint32_t *tile_h, uint32_t *threads, uint32_t *schedule);
 /* Kernels launched by the last mrc_batch_launch (for launch accounting). */
@@ -233,7 +241,8 @@ uint32_t mrc_batch_kernel_launches(const mrc_batch *batch);
  * call after the stream has been synchronised).  Negative when unavailable. */
 float mrc_batch_relax_ms(const mrc_batch *batch);
 /* Work counters of the last launch (after the stream has been synchronised):
- * out[0] = tile activations, out[1] = in-tile sweeps, out[2] = rounds,
+ * out[0] = tile activations, out[1] = in-tile sweeps (passes of the warp
+ * schedule), out[2] = rounds (tile rows relaxed, warp schedule),
  * out[3] = tiles in the batch.  Returns MRC_ERR_BACKEND_UNAVAILABLE if the
  * counters cannot be read. */
 mrc_status mrc_batch_stats(const mrc_batch *batch, uint64_t out[4]);
@@ -280,11 +289,12 @@ mrc_status mrc_route_isolated_plain(mrc_context *ctx, const mrc_isolated_request
  * - A request whose scratch would exceed MRC_NOALLOC_SCRATCH_BYTES (8 B per
  *   window cell for labels plus 4 B per window cell for paths, the board copy,
  *   and per-tile state) fails with MRC_ERR_LIMIT and does no device work.
- * - All calls share the one array and find the previous call's contents in it;
- *   the entry point clears what must start at zero.  Calls serialise on a
- *   process-wide lock and each returns only after its device work finished;
- *   device work that overlaps a call from elsewhere on the same GPU (e.g. a
- *   second process of this library sharing the context) would race.
+ * - The array is per process and per device, and all calls in a process share
+ *   it and find the previous call's contents in it; the entry point clears what
+ *   must start at zero.  Calls serialise on a process-wide lock, and every call
+ *   (an error return included) waits for its own device work before it returns.
+ *   Calls that overlapped on the GPU would race on the array; the lock and the
+ *   wait are what keep them from overlapping.
  * - path_offsets[n+1] and search_costs[n] are always written on success; when
  *   the paths need more than path_cells_capacity cells the call returns
  *   MRC_ERR_LIMIT with the offsets filled so the caller can size the buffer. */

@@ -47,6 +47,7 @@ struct DevBoard {
     const uint32_t *y_edge;     // h-1
     const uint32_t *via_edge;   // layers-1
     const uint4 *directed;      // nullable: in-prices from -y, -x, +x, +y
+    uint32_t *planes;           // nullable: 6 x cells step prices (warp schedule; written by planes_kernel)
 };
 
 // One field = one net solved inside one window.
@@ -71,6 +72,7 @@ struct Ctl {
     uint32_t rounds;
     unsigned long long activations;
     unsigned long long sweeps;
+    unsigned long long rows;    // tile rows relaxed (warp schedule)
 };
 
 __device__ __forceinline__ uint32_t capmul(uint32_t e, uint32_t w) {

@@ -196,6 +196,7 @@ struct mrc_context {
     // autotuned relax configuration per (layers, directed): tile height, CTA
     // width, schedule (0 = bulk-synchronous rounds, 1 = asynchronous queue)
     std::map<uint32_t, std::array<uint32_t, 3>> tuned;
+    uint32_t default_schedule = 1;  // for batches without a tuned configuration
     // board bytes moved to HBM since creation: through the pinned stage or a
     // pageable copy, and straight from the caller's page-locked arrays
     uint64_t staged_bytes = 0, in_place_bytes = 0;
@@ -703,7 +704,11 @@ struct mrc_batch {
     // has the same per-CTA footprint) and a divisor of the co-resident grid.
     uint32_t force_tile_h = 0, force_threads = 0, grid_num = 1, grid_div = 1;
     bool async_q = false;  // relax schedule: asynchronous work queue instead of rounds
+    bool warp = false;     // the warp-per-tile schedule (implies the queue and a +inf-filled arena)
     size_t smem_floor = 0;
+    std::vector<DevBoard> devs;  // the board table (step-price plane pointers patched in by batch_layout)
+    DBuf d_planes, d_pchunks;    // warp schedule: step-price planes of every board, chunk table of their kernel
+    uint64_t n_pchunks = 0;
     ~mrc_batch() {
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
@@ -741,13 +746,16 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
         cudaGraphExecDestroy(bt->graph);
         bt->graph = nullptr;
     }
-    bt->tile_h = tile_h;
-    bt->threads = threads;
-    bt->smem = std::max(relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any), bt->smem_floor);
+    if (bt->warp && bt->max_layers > kWarpMaxLayers) bt->warp = false;  // too many layers for one warp tile
+    if (bt->warp) bt->async_q = true;
+    bt->tile_h = bt->warp ? kWarpTileH : tile_h;
+    bt->threads = bt->warp ? warp_relax_threads() : threads;
+    bt->smem = bt->warp ? 0 : std::max(relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any), bt->smem_floor);
     uint64_t toff = 0;
     uint32_t max_tiles = 1;
     for (DevField &f : bt->fields) {
-        const uint64_t tiles = (uint64_t)((f.ww + 31) / 32) * ((f.wh + tile_h - 1) / tile_h);
+        const uint32_t tw = bt->warp ? warp_tile_w(bt->boards[f.board]->view.layers) : 32u;
+        const uint64_t tiles = (uint64_t)((f.ww + tw - 1) / tw) * ((f.wh + bt->tile_h - 1) / bt->tile_h);
         f.tile_off = (uint32_t)std::min<uint64_t>(toff, 0xFFFFFFFFull);
         toff += tiles;
         max_tiles = (uint32_t)std::max<uint64_t>(max_tiles, tiles);
@@ -756,12 +764,38 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     bt->total_tiles = (uint32_t)std::max<uint64_t>(toff, 1);
     bt->max_tiles = max_tiles;
     int per_sm = 1;
-    MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q), "configure relax kernel");
-    MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q), "relax occupancy");
+    if (bt->warp) {
+        MRC_CUDA(warp_relax_occupancy(&per_sm), "relax occupancy");
+    } else {
+        MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q), "configure relax kernel");
+        MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q), "relax occupancy");
+    }
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
     bt->grid = std::max<uint32_t>(
         1u, (uint32_t)((uint64_t)ctx->sms * (uint32_t)per_sm * bt->grid_num / std::max(1u, bt->grid_div)));
+    // board table, with the step-price planes of every board for the warp schedule
+    if (bt->warp) {
+        std::vector<uint64_t> poff(bt->devs.size()), chunks(bt->devs.size() + 1, 0);
+        uint64_t total = 0;
+        for (size_t k = 0; k < bt->devs.size(); ++k) {
+            const DevBoard &d = bt->devs[k];
+            const uint64_t cells = (uint64_t)d.w * d.h * d.layers;
+            poff[k] = total;
+            total += (cells * 6 * 4 + 255) & ~(uint64_t)255;
+            chunks[k + 1] = chunks[k] + planes_chunks(cells);
+        }
+        MRC_TRY(bt->d_planes.get(ctx, std::max<uint64_t>(total, 256), "step-price planes"));
+        for (size_t k = 0; k < bt->devs.size(); ++k)
+            bt->devs[k].planes = reinterpret_cast<uint32_t *>(bt->d_planes.as<unsigned char>() + poff[k]);
+        bt->n_pchunks = chunks.back();
+        MRC_TRY(upload(ctx, bt->d_pchunks, chunks.data(), chunks.size() * 8, "plane chunk table"));
+    } else {
+        for (DevBoard &d : bt->devs) d.planes = nullptr;
+        bt->d_planes.reset();
+        bt->n_pchunks = 0;
+    }
+    MRC_TRY(upload(ctx, bt->d_boards, bt->devs.data(), bt->devs.size() * sizeof(DevBoard), "upload board table"));
     MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
     MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
     MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
@@ -793,9 +827,11 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         tile_h = tuned->second[0];
         threads = tuned->second[1];
         bt->async_q = tuned->second[2] != 0;
+        bt->warp = tuned->second[2] == 2;
     } else {
         MRC_TRY(choose_tile(ctx, bt->max_layers, bt->directed_any, &tile_h, &smem));
         bt->async_q = true;
+        bt->warp = ctx->default_schedule == 2;
     }
     // largest windows first: the persistent CTAs then finish together
     std::vector<uint32_t> order(n);
@@ -834,10 +870,9 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         if (pads.size() > 0xFFFFFFF0u) return fail(MRC_ERR_LIMIT, "pad lists exceed 2^32 entries");
     }
     bt->total_cells = off;
-    std::vector<DevBoard> devs;
-    devs.reserve(bt->boards.size());
-    for (const mrc_board *b : bt->boards) devs.push_back(b->dev);
-    MRC_TRY(upload(ctx, bt->d_boards, devs.data(), devs.size() * sizeof(DevBoard), "upload board table"));
+    bt->devs.clear();
+    bt->devs.reserve(bt->boards.size());
+    for (const mrc_board *b : bt->boards) bt->devs.push_back(b->dev);
     MRC_TRY(batch_layout(bt, tile_h, threads));
     MRC_TRY(upload(ctx, bt->d_pads, pads.data(), pads.size() * 4, "upload pads"));
     MRC_TRY(bt->d_lab.get(ctx, std::max<uint64_t>(off, 1) * 8, "labels"));
@@ -904,9 +939,17 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
     if (n) {
         const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
         if (bt->ev0) MRC_CUDA(cudaEventRecordWithFlags(bt->ev0, st, rec), "record event");
-        MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q), "launch relax kernel");
+        if (bt->warp) {
+            MRC_CUDA(planes_launch(bt->d_boards.as<DevBoard>(), bt->d_pchunks.as<uint64_t>(),
+                                   (uint32_t)bt->devs.size(), bt->n_pchunks, (uint32_t)bt->ctx->sms, st),
+                     "launch step-price planes");
+            MRC_CUDA(warp_relax_launch(ra, bt->grid, st), "launch relax kernel");
+            launches += 3;  // planes, seeds, relax
+        } else {
+            MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q), "launch relax kernel");
+            launches += bt->async_q ? 2 : 1;  // (+ the seed kernel)
+        }
         if (bt->ev1) MRC_CUDA(cudaEventRecordWithFlags(bt->ev1, st, rec), "record event");
-        launches += bt->async_q ? 2 : 1;  // (+ the seed kernel)
     }
     const PathArgs pa = path_args(bt);
     MRC_CUDA(path_launch(pa, st), "launch path kernels");
@@ -1443,15 +1486,24 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     MRC_CUDA(cudaEventCreate(&e1), "create event");
     float best = -1.0f;
     uint32_t best_th = batch->tile_h, best_nt = batch->threads;
-    bool best_async = batch->async_q;
+    uint32_t best_sched = batch->warp ? 2u : batch->async_q ? 1u : 0u;
     mrc_status rc = MRC_OK;
+    // candidates: (tile height, CTA width, schedule); the warp schedule has one shape
+    std::vector<std::array<uint32_t, 3>> cands;
+    if (layers <= kWarpMaxLayers) cands.push_back({kWarpTileH, warp_relax_threads(), 2u});
     for (uint32_t th : {8u, 16u, 32u, 64u}) {
         if (relax_smem_bytes(layers, th, batch->directed_any) > hard) continue;
         for (uint32_t cfg = 0; cfg < 4; ++cfg) {
             const uint32_t nt = cfg & 1 ? 256u : 128u;
-            const bool async = (cfg & 2) != 0;
             if (4u * layers * th < nt / 2) continue;  // most lanes would idle in the line passes
-            batch->async_q = async;
+            cands.push_back({th, nt, (cfg & 2) ? 1u : 0u});
+        }
+    }
+    for (const auto &cand : cands) {
+        {
+            const uint32_t th = cand[0], nt = cand[1], sched = cand[2];
+            batch->async_q = sched != 0;
+            batch->warp = sched == 2;
             rc = batch_layout(batch, th, nt);
             if (rc != MRC_OK) break;
             float ms = 0.0f, sum = 0.0f;
@@ -1469,7 +1521,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
                 best = sum;
                 best_th = th;
                 best_nt = nt;
-                best_async = async;
+                best_sched = sched;
             }
         }
         if (rc != MRC_OK) break;
@@ -1477,9 +1529,10 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != MRC_OK) return rc;
-    batch->async_q = best_async;
+    batch->async_q = best_sched != 0;
+    batch->warp = best_sched == 2;
     MRC_TRY(batch_layout(batch, best_th, best_nt));
-    ctx->tuned[tune_key(layers, batch->directed_any)] = {best_th, best_nt, best_async ? 1u : 0u};
+    ctx->tuned[tune_key(layers, batch->directed_any)] = {best_th, best_nt, best_sched};
     if (tile_h) *tile_h = best_th;
     if (threads) *threads = best_nt;
     if (best_ms) *best_ms = best;
@@ -1500,18 +1553,31 @@ mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t til
 
 mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule) {
     if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (schedule > 1) return fail(MRC_ERR_INVALID_ARGUMENT, "schedule must be 0 (rounds) or 1 (queue)");
+    if (schedule > 2) return fail(MRC_ERR_INVALID_ARGUMENT, "schedule must be 0 (rounds), 1 (queue) or 2 (warp tiles)");
+    if (schedule == 2 && batch->max_layers > kWarpMaxLayers)
+        return fail(MRC_ERR_LIMIT, "the warp schedule takes boards of at most 16 layers");
     Lock lock(ctx, 0);
     MRC_TRY(set_device(ctx));
-    batch->async_q = schedule == 1;
-    return batch_layout(batch, batch->tile_h, batch->threads);
+    const bool was_warp = batch->warp;
+    batch->async_q = schedule >= 1;
+    batch->warp = schedule == 2;
+    // leaving the warp schedule: the default CTA tile (8 rows, 256 threads)
+    return batch_layout(batch, was_warp ? 8u : batch->tile_h, was_warp ? 256u : batch->threads);
+}
+
+mrc_status mrc_context_set_schedule(mrc_context *ctx, uint32_t schedule) {
+    if (!ctx) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (schedule != 1 && schedule != 2) return fail(MRC_ERR_INVALID_ARGUMENT, "default schedule must be 1 or 2");
+    Lock lock(ctx, 0);
+    ctx->default_schedule = schedule;
+    return MRC_OK;
 }
 
 mrc_status mrc_batch_config(const mrc_batch *batch, uint32_t *tile_h, uint32_t *threads, uint32_t *schedule) {
     if (!batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
     if (tile_h) *tile_h = batch->tile_h;
     if (threads) *threads = batch->threads;
-    if (schedule) *schedule = batch->async_q ? 1u : 0u;
+    if (schedule) *schedule = batch->warp ? 2u : batch->async_q ? 1u : 0u;
     return MRC_OK;
 }
 
@@ -1525,7 +1591,7 @@ mrc_status mrc_batch_stats(const mrc_batch *batch, uint64_t out[4]) {
     if (batch->d_ctl.p) MRC_CUDA(cudaMemcpy(&c, batch->d_ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost), "read counters");
     out[0] = c.activations;
     out[1] = c.sweeps;
-    out[2] = c.rounds;
+    out[2] = batch->warp ? c.rows : c.rounds;
     out[3] = batch->total_tiles;
     return MRC_OK;
 }
@@ -2754,6 +2820,14 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
                                    "entry point has MRC_NOALLOC_SCRATCH_BYTES = " +
                                        std::to_string((size_t)MRC_NOALLOC_SCRATCH_BYTES) + " bytes");
     unsigned char *s = dev->scratch;
+    // From the first enqueued copy on, every return (an error included) waits
+    // for the stream before the lock is released, so no device work of this
+    // call can still read or write the array when the next call starts.
+    // Declared after the lock, so it runs first.
+    struct DrainOnExit {
+        cudaStream_t st;
+        ~DrainOnExit() { cudaStreamSynchronize(st); }
+    } drain{st};
 
     // inputs into the scratch array
     MRC_CUDA(cudaMemcpyAsync(s + o_fields, fields.data(), n * sizeof(DevField), cudaMemcpyHostToDevice, st), "upload fields");
@@ -2784,7 +2858,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     MRC_CUDA(cudaMemsetAsync(s + o_tstamp, 0, tiles * 4, st), "clear tile stamps");
     MRC_CUDA(cudaMemsetAsync(s + o_tvisit, 0, tiles * 4, st), "clear tile flags");
 
-    DevBoard b;
+    DevBoard b{};
     b.w = g.w;
     b.h = g.h;
     b.layers = g.layers;

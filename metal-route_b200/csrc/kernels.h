@@ -117,6 +117,27 @@ cudaError_t overuse_launch(const OveruseArgs &a, cudaStream_t st);
 cudaError_t dirty_launch(const DirtyArgs &a, cudaStream_t st);
 cudaError_t group_overuse_launch(const GroupArgs &a, cudaStream_t st);
 
+// Warp schedule (warp_relax.cu): one warp per tile of (4 S) x 8 cells over all
+// layers, S = 32 / next_pow2(layers) segments per row; boards of up to 16 layers.
+constexpr uint32_t kWarpLaneCells = 4;
+constexpr uint32_t kWarpTileH = 8;
+constexpr uint32_t kWarpMaxLayers = 16;
+__host__ __device__ inline uint32_t warp_segments(uint32_t layers) {
+    uint32_t lp = 1;
+    while (lp < layers) lp <<= 1;
+    return 32u / lp;
+}
+__host__ __device__ inline uint32_t warp_tile_w(uint32_t layers) { return kWarpLaneCells * warp_segments(layers); }
+uint32_t warp_relax_threads();
+cudaError_t warp_relax_occupancy(int *blocks_per_sm);
+// seeds, then the persistent warp kernel (label arena +inf-filled, queue tags zeroed, as for the queue form)
+cudaError_t warp_relax_launch(const RelaxArgs &a, uint32_t grid, cudaStream_t st);
+// Step-price planes of every board of a batch (DevBoard::planes, 6 x cells u32
+// each); chunk_start[k] = first chunk of board k (prefix sum of planes_chunks).
+uint64_t planes_chunks(uint64_t cells);
+cudaError_t planes_launch(const DevBoard *boards, const uint64_t *chunk_start, uint32_t n_boards, uint64_t n_chunks,
+                          uint32_t sms, cudaStream_t st);
+
 // Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
 size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);
 // The relax kernel is instantiated for threads in {128, 256} per CTA.

@@ -29,6 +29,7 @@
 
 #include "device.cuh"
 #include "kernels.h"
+#include "tiles.cuh"
 
 namespace mrc {
 
@@ -54,25 +55,6 @@ __device__ __forceinline__ void cp_async4(uint32_t *smem, const uint32_t *gmem) 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Label extended by a run of `h` steps whose prices sum to `d` (kMax = blocked or
-// saturated); a dist reaching 0xFFFFFFFF is unreachable.  With 32-bit wrapping
-// addition, td or d equal to kMax always gives nd < td or nd == kMax, so those
-// two tests cover the blocked operands too.
-__device__ __forceinline__ u64 ext2(u64 t, uint32_t d, uint32_t h) {
-    const uint32_t td = (uint32_t)(t >> 32);
-    const uint32_t nd = td + d;
-    const bool bad = (nd < td) | (nd == kMax);
-    return bad ? kInf : (((u64)nd << 32) | (uint32_t)((uint32_t)t + h));
-}
-
-// Saturating sum of step prices; kMax absorbs (an operand equal to kMax gives
-// s == kMax or s < a under wrapping addition).
-__device__ __forceinline__ uint32_t dsum(uint32_t a, uint32_t b) {
-    const uint32_t s = a + b;
-    return s < a ? kMax : s;
-}
-
-__device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
 
 // Step-price planes of a staged tile: the move into cell c from its neighbour
 // at -x, +x, -y, +y, the layer below and the layer above.
@@ -408,76 +390,6 @@ __device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
         }
     }
     return ch;
-}
-
-// Work queue of the asynchronous form.  count[0] = tickets handed to pushers
-// (tail), head[0] = tickets handed to poppers, count[1] = items queued or in
-// flight.  lists[0, cap) holds the items, lists[cap, 2 cap) their ticket tags
-// (ticket + 1, zeroed before launch).  A tile is queued at most once at a time
-// (its tstamp word is the queued flag), so cap = total tiles never overflows.
-constexpr uint32_t kQueueSpinLimit = 1u << 26;
-
-// Tile states in the tstamp word: 0 idle, 1 queued, 2 held by a CTA,
-// 3 held and improved again meanwhile (the holder queues it once more when it
-// finishes, so improvements that arrive during a relaxation share one
-// re-activation and no tile is ever relaxed by two CTAs at once).
-constexpr uint32_t kTileIdle = 0, kTileQueued = 1, kTileHeld = 2, kTileHeldDirty = 3;
-
-__device__ __forceinline__ void async_enqueue(const RelaxArgs &a, uint32_t fi, uint32_t u) {
-    Ctl *c = a.ctl;
-    atomicAdd(&c->count[1], 1u);  // in flight before it is visible
-    const uint32_t h = atomicAdd(&c->count[0], 1u);
-    const size_t slot = h % a.list_cap;
-    a.lists[slot] = ((u64)fi << 32) | u;
-    __threadfence();
-    atomicExch(a.lists + a.list_cap + slot, (u64)h + 1u);
-}
-
-__device__ __forceinline__ void async_push(const RelaxArgs &a, uint32_t fi, uint32_t tile_off, uint32_t u) {
-    uint32_t *st = a.tstamp + tile_off + u;
-    for (int tries = 0; tries < 1024; ++tries) {
-        const uint32_t old = atomicCAS(st, kTileIdle, kTileQueued);
-        if (old == kTileIdle) {
-            async_enqueue(a, fi, u);
-            return;
-        }
-        if (old == kTileQueued || old == kTileHeldDirty) return;  // it will read our labels
-        if (atomicCAS(st, kTileHeld, kTileHeldDirty) == kTileHeld) return;
-        // the holder finished in between: try again from idle
-    }
-    atomicOr(&a.ctl->status, kStatusQueueOverflow);  // the state kept changing under us
-}
-
-// Called by the holder after its write-back and pushes: release the tile, or
-// queue it again if a neighbour improved it while it was held.
-__device__ __forceinline__ void async_release(const RelaxArgs &a, uint32_t fi, uint32_t tile_off, uint32_t t) {
-    uint32_t *st = a.tstamp + tile_off + t;
-    if (atomicCAS(st, kTileHeld, kTileIdle) == kTileHeldDirty) {
-        atomicExch(st, kTileQueued);
-        async_enqueue(a, fi, t);
-    }
-}
-
-// Next item for the calling CTA (thread 0), or kInf when no work is left.  The
-// wait is bounded: kQueueSpinLimit polls, then kStatusBarrier and an exit.
-__device__ __forceinline__ u64 async_pop(const RelaxArgs &a) {
-    Ctl *c = a.ctl;
-    const uint32_t h = atomicAdd(&c->head[0], 1u);
-    const size_t slot = h % a.list_cap;
-    const volatile u64 *tag = a.lists + a.list_cap + slot;
-    for (uint32_t spins = 0;; ++spins) {
-        if (*tag == (u64)h + 1u) {
-            __threadfence();
-            return __ldcg(a.lists + slot);
-        }
-        if (*(volatile const uint32_t *)&c->count[1] == 0u) return kInf;  // nothing queued or running
-        if (*(volatile const uint32_t *)&c->status) return kInf;
-        if (spins > kQueueSpinLimit) {
-            atomicOr(&c->status, kStatusBarrier);
-            return kInf;
-        }
-        __nanosleep(spins < 32 ? 32 : 256);
-    }
 }
 
 // One (field, tile) item: stage the tile and its halo, relax it to local

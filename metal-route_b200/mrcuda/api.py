@@ -182,6 +182,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
                                              C.POINTER(C.c_float)]),
             "mrc_batch_destroy": (None, [vp]),
             "mrc_batch_set_schedule": (C.c_int, [vp, vp, C.c_uint32]),
+            "mrc_context_set_schedule": (C.c_int, [vp, C.c_uint32]),
             "mrc_batch_config": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                            C.POINTER(C.c_uint32)]),
             "mrc_net_windows": (C.c_int, [u32, u32, u32, vp, u32, vp]),
@@ -504,7 +505,8 @@ class Batch:
         e._check(e.lib.mrc_batch_set_config(e.ctx, self.handle, int(tile_h), int(threads)))
 
     def set_schedule(self, schedule: int) -> None:
-        """0 = bulk-synchronous rounds, 1 = asynchronous work queue."""
+        """0 = bulk-synchronous rounds, 1 = asynchronous work queue (a CTA per
+        tile), 2 = the queue with a warp per tile."""
         e = self.engine
         e._check(e.lib.mrc_batch_set_schedule(e.ctx, self.handle, int(schedule)))
 
@@ -522,11 +524,15 @@ class Batch:
         return dict(self.config(), ms=float(ms.value))
 
     def stats(self) -> dict:
-        """Work counters of the last launch: tile activations, in-tile sweeps,
-        rounds and the batch's tile count."""
+        """Work counters of the last launch: tile activations, in-tile sweeps
+        (passes), rounds (tile rows relaxed, warp schedule) and the batch's
+        tile count."""
         out = (C.c_uint64 * 4)()
         self.engine._check(self.engine.lib.mrc_batch_stats(self.handle, out))
-        return {"activations": int(out[0]), "sweeps": int(out[1]), "rounds": int(out[2]), "tiles": int(out[3])}
+        d = {"activations": int(out[0]), "sweeps": int(out[1]), "rounds": int(out[2]), "tiles": int(out[3])}
+        if self.config()["schedule"] == 2:
+            d["rows"] = d.pop("rounds")
+        return d
 
     def relax_ms(self) -> float:
         """Device time of the relax kernel in the last launch (needs time_kernels)."""
@@ -776,6 +782,11 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+    def set_schedule(self, schedule: int) -> None:
+        """Relax schedule of batches this engine builds without an autotuned
+        configuration: 1 = a CTA per tile (the default), 2 = a warp per tile."""
+        self._check(self.lib.mrc_context_set_schedule(self.ctx, int(schedule)))
 
     def _check(self, status: int) -> None:
         if status != MRC_OK:

@@ -18,8 +18,8 @@ INCLUDE = os.path.join(REPO, "include")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libmr_cuda.so")
 
-SOURCES = ["relax.cu", "negotiate.cu", "engine.cu"]
-HEADERS = ["device.cuh", "kernels.h"]
+SOURCES = ["relax.cu", "warp_relax.cu", "negotiate.cu", "engine.cu"]
+HEADERS = ["device.cuh", "kernels.h", "tiles.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I" + INCLUDE, "-I" + CSRC]
 

@@ -15,9 +15,11 @@ from snapshot_oracle import SnapshotNegotiation
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def engine():
+@pytest.fixture(scope="module", params=[1, 2], ids=["cta-tiles", "warp-tiles"])
+def engine(request):
+    """Every test runs on both default schedules: a CTA per tile and a warp per tile."""
     e = mrcuda.Engine(0)
+    e.set_schedule(request.param)
     yield e
     e.close()
 

@@ -18,9 +18,11 @@ pytestmark = pytest.mark.gpu
 CASES = load_golden()
 
 
-@pytest.fixture(scope="module")
-def engine():
+@pytest.fixture(scope="module", params=[1, 2], ids=["cta-tiles", "warp-tiles"])
+def engine(request):
+    """Every test runs on both default schedules: a CTA per tile and a warp per tile."""
     e = mrcuda.Engine(0)
+    e.set_schedule(request.param)
     yield e
     e.close()
 
@@ -97,9 +99,9 @@ def test_golden_distance_fields(engine, oracle, case):
         np.testing.assert_array_equal(got[k], exp, err_msg=f"source {s}")
 
 
-def _random_case(rng, trial, directed=False, max_side=40, max_layers=4):
+def _random_case(rng, trial, directed=False, max_side=40, max_layers=4, min_layers=1):
     w, h = int(rng.integers(1, max_side)), int(rng.integers(1, max_side))
-    layers = int(rng.integers(1, max_layers + 1))
+    layers = int(rng.integers(min_layers, max_layers + 1))
     dims = Dims(w, h, layers)
     n = len(dims)
     cost = rng.integers(0, 9, n).astype(np.uint32)
@@ -223,14 +225,23 @@ def test_deterministic_across_calls_and_batches(engine):
         batch.launch()
         c = batch.finish()
         assert c.paths == a.paths and c.search_costs == a.search_costs
-    # relax (+ the seed kernel of the queue schedule), path offsets, path walk
+    # relax (+ the seed kernel of the queue schedules, + the price planes of the
+    # warp schedule), path offsets, path walk
     assert batch.kernel_launches == 3 + batch.config()["schedule"]
-    # every tile height / CTA width the autotuner tries computes the same answer
-    tuned = batch.autotune()
+    # every configuration the autotuner tries computes the same answer (on a
+    # context of its own, so the tuned choice does not steer the other tests)
+    e2 = mrcuda.Engine(0)
+    board2 = e2.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
+    batch2 = mrcuda.Batch(board2, wl.nets, wl.windows)
+    tuned = batch2.autotune()
+    assert tuned["schedule"] in (0, 1, 2)
     assert tuned["tile_h"] in (8, 16, 32, 64) and tuned["threads"] in (128, 256)
-    batch.launch()
-    c = batch.finish()
+    batch2.launch()
+    c = batch2.finish()
     assert c.paths == a.paths and c.search_costs == a.search_costs
+    batch2.close()
+    board2.close()
+    e2.close()
 
 
 def test_edge_cases_and_errors(engine):
@@ -311,5 +322,62 @@ def test_queue_schedule_on_the_congestion_board(engine, oracle, tile_cfg):
         assert got.paths == exp[0] and got.search_costs == exp[1]
     _assert_fields(oracle, req, got, nets_idx={0, 7, 128, 255})
     assert batch.config()["schedule"] == 1
+    batch.close()
+    board.close()
+
+
+@pytest.mark.parametrize("layers", [1, 2, 3, 4, 5, 6, 8, 9, 12, 16])
+def test_warp_schedule_every_tile_geometry(engine, oracle, layers):
+    """The warp schedule's tile width follows the layer count (4 * 32 /
+    next_pow2(layers) cells): seeded adversarial boards of every geometry,
+    ragged windows included, against the oracle's complete fields."""
+    rng = np.random.default_rng(700 + layers)
+    for trial in range(4):
+        req = _random_case(rng, trial, directed=trial % 2 == 1, max_side=70, max_layers=layers,
+                           min_layers=layers)
+        if req is None:
+            continue
+        exp = oracle.isolated_batch(req, retry_full=False, mode="field")
+        board = engine.board(req.grid, req.x_edge_costs, req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
+        batch = mrcuda.Batch(board, req.nets, req.windows, retry_full=False, keep_fields=True)
+        batch.set_schedule(2)
+        batch.launch()
+        got = batch.finish()
+        assert (got.paths, got.search_costs) == exp, (layers, trial)
+        _assert_fields(oracle, req, got)
+        st = batch.stats()
+        assert st["activations"] >= 1 or not any(p is not None for p in got.paths)
+        batch.close()
+        board.close()
+
+
+def test_warp_schedule_refuses_more_than_16_layers(engine):
+    dims = Dims(20, 10, 17)
+    grid = Grid.filled(dims, 1)
+    board = engine.board(grid, [1] * 19, [1] * 9, [3] * 16)
+    batch = mrcuda.Batch(board, [NetEndpoints("a", 0, len(dims) - 1)], [IsolatedRouteWindow.full(dims)])
+    with pytest.raises(mrcuda.LimitExceeded):
+        batch.set_schedule(2)
+    batch.close()
+    board.close()
+
+
+def test_warp_schedule_on_the_congestion_board(engine, oracle):
+    """All 256 nets of the congestion board on the warp schedule, three
+    launches in a row, plus complete fields of a sample of nets."""
+    wl = W.congestion_board()
+    req = wl.request()
+    exp = oracle.isolated_batch(req, mode="astar")
+    board = engine.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
+    batch = mrcuda.Batch(board, wl.nets, wl.windows, keep_fields=True)
+    batch.set_schedule(2)
+    assert batch.config()["schedule"] == 2
+    for _ in range(3):
+        batch.launch()
+        got = batch.finish()
+        assert got.paths == exp[0] and got.search_costs == exp[1]
+    _assert_fields(oracle, req, got, nets_idx={0, 7, 128, 255})
+    st = batch.stats()
+    assert st["activations"] >= st["tiles"] // 4 and st["rows"] > 0
     batch.close()
     board.close()

@@ -2,7 +2,8 @@
 
 Each request's result must be the same bit for bit whether it is solved alone
 (mrc_route_isolated_batch) or merged with others into shared launches, with
-several launches in flight, under a tight memory budget, or one at a time.
+several launches in flight, under a tight memory budget, or one at a time, and
+equal the CPU oracle's answer for the same request.
 """
 import threading
 
@@ -71,14 +72,26 @@ def _submit_all(srv, reqs, threads=4, keep=False):
     return [srv.wait(t) for t in tickets]
 
 
+_ORACLE_CACHE = {}
+
+
+def _oracle_results(oracle, reqs, key):
+    """The oracle's (paths, costs) per request, with the full-board retry."""
+    if key not in _ORACLE_CACHE:
+        _ORACLE_CACHE[key] = [oracle.isolated_batch(r, retry_full=True, mode="field") for r in reqs]
+    return _ORACLE_CACHE[key]
+
+
 @pytest.mark.parametrize("slots,max_batch", [(2, 64), (3, 5), (1, 1)])
-def test_same_result_alone_and_in_the_mix(engine, slots, max_batch):
+def test_same_result_alone_and_in_the_mix(engine, oracle, slots, max_batch):
     reqs = _mixed_requests()
+    exp = _oracle_results(oracle, reqs, "mixed-24-31")
     alone = _alone(engine, reqs)
     srv = engine.server(slots=slots, max_batch_requests=max_batch)
     got = _submit_all(srv, reqs)
-    for (res, info), ref in zip(got, alone):
+    for (res, info), ref, (ep, ec) in zip(got, alone, exp):
         _same(res, ref)
+        assert res.paths == ep and res.search_costs == ec
         assert info["status"] == 0 and info["total_ms"] >= info["run_ms"] >= 0
     st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 0
@@ -153,9 +166,10 @@ def test_submit_validation_and_unknown_tickets(engine):
     srv.close()
 
 
-def test_resident_boards_mixed_with_uploaded_ones(engine):
+def test_resident_boards_mixed_with_uploaded_ones(engine, oracle):
     """Requests against boards kept in HBM and requests that bring their own
-    board share launches; every result equals the request solved alone."""
+    board share launches; every result equals the request solved alone and the
+    oracle's answer."""
     pool = [W.congestion_board(seed=200 + k, w=96 + 40 * k, h=80 + 30 * k, layers=2 + k, n_nets=0) for k in range(3)]
     boards = [engine.board(b.grid, b.x, b.y, b.vias, b.directed) for b in pool]
     trace = W.serving_trace(pool, 50.0, 30, seed=4, min_nets=4, max_nets=48)
@@ -169,6 +183,8 @@ def test_resident_boards_mixed_with_uploaded_ones(engine):
     for t, (_, wl) in zip(tickets, trace):
         res, _ = srv.wait(t)
         _same(res, engine.route_isolated_batch(wl.request()))
+        ep, ec = oracle.isolated_batch(wl.request(), retry_full=True, mode="field")
+        assert res.paths == ep and res.search_costs == ec
     assert srv.stats()["largest_launch"] >= 1
     srv.close()
     for b in boards:

@@ -7,8 +7,9 @@ allowed.  For them the library keeps one static device array and carves every
 scratch buffer of a window solve from it.  These tests call that entry point
 through the C ABI and require its paths and search costs to equal, bit for
 bit, those of the allocating entry point (mrc_route_isolated_batch without the
-full-board retry) on two calls in a row, and require a request that does not
-fit the array to be refused with a clear error.
+full-board retry) and those of the CPU oracle on the same requests, on two
+calls in a row, and require a request that does not fit the array to be
+refused with a clear error.
 """
 import ctypes as C
 
@@ -42,7 +43,7 @@ def _noalloc(lib, req):
     return paths, [int(c) for c in costs[:n]]
 
 
-def test_noalloc_entry_point_matches_the_allocating_one_on_two_calls_in_a_row():
+def test_noalloc_entry_point_matches_the_allocating_one_on_two_calls_in_a_row(oracle):
     lib = mrcuda.load_library()
     eng = mrcuda.Engine(0)
     try:
@@ -52,8 +53,9 @@ def test_noalloc_entry_point_matches_the_allocating_one_on_two_calls_in_a_row():
             req = wl.request()
             ref = eng.route_isolated_batch(req, retry_full=False)
             got_paths, got_costs = _noalloc(lib, req)
-            assert got_paths == ref.paths
-            assert got_costs == ref.search_costs
+            exp_paths, exp_costs = oracle.isolated_batch(req, retry_full=False, mode="astar")
+            assert got_paths == ref.paths == exp_paths
+            assert got_costs == ref.search_costs == exp_costs
             assert all(p is not None for p in got_paths)
     finally:
         eng.close()
