@@ -46,23 +46,15 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_value(kernel_profile: str, key: str):
-    """A `key: value` figure from the committed ncu summary, when present."""
-    path = os.path.join(ROOT, "profiles", kernel_profile)
+def _profile_figures(kernel: str, workload: str):
+    """Figures of one kernel on one workload from the ncu captures summarised in
+    profiles/roofline.json (DRAM bytes of one full-size launch, instructions
+    per window cell, IPC), or None when that pair was not captured."""
     try:
-        with open(path) as f:
-            for line in f:
-                if line.strip().startswith(key + ":"):
-                    return float(line.split(":", 1)[1].strip().split()[0])
-    except OSError:
-        pass
-    return None
-
-
-def _traffic_per_launch(kernel_profile: str):
-    """DRAM bytes per relax launch from the committed ncu summary, when present."""
-    v = _profile_value(kernel_profile, "traffic_bytes_per_launch")
-    return None if v is None else int(v)
+        with open(os.path.join(ROOT, "profiles", "roofline.json")) as f:
+            return json.load(f).get(f"{kernel}/{workload}")
+    except (OSError, ValueError):
+        return None
 
 
 def _workload(name: str, rank: int, nets: int = 0):
@@ -108,10 +100,11 @@ class Job:
         return [wl.request() for wl in self.boards]
 
     def route(self, eng):
-        """The public host-buffer call: one request, or many instances."""
+        """The public host-buffer call (one request, or many instances in one
+        call); returns the result in its CSR form (paths as numpy arrays)."""
         if len(self.boards) == 1:
-            return eng.route_isolated_batch(self.boards[0].request()).paths
-        return [p for r in eng.route_instances(self.requests()) for p in r.paths]
+            return eng.route_isolated_batch(self.boards[0].request())
+        return eng.route_instances(self.requests(), split=False)
 
     def h2d_bytes(self) -> int:
         b = 0
@@ -173,9 +166,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _cpu_sample_rate(job, n_sample: int, threads: int = 0):
-    """The oracle's A* alone-path search (window, then full board) on a sample of
-    nets, all host threads: nets/s.  Oracle code, timed as the CPU baseline; never the measured GPU path."""
+def _cpu_sample_rate(job, n_sample: int, threads: int = 0, mode: str = "astar"):
+    """The oracle's alone-path search (window, then full board) on a sample of
+    nets, all host threads: nets/s.  mode "astar" is the targeted search with
+    early stop (LeeRouter / the rayon alone-path batch); mode "field" expands
+    the whole window with h = 0 (the complete field, bfs_distance_field) and
+    walks the canonical path.  Oracle code, timed as the CPU baseline; never the
+    measured GPU path."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     from mrcuda.types import IsolatedRouteRequest
@@ -186,7 +183,7 @@ def _cpu_sample_rate(job, n_sample: int, threads: int = 0):
         sub = IsolatedRouteRequest(req.grid, req.nets[:n_sample], req.windows[:n_sample], req.x_edge_costs,
                                    req.y_edge_costs, req.via_edge_costs, req.directed_in_costs)
         t0 = time.perf_counter()
-        o.isolated_batch(sub, retry_full=True, mode="astar", threads=threads)
+        o.isolated_batch(sub, retry_full=True, mode=mode, threads=threads)
         dt = time.perf_counter() - t0
         return n_sample / dt, dt
     # instances: one search per instance, spread over the host threads
@@ -200,7 +197,7 @@ def _cpu_sample_rate(job, n_sample: int, threads: int = 0):
     n = sum(len(r.nets) for r in reqs)
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
-        list(ex.map(lambda r: o.isolated_batch(r, retry_full=True, mode="astar", threads=1), reqs))
+        list(ex.map(lambda r: o.isolated_batch(r, retry_full=True, mode=mode, threads=1), reqs))
     dt = time.perf_counter() - t0
     return n / dt, dt
 
@@ -211,7 +208,9 @@ def run_reference(args):
         return 0
     wl = _workload(args.workload, 0, args.nets)
     cores = os.cpu_count() or 1
-    n_sample = min(args.cpu_sample or (2048 if len(wl.boards) > 1 else 128), len(wl.nets))
+    # every net of the workload per step (the snapshot board's 3000 nets of
+    # up to 1.5 M window cells each would take minutes: a sample there)
+    n_sample = min(args.cpu_sample or (48 if args.workload == "snapshot" else len(wl.nets)), len(wl.nets))
     for _ in range(args.warmup):
         _cpu_sample_rate(wl, max(n_sample // 4, 1))
     rates = []
@@ -229,36 +228,34 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{n_sample} of {len(wl.nets)} nets per step: A* alone-path search "
                                    f"(window, then full board), {cores} host threads"},
+        "same_config": n_sample == len(wl.nets),
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
-def run_engine(args):
-    import numpy as np
+def measure_batch(args, name, eng, rank, world, local, dist, nets=0, steps=None, main=True):
+    """One batched workload on the resident engine: autotune, graph capture,
+    warm-up, K device-timed steps (L2 flushed between them), the end-to-end
+    public call with host buffers, the roofline of the relax kernel.  Returns
+    the JSON line (without the plain-form and CPU legs) and the objects the
+    caller may still need."""
     import torch
 
     import mrcuda
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    from mrcuda.dist import init_from_env, max_over_ranks
+    from mrcuda.dist import max_over_ranks
     from mrcuda.workloads import pin_boards
 
-    dist = init_from_env("nccl", timeout_s=120.0, device=torch.device("cuda", local))
-
-    wl = _workload(args.workload, rank, args.nets)
-    eng = mrcuda.Engine(local)
+    steps = args.steps if steps is None else steps
+    wl = _workload(name, rank, nets)
     boards = [eng.board(b.grid, b.x, b.y, b.vias, b.directed) for b in wl.boards]
     if len(boards) == 1:
         batch = mrcuda.Batch(boards[0], wl.nets, wl.windows, retry_full=True, time_kernels=True)
     else:
         batch = mrcuda.Batch(boards, wl.nets, wl.windows, retry_full=True, time_kernels=True, net_board=wl.net_board)
     # setup, outside the timed region: tile autotune, then capture the launch sequence as a graph
-    if args.config:
+    if args.config and main:
         cfg = [int(v) for v in args.config.split(",")]
         batch.set_config(cfg[0], cfg[1])
         if len(cfg) > 2:
@@ -288,7 +285,7 @@ def run_engine(args):
     clocks = ClockSampler(local)
     clocks.start()
     step_ms, relax_ms = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -309,41 +306,50 @@ def run_engine(args):
 
     # end to end through the public call with host buffers: first the caller's
     # ordinary (pageable) arrays, then the same boards in page-locked memory
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(1, min(steps, 5))
 
     def e2e_time():
         wl.route(eng)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            paths = wl.route(eng)
+            res = wl.route(eng)
         torch.cuda.synchronize()
-        return (time.perf_counter() - t0) / e2e_steps, paths
+        return (time.perf_counter() - t0) / e2e_steps, res
 
-    e2e_pageable_s, out_pageable = e2e_time()
+    e2e_pageable_s, res_pageable = e2e_time()
     pin_boards(eng, wl.boards)
-    e2e_s, out_paths = e2e_time()
-    assert out_pageable == out_paths, "page-locked inputs changed the answer"
+    e2e_s, res = e2e_time()
+    out_paths = res.paths  # lists built after the timed calls, for the checks below
+    assert res_pageable.paths == out_paths, "page-locked inputs changed the answer"
     e2e_value = len(wl.nets) * world / max_over_ranks(e2e_s, device="cuda")
     e2e_pageable = len(wl.nets) * world / max_over_ranks(e2e_pageable_s, device="cuda")
     h2d = wl.h2d_bytes()
-    d2h = 8 * (len(wl.nets) + 1) + 4 * len(wl.nets) + 4 * sum(len(p) for p in out_paths if p) + 4
+    d2h = int(res.offsets.nbytes + res.costs.nbytes + res.cells.nbytes) + 4  # + the status word
     assert out_paths == first.paths, "end-to-end call disagrees with the resident batch"
 
-    # roofline of the dominant kernel (relax_rounds_kernel)
+    # roofline of the dominant kernel (the relax kernel)
     peak, peak_kind = _peaks()
     alg_bytes = wl.algorithmic_bytes() + 4 * path_cells
     relax_avg = statistics.fmean(relax_ms) if relax_ms and min(relax_ms) > 0 else ms
     achieved = alg_bytes / (relax_avg / 1000.0) / 1e9
     sched = batch.config()
-    kname = "relax_async_kernel" if sched["schedule"] == 1 else "relax_rounds_kernel"
-    # DRAM bytes per launch from the committed ncu summary of this kernel and workload
-    prof = f"{kname.replace('_kernel', '')}_{args.workload}.md"
-    traffic = _traffic_per_launch(prof)
-    ipc = _profile_value(prof, "ipc_per_sm")
+    kname = {0: "relax_rounds_kernel", 1: "relax_async_kernel", 2: "relax_warp_kernel"}[sched["schedule"]]
+    kfull = "relax_warp_kernel" if sched["schedule"] == 2 else f"{kname}<{sched['tile_h']},{sched['threads']}>"
+    # DRAM bytes and instruction counts of one launch, from the ncu capture of this kernel and workload
+    prof = _profile_figures(kname, name)
+    acts = max(work["activations"], 1)
+    counters = {"tile_activations": work["activations"], "tiles": work["tiles"],
+                "activations_per_tile": work["activations"] / max(work["tiles"], 1),
+                "passes_per_activation" if sched["schedule"] == 2 else "sweeps_per_activation": work["sweeps"] / acts,
+                "in_tile_sweeps": work["sweeps"]}
+    if sched["schedule"] == 2:
+        counters["rows_per_activation"] = work["rows"] / acts
+    else:
+        counters["rounds"] = work["rounds"]
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl.meta["workload"], "nets_per_rank": len(wl.nets), "window_cells": wl.window_cells(),
@@ -351,18 +357,74 @@ def run_engine(args):
                    "windows": wl.meta.get("windows"), "autotuned": tuned, "graph": not args.no_graph,
                    "instances": len(wl.boards)},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "inputs": "page-locked host arrays", "pageable_value": e2e_pageable},
-        "gpu_launches": batch.kernel_launches * args.steps,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind, "kernel": f"{kname}<{sched['tile_h']},{sched['threads']}>",
-                     "kernel_ms": relax_avg, "algorithmic_bytes_per_launch": int(alg_bytes),
-                     "bytes_per_cell": round(wl.bytes_per_cell(), 3), "tile_activations": work["activations"],
-                     "in_tile_sweeps": work["sweeps"], "rounds": work["rounds"], "tiles": work["tiles"],
-                     # what does bind the kernel: instruction issue (ncu, small case of the same kernel)
-                     "issue": None if ipc is None else {"ipc_per_sm": ipc, "peak_ipc_per_sm": 4.0,
-                                                        "frac": ipc / 4.0, "source": f"profiles/{prof}"}},
+                "inputs": "page-locked host arrays", "outputs": "CSR arrays (offsets, cells, costs)",
+                "pageable_value": e2e_pageable,
+                "vs_device_value": e2e_value / value},
+        "gpu_launches": batch.kernel_launches * steps,
+        "roofline": dict({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                          "traffic": None if prof is None else prof.get("dram_bytes_per_launch"),
+                          "peak_kind": peak_kind, "kernel": kfull, "kernel_ms": relax_avg,
+                          "algorithmic_bytes_per_launch": int(alg_bytes),
+                          "bytes_per_cell": round(wl.bytes_per_cell(), 3)}, **counters),
         "clocks": clk,
     }
+    if prof is not None:
+        # what does bind the kernel: instruction issue (ncu, the same kernel and workload)
+        line["roofline"]["issue"] = {k: prof[k] for k in ("ipc_per_sm", "inst_per_cell", "capture") if k in prof}
+    return line, wl, batch, boards, first
+
+
+def _summary(line):
+    """The compact form of a workload's line inside `workloads`."""
+    out = {"workload": line["config"]["workload"], "value": line["value"], "unit": line["unit"],
+           "ms_per_step": line["ms_per_step"], "e2e": line["e2e"]["value"], "clocks": line.get("clocks")}
+    r = line.get("roofline")
+    if r:
+        out["roofline"] = {k: r[k] for k in ("kernel", "kernel_ms", "achieved", "frac", "traffic",
+                                             "activations_per_tile", "passes_per_activation",
+                                             "sweeps_per_activation", "rows_per_activation") if k in r}
+    if "cpu_baseline" in line:
+        out["cpu_baseline"] = line["cpu_baseline"]["value"]
+    return out
+
+
+def other_workloads(args, eng, local):
+    """The configurations beside the headline one, measured in the same
+    invocation on the same GPU: the plain board (config 1), 4096 uneven
+    instances in one launch (config 3), snapshot negotiation rounds (config 4)
+    and the serving loop (config 5)."""
+    out = {}
+    for name in ("plain", "uneven"):
+        line, _, batch, boards, _ = measure_batch(args, name, eng, 0, 1, local, None, steps=min(args.steps, 10),
+                                                  main=False)
+        out[name] = _summary(line)
+        batch.close()
+        for b in boards:
+            b.close()
+    line = measure_snapshot(args, eng, local, rounds=3, warmup=2, cpu=False)
+    out["snapshot"] = _summary(line)
+    out["snapshot"]["per_round"] = line["config"]["per_round"]
+    rows, clk = measure_serving(args, eng, local, rates=[20.0, 100.0, 400.0], seconds=2.0, max_requests=500)
+    out["serving"] = {"workload": "serving, Poisson arrivals (3 rates, 2 s of arrivals each)", "rates": rows,
+                      "clocks": clk}
+    return out
+
+
+def run_engine(args):
+    import torch
+
+    import mrcuda
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from mrcuda.dist import init_from_env
+
+    dist = init_from_env("nccl", timeout_s=120.0, device=torch.device("cuda", local))
+    eng = mrcuda.Engine(local)
+    line, wl, batch, boards, first = measure_batch(args, args.workload, eng, rank, world, local, dist)
+    value = line["value"]
 
     if rank == 0 and world == 1 and not args.no_plain:
         ps = min(args.plain_sample or (64 if len(wl.boards) > 1 else 8), len(wl.nets))
@@ -380,25 +442,39 @@ def run_engine(args):
         line["vs_plain"] = value / (ps / dt)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # p50 of 7 warm runs on all host threads, and the same single-threaded on
-        # a smaller sample (the reference's rayon batch and its LeeRouter loop)
+        # a smaller sample (the reference's rayon batch and its LeeRouter loop),
+        # for the targeted search (paths) and for complete fields (h = 0)
         n_sample = min(args.cpu_sample or (2048 if len(wl.boards) > 1 else 128), len(wl.nets))
         n_one = max(1, n_sample // 8)
         cores = os.cpu_count() or 1
-        _cpu_sample_rate(wl, max(n_sample // 4, 1))
-        runs = [_cpu_sample_rate(wl, n_sample) for _ in range(7)]
-        rate = statistics.median(r for r, _ in runs)
-        one = statistics.median(_cpu_sample_rate(wl, n_one, threads=1)[0] for _ in range(7))
+
+        def timed(mode):
+            _cpu_sample_rate(wl, max(n_sample // 4, 1), mode=mode)
+            runs = [_cpu_sample_rate(wl, n_sample, mode=mode) for _ in range(7)]
+            one = statistics.median(_cpu_sample_rate(wl, n_one, threads=1, mode=mode)[0] for _ in range(7))
+            return statistics.median(r for r, _ in runs), sum(d for _, d in runs), one
+
+        rate, secs, one = timed("astar")
+        f_rate, f_secs, f_one = timed("field")
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{n_sample} of {len(wl.nets)} nets, A* alone-path search (window, then "
                                           f"full board), {cores} host threads, p50 of 7 warm runs "
-                                          f"({sum(d for _, d in runs):.2f} s in all)",
+                                          f"({secs:.2f} s in all)",
                                 "single_thread": {"value": one, "unit": UNIT,
-                                                  "sample": f"{n_one} nets, 1 thread, p50 of 7 warm runs"}}
-    if rank == 0:
-        print(json.dumps(line))
+                                                  "sample": f"{n_one} nets, 1 thread, p50 of 7 warm runs"},
+                                "fields": {"value": f_rate, "unit": UNIT, "cores": cores,
+                                           "sample": f"{n_sample} nets, complete window field (h = 0 Dijkstra, "
+                                                     f"every window cell settled) + canonical path, {cores} host "
+                                                     f"threads, p50 of 7 warm runs ({f_secs:.2f} s in all)",
+                                           "single_thread": {"value": f_one, "unit": UNIT,
+                                                             "sample": f"{n_one} nets, 1 thread, p50 of 7"}}}
     batch.close()
     for b in boards:
         b.close()
+    if rank == 0 and world == 1 and not args.no_workloads and args.workload == "congestion":
+        line["workloads"] = other_workloads(args, eng, local)
+    if rank == 0:
+        print(json.dumps(line))
     eng.close()
     if dist:
         dist.destroy_process_group()
@@ -423,6 +499,23 @@ def run_snapshot(args):
         if args.groups:
             raise SystemExit("--groups: connection groups need every path, so they do not run sharded")
         return run_snapshot_sharded(args, rank, world, local)
+    eng = mrcuda.Engine(local)
+    line = measure_snapshot(args, eng, local, rounds=args.steps, warmup=max(args.warmup, 3),
+                            cpu=not args.no_cpu_baseline)
+    print(json.dumps(line))
+    eng.close()
+    return 0
+
+
+def measure_snapshot(args, eng, local, rounds, warmup, cpu):
+    """Snapshot negotiation rounds from a fresh start on the 2048x2048x6 board:
+    `rounds` timed rounds (fewer if it converges) after `warmup` rounds of a
+    separate negotiation.  Returns the JSON line."""
+    import torch
+
+    import mrcuda
+    from mrcuda import workloads as W
+
     wl = W.snapshot_board(n_nets=args.nets or 3000)
     groups = None
     if args.groups:
@@ -431,9 +524,8 @@ def run_snapshot(args):
                                        nt.passable_pads, nt.via_passable_pads) for i, nt in enumerate(wl.nets)]
         groups = "connections"
     req = wl.request()
-    eng = mrcuda.Engine(local)
     warm = eng.negotiation(req, groups=groups)
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(warmup):
         warm.round()
     warm.close()
     torch.cuda.synchronize()
@@ -441,8 +533,9 @@ def run_snapshot(args):
     clocks.start()
     t0 = time.perf_counter()
     neg = eng.negotiation(req, groups=groups)
+    n_rounds = rounds
     rounds = []
-    for _ in range(args.steps):
+    for _ in range(n_rounds):
         st = neg.round()
         if not st["dirty"]:
             break
@@ -461,7 +554,7 @@ def run_snapshot(args):
     h2d = wl.grid.cost.nbytes + wl.directed.nbytes + 40 * len(wl.nets) + 16 * len(wl.windows)
     line = {
         "metric": METRIC, "value": routed / (dev_ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": len(rounds),
-        "warmup": max(args.warmup, 3), "ms_per_step": dev_ms / max(len(rounds), 1), "higher_is_better": True,
+        "warmup": warmup, "ms_per_step": dev_ms / max(len(rounds), 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl.meta["workload"], "rounds": len(rounds), "nets_routed": routed,
                    "groups": (f"connection groups: '#'-siblings of {args.groups} nets, plus shared endpoints"
@@ -477,7 +570,7 @@ def run_snapshot(args):
                      "algorithmic_bytes": int(alg), "bytes_per_cell": wl.bytes_per_cell()},
         "clocks": clk,
     }
-    if not args.no_cpu_baseline:
+    if cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
 
@@ -493,10 +586,8 @@ def run_snapshot(args):
                                           f"(directed prices), {cores} host threads, {dt:.2f} s"}
     # gpu launches: per round 4 negotiation kernels + the batch sequence (+ a retry batch)
     line["gpu_launches"] = sum(4 + 4 + (4 if r["retried"] else 0) + (1 if groups else 0) for r in rounds)
-    print(json.dumps(line))
     neg.close()
-    eng.close()
-    return 0
+    return line
 
 
 def _run_trace(eng, trace, slots, max_batch, boards):
@@ -617,24 +708,9 @@ def run_serving(args):
     torch.cuda.set_device(local)
     if rank != 0:
         return 0
-    pool = W.serving_pool(n_boards=16)
     eng = mrcuda.Engine(local)
-    boards = [eng.board(b.grid, b.x, b.y, b.vias, b.directed) for b in pool]  # device-resident grids
     rates = [float(r) for r in args.rates.split(",")]
-    rows = []
-    clocks = ClockSampler(local)
-    clocks.start()
-    for rate in rates:
-        n = max(20, min(int(rate * args.serve_seconds), args.serve_max))
-        trace = W.serving_trace(pool, rate, n, seed=int(rate))
-        row = {"rate_req_s": rate, "requests": n}
-        for name, slots, mb in (("batched", args.slots, 64), ("one_at_a_time", 1, 1)):
-            lat, nets, span, st = _run_trace(eng, trace, slots, mb, boards)
-            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                         "nets_per_s": nets / span, "req_per_s": n / span, "launches": st["launches"],
-                         "largest_launch": st["largest_launch"], "peak_gb": st["peak_bytes"] / 1e9}
-        rows.append(row)
-    clk = clocks.stop()
+    rows, clk = measure_serving(args, eng, local, rates, args.serve_seconds, args.serve_max)
     top = rows[-1]["batched"]
     line = {
         "metric": METRIC, "value": top["nets_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(rates),
@@ -651,10 +727,36 @@ def run_serving(args):
         "clocks": clk,
     }
     print(json.dumps(line))
-    for b in boards:
-        b.close()
     eng.close()
     return 0
+
+
+def measure_serving(args, eng, local, rates, seconds, max_requests):
+    """Each rate's Poisson trace through the continuous-batching server and
+    through the one-request-at-a-time loop; returns (rows, clocks)."""
+    import numpy as np
+
+    from mrcuda import workloads as W
+
+    pool = W.serving_pool(n_boards=16)
+    boards = [eng.board(b.grid, b.x, b.y, b.vias, b.directed) for b in pool]  # device-resident grids
+    rows = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for rate in rates:
+        n = max(20, min(int(rate * seconds), max_requests))
+        trace = W.serving_trace(pool, rate, n, seed=int(rate))
+        row = {"rate_req_s": rate, "requests": n}
+        for name, slots, mb in (("batched", args.slots, 64), ("one_at_a_time", 1, 1)):
+            lat, nets, span, st = _run_trace(eng, trace, slots, mb, boards)
+            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "nets_per_s": nets / span, "req_per_s": n / span, "launches": st["launches"],
+                         "largest_launch": st["largest_launch"], "peak_gb": st["peak_bytes"] / 1e9}
+        rows.append(row)
+    clk = clocks.stop()
+    for b in boards:
+        b.close()
+    return rows, clk
 
 
 def main():
@@ -679,8 +781,12 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="measure only the chosen workload (by default the congestion line also carries the "
+                         "plain, uneven, snapshot and serving workloads)")
     ap.add_argument("--config", default="",
-                    help="force the relax tile height, CTA width and schedule (0 rounds, 1 queue), e.g. 8,256,1")
+                    help="force the relax tile height, CTA width and schedule (0 rounds, 1 queue, 2 warp "
+                         "tiles), e.g. 8,256,1")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -570,9 +570,17 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
     // step up from the lower one.  The source tile starts fully open.
     const uint32_t all = (1u << TH) - 1u;
     RowMarks m{all, 1u, 1u << (TH - 1), 0u};
+    uint32_t fell = 0;
     {
-        const uint32_t sr = f.src % plane, sy = sr / t.w, sx = sr - sy * t.w;
-        if (sx >= t.tx0 && sx < t.tx0 + t.tw && sy >= t.ty0 && sy < t.ty0 + t.th) m = RowMarks{all, all, all, all};
+        const uint32_t sl = f.src / plane, sr = f.src - sl * plane, sy = sr / t.w, sx = sr - sy * t.w;
+        if (sx >= t.tx0 && sx < t.tx0 + t.tw && sy >= t.ty0 && sy < t.ty0 + t.th) {
+            m = RowMarks{all, all, all, all};
+            // The seeded source label never falls here, yet a neighbour tile
+            // may be reachable only through its step across the border: it
+            // counts as fallen, so the push checks see it.
+            const uint32_t x = sx - t.tx0;
+            if (t.act && t.l == sl && x >= t.xb && x < t.xb + K) fell |= 1u << ((sy - t.ty0) * K + (x - t.xb));
+        }
     }
     // start with the vertical direction whose entry halo is closer to the source
     uint32_t dtop = kMax, dbot = kMax;
@@ -585,7 +593,7 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
     dbot = __reduce_min_sync(kFull, dbot);
     // passes cycle (first vertical direction, the other one, stacks)
     bool down = dtop <= dbot;
-    uint32_t fell = 0, passes = 0, rows = 0;
+    uint32_t passes = 0, rows = 0;
     const uint32_t pass_limit = 12u * TH * t.TW * t.L + 48u;
     for (uint32_t step = 0;; ++step) {
         const uint32_t phase = step % 3;

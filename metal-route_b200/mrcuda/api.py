@@ -384,15 +384,70 @@ def _marshal_requests(m: _Marshal, requests: Sequence[IsolatedRouteRequest]):
     return reqs
 
 
-@dataclass
 class IsolatedBatchResult:
-    """Per-net outputs, aligned with the request's nets."""
+    """Per-net outputs, aligned with the request's nets.
 
-    paths: List[Optional[List[int]]]
-    search_costs: List[int]
-    fields: Optional[List[np.ndarray]] = None
-    field_windows: Optional[List[IsolatedRouteWindow]] = None
-    retried: int = 0
+    The library hands the paths back in CSR form, kept here as numpy arrays:
+    ``offsets`` (n + 1 u64), ``cells`` (u32 global CellIdx) and ``costs`` (n u32,
+    0xFFFFFFFF = unreachable); net i's path is cells[offsets[i]:offsets[i+1]],
+    empty when the net has none.  ``paths`` (the provider's
+    Vec<Option<Vec<CellIdx>>>) and ``search_costs`` are the same data as Python
+    lists, built on first use, so callers that work on the arrays never pay
+    for per-path list objects."""
+
+    def __init__(self, paths: Optional[List[Optional[List[int]]]] = None, search_costs: Optional[List[int]] = None,
+                 fields: Optional[List[np.ndarray]] = None, field_windows: Optional[List[IsolatedRouteWindow]] = None,
+                 retried: int = 0, *, offsets: Optional[np.ndarray] = None, cells: Optional[np.ndarray] = None,
+                 costs: Optional[np.ndarray] = None):
+        if offsets is None:
+            paths = [] if paths is None else list(paths)
+            search_costs = [] if search_costs is None else list(search_costs)
+            lens = [len(p) if p else 0 for p in paths]
+            offsets = np.zeros(len(paths) + 1, np.uint64)
+            offsets[1:] = np.cumsum(lens, dtype=np.uint64)
+            cells = np.array([c for p in paths if p for c in p], dtype=np.uint32)
+            costs = np.array(search_costs, dtype=np.uint32)
+        self.offsets = offsets
+        self.cells = cells
+        self.costs = costs
+        self._paths = paths
+        self._search_costs = search_costs
+        self.fields = fields
+        self.field_windows = field_windows
+        self.retried = retried
+
+    def __len__(self) -> int:
+        return len(self.offsets) - 1
+
+    @property
+    def paths(self) -> List[Optional[List[int]]]:
+        if self._paths is None:
+            cl, ol = self.cells.tolist(), self.offsets.tolist()
+            self._paths = [cl[ol[i]:ol[i + 1]] if ol[i + 1] > ol[i] else None for i in range(len(ol) - 1)]
+        return self._paths
+
+    @property
+    def search_costs(self) -> List[int]:
+        if self._search_costs is None:
+            self._search_costs = self.costs.tolist()
+        return self._search_costs
+
+    def path(self, i: int) -> Optional[np.ndarray]:
+        """Net i's path as a u32 view of ``cells`` (None when unreachable)."""
+        a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+        return self.cells[a:b] if b > a else None
+
+    def routed(self) -> int:
+        return int(np.count_nonzero(np.diff(self.offsets)))
+
+    def slice(self, start: int, stop: int) -> "IsolatedBatchResult":
+        """Nets [start, stop) as a result of their own (views, offsets rebased)."""
+        off = self.offsets[start:stop + 1]
+        a, b = int(off[0]), int(off[-1])
+        return IsolatedBatchResult(fields=self.fields[start:stop] if self.fields is not None else None,
+                                   field_windows=(self.field_windows[start:stop]
+                                                  if self.field_windows is not None else None),
+                                   offsets=off - np.uint64(a), cells=self.cells[a:b], costs=self.costs[start:stop])
 
 
 def _take_result(L, res, n: int, fields: bool, layers: int = 1) -> IsolatedBatchResult:
@@ -405,9 +460,7 @@ def _take_result(L, res, n: int, fields: bool, layers: int = 1) -> IsolatedBatch
                  if total else np.zeros(0, np.uint32))
         costs = (np.ctypeslib.as_array(L.mrc_result_search_costs(res), shape=(n,)).copy()
                  if n else np.zeros(0, np.uint32))
-        cl, ol = cells.tolist(), off.tolist()
-        paths = [cl[ol[i]:ol[i + 1]] if ol[i + 1] > ol[i] else None for i in range(n)]
-        out = IsolatedBatchResult(paths, costs.tolist(), retried=int(L.mrc_result_retried(res)))
+        out = IsolatedBatchResult(retried=int(L.mrc_result_retried(res)), offsets=off, cells=cells, costs=costs)
         wp = L.mrc_result_field_windows(res) if fields else None
         if n and wp:
             wa = np.ctypeslib.as_array(C.cast(wp, C.POINTER(C.c_uint32)), shape=(n * 4,)).tolist()
@@ -844,9 +897,10 @@ class Engine:
         return _take_result(self.lib, res, len(req.nets), keep_fields)
 
     def route_instances(self, requests: Sequence[IsolatedRouteRequest], retry_full: bool = True,
-                        keep_fields: bool = False) -> List[IsolatedBatchResult]:
+                        keep_fields: bool = False, split: bool = True):
         """Solve many independent instances (own board, nets, windows) in one
-        persistent launch; one result per instance."""
+        persistent launch; one result per instance, or with split=False one
+        result over the instances' nets in order."""
         m = _Marshal()
         reqs = _marshal_requests(m, requests)
         flags = (MRC_FLAG_RETRY_FULL if retry_full else 0) | (MRC_FLAG_KEEP_FIELDS if keep_fields else 0)
@@ -855,13 +909,12 @@ class Engine:
                                                  C.byref(res)))
         total = sum(len(rq.nets) for rq in requests)
         allr = _take_result(self.lib, res, total, keep_fields)
+        if not split:
+            return allr
         out, o = [], 0
         for rq in requests:
             n = len(rq.nets)
-            sl = slice(o, o + n)
-            out.append(IsolatedBatchResult(allr.paths[sl], allr.search_costs[sl],
-                                           allr.fields[sl] if allr.fields is not None else None,
-                                           allr.field_windows[sl] if allr.field_windows is not None else None))
+            out.append(allr.slice(o, o + n))
             o += n
         return out
 
