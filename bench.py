@@ -404,7 +404,8 @@ def other_workloads(args, eng, local):
     line = measure_snapshot(args, eng, local, rounds=3, warmup=2, cpu=False)
     out["snapshot"] = _summary(line)
     out["snapshot"]["per_round"] = line["config"]["per_round"]
-    rows, clk = measure_serving(args, eng, local, rates=[20.0, 100.0, 400.0], seconds=2.0, max_requests=500)
+    rows, clk = measure_serving(args, eng, local, rates=[20.0, 100.0, 400.0], seconds=2.0, max_requests=400,
+                                repeats=1)
     out["serving"] = {"workload": "serving, Poisson arrivals (3 rates, 2 s of arrivals each)", "rates": rows,
                       "clocks": clk}
     return out
@@ -620,7 +621,7 @@ def _run_trace(eng, trace, slots, max_batch, boards):
         ready.acquire()
         res, info = srv.wait(tickets[i])
         lat.append(info["total_ms"])
-        nets += len(res.paths)
+        nets += len(res)
     makespan = time.perf_counter() - t0
     th.join()
     st = srv.stats()
@@ -710,7 +711,7 @@ def run_serving(args):
         return 0
     eng = mrcuda.Engine(local)
     rates = [float(r) for r in args.rates.split(",")]
-    rows, clk = measure_serving(args, eng, local, rates, args.serve_seconds, args.serve_max)
+    rows, clk = measure_serving(args, eng, local, rates, args.serve_seconds, args.serve_max, args.serve_repeats)
     top = rows[-1]["batched"]
     line = {
         "metric": METRIC, "value": top["nets_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(rates),
@@ -731,9 +732,16 @@ def run_serving(args):
     return 0
 
 
-def measure_serving(args, eng, local, rates, seconds, max_requests):
+# request size classes by window cells (all nets, all layers): the boards span
+# 64^2-1024^2 cells and 16-512 nets, so request work spans four decades
+SIZE_CLASSES = (("small", 0, 4 << 20), ("medium", 4 << 20, 64 << 20), ("large", 64 << 20, 1 << 62))
+
+
+def measure_serving(args, eng, local, rates, seconds, max_requests, repeats=1):
     """Each rate's Poisson trace through the continuous-batching server and
-    through the one-request-at-a-time loop; returns (rows, clocks)."""
+    through the one-request-at-a-time loop, `repeats` times (different
+    arrival draws); latency percentiles over all repeats, overall and per
+    request size class.  Returns (rows, clocks)."""
     import numpy as np
 
     from mrcuda import workloads as W
@@ -743,15 +751,32 @@ def measure_serving(args, eng, local, rates, seconds, max_requests):
     rows = []
     clocks = ClockSampler(local)
     clocks.start()
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if len(v) else None
+
     for rate in rates:
         n = max(20, min(int(rate * seconds), max_requests))
-        trace = W.serving_trace(pool, rate, n, seed=int(rate))
-        row = {"rate_req_s": rate, "requests": n}
+        traces = [W.serving_trace(pool, rate, n, seed=int(rate) + 1000 * r) for r in range(repeats)]
+        row = {"rate_req_s": rate, "requests": n, "repeats": repeats}
         for name, slots, mb in (("batched", args.slots, 64), ("one_at_a_time", 1, 1)):
-            lat, nets, span, st = _run_trace(eng, trace, slots, mb, boards)
-            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                         "nets_per_s": nets / span, "req_per_s": n / span, "launches": st["launches"],
-                         "largest_launch": st["largest_launch"], "peak_gb": st["peak_bytes"] / 1e9}
+            lat, cells, runs = [], [], []
+            for trace in traces:
+                l, nets, span, st = _run_trace(eng, trace, slots, mb, boards)
+                lat += l
+                cells += [wl.window_cells() for _, wl in trace]
+                runs.append({"p50_ms": pct(l, 50), "p99_ms": pct(l, 99), "nets_per_s": nets / span,
+                             "req_per_s": n / span, "launches": st["launches"],
+                             "largest_launch": st["largest_launch"], "peak_gb": st["peak_bytes"] / 1e9})
+            lat, cells = np.array(lat), np.array(cells)
+            row[name] = {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                         "nets_per_s": float(np.mean([r["nets_per_s"] for r in runs])),
+                         "req_per_s": float(np.mean([r["req_per_s"] for r in runs])),
+                         "by_size": {c: {"requests": int(((cells >= lo) & (cells < hi)).sum()),
+                                         "p50_ms": pct(lat[(cells >= lo) & (cells < hi)], 50),
+                                         "p99_ms": pct(lat[(cells >= lo) & (cells < hi)], 99)}
+                                     for c, lo, hi in SIZE_CLASSES},
+                         "runs": runs}
         rows.append(row)
     clk = clocks.stop()
     for b in boards:
@@ -771,6 +796,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: seconds of arrivals per rate")
     ap.add_argument("--serve-max", type=int, default=600, help="serving: most requests per rate")
     ap.add_argument("--slots", type=int, default=2, help="serving: launches in flight")
+    ap.add_argument("--serve-repeats", type=int, default=3, help="serving: arrival draws per rate")
     ap.add_argument("--shards", action="store_true", help="snapshot: run the sharded rounds even on one rank")
     ap.add_argument("--groups", type=int, default=0,
                     help="snapshot: group nets into '#'-sibling connection groups of this size (0 = none)")

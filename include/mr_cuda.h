@@ -430,6 +430,10 @@ typedef struct {
     uint32_t max_batch_requests;  /* requests merged into one launch (>= 1) */
     uint64_t max_batch_cells;     /* window cells per launch (0 = no limit) */
     uint32_t max_layers;          /* largest layer count accepted (sizes the tile; <= 12) */
+    uint32_t merge_ratio;         /* size-aware merging: a request joins a launch only when its window cells
+                                   * are within this factor of the launch's first request, either way, so a
+                                   * small request never waits in a launch that carries a much larger one
+                                   * (0 = merge regardless of size) */
 } mrc_server_params;
 
 typedef struct {

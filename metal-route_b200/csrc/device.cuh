@@ -64,12 +64,19 @@ struct DevField {
 };
 
 // Control block of one batch launch (device memory, zeroed before launch).
+// The words that workers update atomically on every item (the list counts,
+// the consumption cursors) and the words idle workers poll (status) sit on
+// their own 128-byte lines, so polling never queues behind the atomics.
 struct Ctl {
-    uint32_t count[3];          // items in the three rotating tile lists
+    uint32_t count[3];          // items in the three rotating tile lists (queue form: [0] tail, [1] in flight)
+    uint32_t pad_count[29];
     uint32_t head[3];           // consumption cursors
+    uint32_t pad_head[29];
     uint32_t bar_count, bar_gen;
+    uint32_t pad_bar[30];
     uint32_t status;
     uint32_t rounds;
+    uint32_t pad_status[30];
     unsigned long long activations;
     unsigned long long sweeps;
     unsigned long long rows;    // tile rows relaxed (warp schedule)

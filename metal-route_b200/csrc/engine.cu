@@ -2208,6 +2208,8 @@ void server_reap(mrc_server *s, ServerBatch *b) {
     b->pack.data.reset();
 }
 
+constexpr uint32_t kMergeScan = 256;  // queued requests a forming launch looks at
+
 void server_loop(mrc_server *s) {
     std::unique_lock<std::mutex> lk(s->mu);
     auto free_slot = [&]() -> int {
@@ -2272,12 +2274,31 @@ void server_loop(mrc_server *s) {
             b->flags = head->flags;
             uint64_t cells = 0;
             const auto now = Clock::now();
-            while (!s->queue.empty() && b->reqs.size() < s->p.max_batch_requests) {
-                std::shared_ptr<ServerRequest> r = s->queue.front();
-                if (r->flags != b->flags) break;
-                if (!b->reqs.empty() && s->p.max_batch_cells && cells + r->cells > s->p.max_batch_cells) break;
-                if (s->inflight_bytes + b->footprint + r->footprint > s->budget) break;
-                s->queue.pop_front();
+            // The queue head always goes; later requests join in queue order when
+            // they have the same flags, fit the budget and the cell limit and, with
+            // a merge ratio, are of a similar size (window cells within the ratio of
+            // the head's, either way).  A request that does not join keeps its place
+            // for the next launch, which may start on another free slot at once.
+            const uint64_t head_cells = std::max<uint64_t>(head->cells, 1);
+            const uint64_t ratio = s->p.merge_ratio;
+            uint32_t scanned = 0;
+            for (auto it = s->queue.begin(); it != s->queue.end() && b->reqs.size() < s->p.max_batch_requests &&
+                                             scanned < kMergeScan;
+                 ++scanned) {
+                std::shared_ptr<ServerRequest> r = *it;
+                const uint64_t rc = std::max<uint64_t>(r->cells, 1);
+                bool join = b->reqs.empty();
+                if (!join) {
+                    join = r->flags == b->flags &&
+                           !(s->p.max_batch_cells && cells + r->cells > s->p.max_batch_cells) &&
+                           s->inflight_bytes + b->footprint + r->footprint <= s->budget &&
+                           (!ratio || (rc <= head_cells * ratio && head_cells <= rc * ratio));
+                }
+                if (!join) {
+                    ++it;
+                    continue;
+                }
+                it = s->queue.erase(it);
                 r->t_stage = now;
                 cells += r->cells;
                 b->footprint += r->footprint;
@@ -2343,7 +2364,7 @@ mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, 
     *out = nullptr;
     std::unique_ptr<mrc_server> s(new mrc_server());
     s->ctx = ctx;
-    s->p = params ? *params : mrc_server_params{0.8f, 2, 64, 0, 8};
+    s->p = params ? *params : mrc_server_params{0.8f, 2, 64, 0, 8, 8};
     if (s->p.hbm_fraction <= 0.f || s->p.hbm_fraction > 1.f) s->p.hbm_fraction = 0.8f;
     s->p.slots = std::max(1u, std::min(s->p.slots, 8u));
     s->p.max_batch_requests = std::max(1u, s->p.max_batch_requests);

@@ -36,7 +36,7 @@ __device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
 // flight.  lists[0, cap) holds the items, lists[cap, 2 cap) their ticket tags
 // (ticket + 1, zeroed before launch).  A tile is queued at most once at a time
 // (its tstamp word is the queued flag), so cap = total tiles never overflows.
-constexpr uint32_t kQueueSpinLimit = 1u << 26;
+constexpr uint32_t kQueueSpinLimit = 1u << 24;  // polls of one wait (~16 s with the backoff below)
 
 // Tile states in the tstamp word: 0 idle, 1 queued, 2 held by a worker,
 // 3 held and improved again meanwhile (the holder queues it once more when it
@@ -86,18 +86,24 @@ __device__ __forceinline__ u64 async_pop(const RelaxArgs &a) {
     const uint32_t h = atomicAdd(&c->head[0], 1u);
     const size_t slot = h % a.list_cap;
     const volatile u64 *tag = a.lists + a.list_cap + slot;
+    // Each waiter polls its own slot tag; the shared in-flight count and status
+    // words (which every worker updates) are read only every 16th poll, and the
+    // sleep between polls doubles up to 1 us, so thousands of idle waiters do
+    // not flood one L2 line while the busy workers update it.
     for (uint32_t spins = 0;; ++spins) {
         if (*tag == (u64)h + 1u) {
             __threadfence();
             return __ldcg(a.lists + slot);
         }
-        if (*(volatile const uint32_t *)&c->count[1] == 0u) return kInf;  // nothing queued or running
-        if (*(volatile const uint32_t *)&c->status) return kInf;
+        if ((spins & 15u) == 15u) {
+            if (*(volatile const uint32_t *)&c->count[1] == 0u) return kInf;  // nothing queued or running
+            if (*(volatile const uint32_t *)&c->status) return kInf;
+        }
         if (spins > kQueueSpinLimit) {
             atomicOr(&c->status, kStatusBarrier);
             return kInf;
         }
-        __nanosleep(spins < 32 ? 32 : 256);
+        __nanosleep(32u << min(spins >> 4, 5u));
     }
 }
 

@@ -450,7 +450,22 @@ __device__ __forceinline__ uint32_t neighbour_price(const WTile &t, int dir, uin
     return p;
 }
 
-__device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSmem &sm, uint32_t lane) {
+// Work counters a warp accumulates and adds to the control block in batches.
+struct WarpStats {
+    uint32_t acts = 0, passes = 0, rows = 0;
+};
+
+__device__ __forceinline__ void flush_stats(const RelaxArgs &a, WarpStats &w) {
+    if (!w.acts) return;
+    if (atomicAdd(&a.ctl->activations, (unsigned long long)w.acts) + w.acts > a.activation_limit)
+        atomicOr(&a.ctl->status, kStatusActivationLimit);
+    atomicAdd(&a.ctl->sweeps, (unsigned long long)w.passes);
+    atomicAdd(&a.ctl->rows, (unsigned long long)w.rows);
+    w = WarpStats{};
+}
+
+__device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSmem &sm, uint32_t lane,
+                          WarpStats &ws) {
     WTile t;
     const DevField f = a.fields[fi];
     t.fp = a.fields + fi;
@@ -669,9 +684,10 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
     pt = __any_sync(kFull, pt);
     pb = __any_sync(kFull, pb);
     if (lane == 0) {
-        if (atomicAdd(&ctl->activations, 1ull) >= a.activation_limit) atomicOr(&ctl->status, kStatusActivationLimit);
-        atomicAdd(&ctl->sweeps, (unsigned long long)passes);
-        atomicAdd(&ctl->rows, (unsigned long long)rows);
+        ws.acts += 1;
+        ws.passes += passes;
+        ws.rows += rows;
+        if (ws.acts == 32) flush_stats(a, ws);
         if (pl) async_push(a, fi, f.tile_off, tile - 1);
         if (pr) async_push(a, fi, f.tile_off, tile + 1);
         if (pt) async_push(a, fi, f.tile_off, tile - ntx);
@@ -687,13 +703,15 @@ __global__ void __launch_bounds__(NW * 32, 4) relax_warp_kernel(RelaxArgs a) {
     __shared__ WarpSmem smem[NW];
     WarpSmem &sm = smem[threadIdx.x >> 5];
     const uint32_t lane = threadIdx.x & 31;
+    WarpStats ws;
     for (;;) {
         u64 item = 0;
         if (lane == 0) item = async_pop(a);
         item = __shfl_sync(kFull, item, 0);
         if (item == kInf) break;
-        warp_item(a, (uint32_t)(item >> 32), (uint32_t)item, sm, lane);
+        warp_item(a, (uint32_t)(item >> 32), (uint32_t)item, sm, lane, ws);
     }
+    if (lane == 0) flush_stats(a, ws);
 }
 
 // Seeds: the source label and the source tile (warp tile geometry) of every

@@ -125,7 +125,7 @@ class _RoundStats(C.Structure):
 
 class _ServerParams(C.Structure):
     _fields_ = [("hbm_fraction", C.c_float), ("slots", C.c_uint32), ("max_batch_requests", C.c_uint32),
-                ("max_batch_cells", C.c_uint64), ("max_layers", C.c_uint32)]
+                ("max_batch_cells", C.c_uint64), ("max_layers", C.c_uint32), ("merge_ratio", C.c_uint32)]
 
 
 class _RequestInfo(C.Structure):
@@ -737,10 +737,12 @@ class Server:
     under an HBM budget with `slots` launches in flight."""
 
     def __init__(self, engine: "Engine", hbm_fraction: float = 0.8, slots: int = 2, max_batch_requests: int = 64,
-                 max_batch_cells: int = 0, max_layers: int = 8):
+                 max_batch_cells: int = 0, max_layers: int = 8, merge_ratio: int = 8):
+        """merge_ratio: requests merge into one launch only when their window
+        cells are within this factor of each other (0 = regardless of size)."""
         self.engine = engine
         h = C.c_void_p()
-        prm = _ServerParams(hbm_fraction, slots, max_batch_requests, max_batch_cells, max_layers)
+        prm = _ServerParams(hbm_fraction, slots, max_batch_requests, max_batch_cells, max_layers, merge_ratio)
         engine._check(engine.lib.mrc_server_create(engine.ctx, C.byref(prm), C.byref(h)))
         self.handle = h
         self._live = {}
