@@ -424,7 +424,8 @@ def run_engine(args):
 
     dist = init_from_env("nccl", timeout_s=120.0, device=torch.device("cuda", local))
     eng = mrcuda.Engine(local)
-    line, wl, batch, boards, first = measure_batch(args, args.workload, eng, rank, world, local, dist)
+    line, wl, batch, boards, first = measure_batch(args, args.workload, eng, rank, world, local, dist,
+                                                   nets=args.nets)
     value = line["value"]
 
     if rank == 0 and world == 1 and not args.no_plain:

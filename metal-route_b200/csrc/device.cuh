@@ -47,7 +47,8 @@ struct DevBoard {
     const uint32_t *y_edge;     // h-1
     const uint32_t *via_edge;   // layers-1
     const uint4 *directed;      // nullable: in-prices from -y, -x, +x, +y
-    uint32_t *planes;           // nullable: 6 x cells step prices (warp schedule; written by planes_kernel)
+    uint32_t *planes;           // nullable: 6 planes of step prices, rows padded (written by planes_kernel)
+    const void *tmap;           // nullable: TMA tensor map (CUtensorMap, 64-byte aligned) over `planes`
 };
 
 // One field = one net solved inside one window.

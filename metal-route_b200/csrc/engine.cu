@@ -6,6 +6,7 @@
 // computed by the kernels in relax.cu, and any device failure is returned as a
 // status so the caller can take its own CPU fallback (the contract of
 // crates/mr-cpu/src/negotiated.rs:539-553).
+#include <cuda.h>  // CUtensorMap and its encoder's types (the encoder is reached through the runtime)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -705,9 +706,11 @@ struct mrc_batch {
     uint32_t force_tile_h = 0, force_threads = 0, grid_num = 1, grid_div = 1;
     bool async_q = false;  // relax schedule: asynchronous work queue instead of rounds
     bool warp = false;     // the warp-per-tile schedule (implies the queue and a +inf-filled arena)
+    bool cta_planes = true;  // the CTA queue form stages step prices from the price planes by TMA
     size_t smem_floor = 0;
     std::vector<DevBoard> devs;  // the board table (step-price plane pointers patched in by batch_layout)
-    DBuf d_planes, d_pchunks;    // warp schedule: step-price planes of every board, chunk table of their kernel
+    DBuf d_planes, d_pchunks;    // step-price planes of every board, chunk table of their kernel
+    DBuf d_tmaps;                // one TMA tensor map per board over its planes (CTA queue form)
     uint64_t n_pchunks = 0;
     ~mrc_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -725,7 +728,7 @@ mrc_status choose_tile(mrc_context *ctx, uint32_t layers, bool directed, uint32_
     const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
     for (size_t budget : {(size_t)(75u << 10), (size_t)(110u << 10), hard}) {
         for (uint32_t th : {8u, 16u, 32u, 64u}) {
-            const size_t s = relax_smem_bytes(layers, th, directed);
+            const size_t s = std::max(relax_smem_bytes(layers, th, directed, true), relax_smem_bytes(layers, th, directed, false));
             if (s <= budget) {
                 *tile_h = th;
                 *smem = s;
@@ -738,6 +741,45 @@ mrc_status choose_tile(mrc_context *ctx, uint32_t layers, bool directed, uint32_
 
 uint32_t tune_key(uint32_t layers, bool directed) { return layers * 2u + (directed ? 1u : 0u); }
 
+// cuTensorMapEncodeTiled, looked up once through the runtime's driver entry
+// point (the library links only the CUDA runtime).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+mrc_status encode_fn(EncodeTiledFn *out) {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (err == cudaSuccess && q == cudaDriverEntryPointSuccess) fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    if (!fn) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "cuTensorMapEncodeTiled is not available");
+    *out = fn;
+    return MRC_OK;
+}
+
+// The tensor map of one board's price planes: u32 elements, dims {pitch, h,
+// layers, 6}, a box of kPlaneTmaBoxW x tile_h x layers x 6 (one tile's planes).
+mrc_status encode_planes_map(const DevBoard &d, uint32_t tile_h, CUtensorMap *map) {
+    EncodeTiledFn enc = nullptr;
+    MRC_TRY(encode_fn(&enc));
+    const uint64_t wp = planes_pitch(d.w);
+    const cuuint64_t dims[4] = {wp, d.h, d.layers, 6};
+    const cuuint64_t strides[3] = {wp * 4, wp * d.h * 4, wp * d.h * d.layers * 4};
+    const cuuint32_t box[4] = {kPlaneTmaBoxW, tile_h, d.layers, 6};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, d.planes, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MRC_ERR_BACKEND_UNAVAILABLE, "encode price-plane tensor map: error " +
+                                                                   std::to_string((int)r));
+    return MRC_OK;
+}
+
 // Tile-dependent layout of a staged batch: tile offsets, the CTA grid and the
 // per-tile buffers.  Re-run by the autotuner for every candidate.
 mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
@@ -748,9 +790,11 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     }
     if (bt->warp && bt->max_layers > kWarpMaxLayers) bt->warp = false;  // too many layers for one warp tile
     if (bt->warp) bt->async_q = true;
+    const bool cta_pl = bt->async_q && !bt->warp && bt->cta_planes;
     bt->tile_h = bt->warp ? kWarpTileH : tile_h;
     bt->threads = bt->warp ? warp_relax_threads() : threads;
-    bt->smem = bt->warp ? 0 : std::max(relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any), bt->smem_floor);
+    bt->smem =
+        bt->warp ? 0 : std::max(relax_smem_bytes(bt->max_layers, tile_h, bt->directed_any, cta_pl), bt->smem_floor);
     uint64_t toff = 0;
     uint32_t max_tiles = 1;
     for (DevField &f : bt->fields) {
@@ -767,22 +811,23 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     if (bt->warp) {
         MRC_CUDA(warp_relax_occupancy(&per_sm), "relax occupancy");
     } else {
-        MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q), "configure relax kernel");
-        MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q), "relax occupancy");
+        MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q, cta_pl), "configure relax kernel");
+        MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q, cta_pl), "relax occupancy");
     }
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
     bt->grid = std::max<uint32_t>(
         1u, (uint32_t)((uint64_t)ctx->sms * (uint32_t)per_sm * bt->grid_num / std::max(1u, bt->grid_div)));
-    // board table, with the step-price planes of every board for the warp schedule
-    if (bt->warp) {
+    // board table, with the step-price planes of every board (warp schedule,
+    // CTA queue form) and their tensor maps (CTA queue form)
+    if (bt->warp || cta_pl) {
         std::vector<uint64_t> poff(bt->devs.size()), chunks(bt->devs.size() + 1, 0);
         uint64_t total = 0;
         for (size_t k = 0; k < bt->devs.size(); ++k) {
             const DevBoard &d = bt->devs[k];
             const uint64_t cells = (uint64_t)d.w * d.h * d.layers;
             poff[k] = total;
-            total += (cells * 6 * 4 + 255) & ~(uint64_t)255;
+            total += ((uint64_t)planes_pitch(d.w) * d.h * d.layers * 6 * 4 + 255) & ~(uint64_t)255;
             chunks[k + 1] = chunks[k] + planes_chunks(cells);
         }
         MRC_TRY(bt->d_planes.get(ctx, std::max<uint64_t>(total, 256), "step-price planes"));
@@ -790,9 +835,23 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
             bt->devs[k].planes = reinterpret_cast<uint32_t *>(bt->d_planes.as<unsigned char>() + poff[k]);
         bt->n_pchunks = chunks.back();
         MRC_TRY(upload(ctx, bt->d_pchunks, chunks.data(), chunks.size() * 8, "plane chunk table"));
+        if (cta_pl) {
+            std::vector<CUtensorMap> maps(bt->devs.size());
+            for (size_t k = 0; k < bt->devs.size(); ++k) MRC_TRY(encode_planes_map(bt->devs[k], tile_h, &maps[k]));
+            // pool blocks are 256-byte aligned: every 128-byte map is 64-byte aligned
+            MRC_TRY(upload(ctx, bt->d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), "tensor maps"));
+            for (size_t k = 0; k < bt->devs.size(); ++k) bt->devs[k].tmap = bt->d_tmaps.as<CUtensorMap>() + k;
+        } else {
+            for (DevBoard &d : bt->devs) d.tmap = nullptr;
+            bt->d_tmaps.reset();
+        }
     } else {
-        for (DevBoard &d : bt->devs) d.planes = nullptr;
+        for (DevBoard &d : bt->devs) {
+            d.planes = nullptr;
+            d.tmap = nullptr;
+        }
         bt->d_planes.reset();
+        bt->d_tmaps.reset();
         bt->n_pchunks = 0;
     }
     MRC_TRY(upload(ctx, bt->d_boards, bt->devs.data(), bt->devs.size() * sizeof(DevBoard), "upload board table"));
@@ -828,6 +887,7 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         threads = tuned->second[1];
         bt->async_q = tuned->second[2] != 0;
         bt->warp = tuned->second[2] == 2;
+        bt->cta_planes = tuned->second[2] != 3;
     } else {
         MRC_TRY(choose_tile(ctx, bt->max_layers, bt->directed_any, &tile_h, &smem));
         bt->async_q = true;
@@ -939,14 +999,19 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
     if (n) {
         const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
         if (bt->ev0) MRC_CUDA(cudaEventRecordWithFlags(bt->ev0, st, rec), "record event");
-        if (bt->warp) {
+        const bool cta_pl = bt->async_q && !bt->warp && bt->cta_planes;
+        if (bt->warp || cta_pl) {
             MRC_CUDA(planes_launch(bt->d_boards.as<DevBoard>(), bt->d_pchunks.as<uint64_t>(),
                                    (uint32_t)bt->devs.size(), bt->n_pchunks, (uint32_t)bt->ctx->sms, st),
                      "launch step-price planes");
+            launches += 1;
+        }
+        if (bt->warp) {
             MRC_CUDA(warp_relax_launch(ra, bt->grid, st), "launch relax kernel");
-            launches += 3;  // planes, seeds, relax
+            launches += 2;  // seeds, relax
         } else {
-            MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q), "launch relax kernel");
+            MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q, cta_pl),
+                     "launch relax kernel");
             launches += bt->async_q ? 2 : 1;  // (+ the seed kernel)
         }
         if (bt->ev1) MRC_CUDA(cudaEventRecordWithFlags(bt->ev1, st, rec), "record event");
@@ -1486,17 +1551,18 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     MRC_CUDA(cudaEventCreate(&e1), "create event");
     float best = -1.0f;
     uint32_t best_th = batch->tile_h, best_nt = batch->threads;
-    uint32_t best_sched = batch->warp ? 2u : batch->async_q ? 1u : 0u;
+    uint32_t best_sched = batch->warp ? 2u : !batch->async_q ? 0u : batch->cta_planes ? 1u : 3u;
     mrc_status rc = MRC_OK;
     // candidates: (tile height, CTA width, schedule); the warp schedule has one shape
     std::vector<std::array<uint32_t, 3>> cands;
     if (layers <= kWarpMaxLayers) cands.push_back({kWarpTileH, warp_relax_threads(), 2u});
     for (uint32_t th : {8u, 16u, 32u, 64u}) {
-        if (relax_smem_bytes(layers, th, batch->directed_any) > hard) continue;
-        for (uint32_t cfg = 0; cfg < 4; ++cfg) {
-            const uint32_t nt = cfg & 1 ? 256u : 128u;
+        if (relax_smem_bytes(layers, th, batch->directed_any, true) > hard ||
+            relax_smem_bytes(layers, th, batch->directed_any, false) > hard)
+            continue;
+        for (uint32_t nt : {128u, 256u}) {
             if (4u * layers * th < nt / 2) continue;  // most lanes would idle in the line passes
-            cands.push_back({th, nt, (cfg & 2) ? 1u : 0u});
+            for (uint32_t sched : {0u, 1u, 3u}) cands.push_back({th, nt, sched});
         }
     }
     for (const auto &cand : cands) {
@@ -1504,6 +1570,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
             const uint32_t th = cand[0], nt = cand[1], sched = cand[2];
             batch->async_q = sched != 0;
             batch->warp = sched == 2;
+            batch->cta_planes = sched != 3;
             rc = batch_layout(batch, th, nt);
             if (rc != MRC_OK) break;
             float ms = 0.0f, sum = 0.0f;
@@ -1531,6 +1598,7 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
     if (rc != MRC_OK) return rc;
     batch->async_q = best_sched != 0;
     batch->warp = best_sched == 2;
+    batch->cta_planes = best_sched != 3;
     MRC_TRY(batch_layout(batch, best_th, best_nt));
     ctx->tuned[tune_key(layers, batch->directed_any)] = {best_th, best_nt, best_sched};
     if (tile_h) *tile_h = best_th;
@@ -1546,14 +1614,17 @@ mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t til
     Lock lock(ctx, 0);
     MRC_TRY(set_device(ctx));
     const size_t hard = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : (227u << 10), 227u << 10) - 1024;
-    if (relax_smem_bytes(batch->max_layers, tile_h, batch->directed_any) > hard)
+    if (relax_smem_bytes(batch->max_layers, tile_h, batch->directed_any, true) > hard ||
+        relax_smem_bytes(batch->max_layers, tile_h, batch->directed_any, false) > hard)
         return fail(MRC_ERR_LIMIT, "tile does not fit in shared memory");
     return batch_layout(batch, tile_h, threads);
 }
 
 mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule) {
     if (!ctx || !batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (schedule > 2) return fail(MRC_ERR_INVALID_ARGUMENT, "schedule must be 0 (rounds), 1 (queue) or 2 (warp tiles)");
+    if (schedule > 3)
+        return fail(MRC_ERR_INVALID_ARGUMENT,
+                    "schedule must be 0 (rounds), 1 (queue), 2 (warp tiles) or 3 (queue, prices computed per tile)");
     if (schedule == 2 && batch->max_layers > kWarpMaxLayers)
         return fail(MRC_ERR_LIMIT, "the warp schedule takes boards of at most 16 layers");
     Lock lock(ctx, 0);
@@ -1561,6 +1632,7 @@ mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t s
     const bool was_warp = batch->warp;
     batch->async_q = schedule >= 1;
     batch->warp = schedule == 2;
+    batch->cta_planes = schedule != 3;
     // leaving the warp schedule: the default CTA tile (8 rows, 256 threads)
     return batch_layout(batch, was_warp ? 8u : batch->tile_h, was_warp ? 256u : batch->threads);
 }
@@ -1577,7 +1649,7 @@ mrc_status mrc_batch_config(const mrc_batch *batch, uint32_t *tile_h, uint32_t *
     if (!batch) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
     if (tile_h) *tile_h = batch->tile_h;
     if (threads) *threads = batch->threads;
-    if (schedule) *schedule = batch->warp ? 2u : batch->async_q ? 1u : 0u;
+    if (schedule) *schedule = batch->warp ? 2u : !batch->async_q ? 0u : batch->cta_planes ? 1u : 3u;
     return MRC_OK;
 }
 
@@ -2380,10 +2452,10 @@ mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, 
         s->budget = allowed > 0 ? (size_t)allowed : 0;
         s->tile_h = 8;
         s->threads = kRelaxThreads;
-        s->smem_floor = relax_smem_bytes(s->p.max_layers, s->tile_h, true);
+        s->smem_floor = relax_smem_bytes(s->p.max_layers, s->tile_h, true, true);
         int per_sm = 0;
-        MRC_CUDA(relax_configure(s->tile_h, s->threads, s->smem_floor, true), "configure relax kernel");
-        MRC_CUDA(relax_occupancy(s->tile_h, s->threads, s->smem_floor, &per_sm, true), "relax occupancy");
+        MRC_CUDA(relax_configure(s->tile_h, s->threads, s->smem_floor, true, true), "configure relax kernel");
+        MRC_CUDA(relax_occupancy(s->tile_h, s->threads, s->smem_floor, &per_sm, true, true), "relax occupancy");
         if ((uint32_t)per_sm * (uint32_t)ctx->sms < s->p.slots) return fail(MRC_ERR_LIMIT, "too many slots");
         s->streams.resize(s->p.slots);
         s->staged.resize(s->p.slots);

@@ -134,20 +134,29 @@ cudaError_t warp_relax_occupancy(int *blocks_per_sm);
 cudaError_t warp_relax_launch(const RelaxArgs &a, uint32_t grid, cudaStream_t st);
 // Step-price planes of every board of a batch (DevBoard::planes, 6 x cells u32
 // each); chunk_start[k] = first chunk of board k (prefix sum of planes_chunks).
+// Columns of the TMA box that brings one tile's price planes to shared memory:
+// the tile's 32 columns plus the slack of rounding its first column down to a
+// multiple of 4 (16 bytes, the TMA rule for the innermost coordinate).
+constexpr uint32_t kPlaneTmaBoxW = 36;
+// Rows of a price plane are padded to a multiple of 4 cells (16 bytes), so a
+// tensor map over the planes has 16-byte strides.
+__host__ __device__ inline uint32_t planes_pitch(uint32_t w) { return (w + 3u) & ~3u; }
 uint64_t planes_chunks(uint64_t cells);
 cudaError_t planes_launch(const DevBoard *boards, const uint64_t *chunk_start, uint32_t n_boards, uint64_t n_chunks,
                           uint32_t sms, cudaStream_t st);
 
-// Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}).
-size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed);
+// Shared memory of one tile of 32 x tile_h cells over `layers` (tile_h in {8, 16, 32, 64}); `planes`: the
+// queue form that stages the step prices from the boards' price planes by TMA (DevBoard::planes, ::tmap).
+size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed, bool planes = false);
 // The relax kernel is instantiated for threads in {128, 256} per CTA.
 // `async` selects the queue-driven form (relax_async_kernel) over the
 // bulk-synchronous rounds (relax_rounds_kernel); the async form needs the label
 // arena filled with 0xFF and the queue tags (lists[cap, 2 cap)) zeroed.
-cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async = false);
-cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async = false);
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async = false, bool planes = false);
+cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async = false,
+                            bool planes = false);
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
-                         bool async = false);
+                         bool async = false, bool planes = false);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);

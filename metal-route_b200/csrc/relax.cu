@@ -44,6 +44,37 @@ constexpr uint32_t kStPitch = 32;
 constexpr uint32_t kFlPitch = 36;  // flag bytes per staged row (34 used)
 constexpr int kStageUnroll = 4;    // cells whose loads one thread issues together
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kTmaSpinLimit = 1u << 22;
+
+// ---- TMA and mbarrier primitives (sm_90+ PTX) ---------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy (TMA) writes to the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// One tiled 4-D TMA load (coordinates innermost first) completing on `bar`.
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~ seconds with the backoff below
 
 // Asynchronous 4-byte global -> shared copy (cp.async, L1-allocating) and its
@@ -63,30 +94,38 @@ enum { kFromNegX = 0, kFromPosX = 1, kFromNegY = 2, kFromPosY = 3, kFromBelow = 
 template <int TH>
 struct Tile {
     u64 *lab;        // [L][TH+2][34] labels with a one-cell halo ring
-    uint32_t *st;    // [6][L][TH][32] step prices into interior cells
+    uint32_t *st;    // [6][L][TH][sp] step prices into interior cells (column x at sp-offset xo + x)
     uint8_t *rowd;   // [L][TH] row needs a sweep
     uint8_t *cold;   // [L][32] column needs a sweep
     uint8_t *stackd; // [TH][32] layer stack needs a sweep
-    uint8_t *fl;     // [L][TH+2][kFlPitch] board flag bytes of the tile and its halo
+    uint32_t *fellw; // [L][TH] bit x: the label of (l, y, x) fell in this activation
+    uint8_t *fl;     // [L][TH+2][kFlPitch] board flag bytes of the tile and its halo (computed prices only)
     uint32_t L;
+    uint32_t sp, xo; // price row pitch and column offset: 32, 0 computed; kPlaneTmaBoxW, tx0 & 3 from the planes
     __device__ __forceinline__ uint32_t li(uint32_t l, uint32_t sy, uint32_t sx) const {
         return (l * (TH + 2) + sy) * kLabPitch + sx;
     }
     __device__ __forceinline__ uint32_t si(uint32_t plane, uint32_t l, uint32_t y, uint32_t x) const {
-        return ((plane * L + l) * TH + y) * kStPitch + x;
+        return ((plane * L + l) * TH + y) * sp + x + xo;
+    }
+    __device__ __forceinline__ void fell(uint32_t l, uint32_t y, uint32_t x) const {
+        atomicOr(&fellw[l * TH + y], 1u << x);
     }
     // a label of interior cell (l, y, x) fell: every other line through it must be swept again
     __device__ __forceinline__ void touched_by_row(uint32_t l, uint32_t y, uint32_t x) const {
         cold[l * 32 + x] = 1;
         stackd[y * 32 + x] = 1;
+        fell(l, y, x);
     }
     __device__ __forceinline__ void touched_by_col(uint32_t l, uint32_t y, uint32_t x) const {
         rowd[l * TH + y] = 1;
         stackd[y * 32 + x] = 1;
+        fell(l, y, x);
     }
     __device__ __forceinline__ void touched_by_stack(uint32_t l, uint32_t y, uint32_t x) const {
         rowd[l * TH + y] = 1;
         cold[l * 32 + x] = 1;
+        fell(l, y, x);
     }
 };
 
@@ -394,9 +433,30 @@ __device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
 
 // One (field, tile) item: stage the tile and its halo, relax it to local
 // convergence, write it back and queue the neighbours it improves.
-template <int TH, bool ASYNC>
+// Shared-memory layout of one staged tile (relax_smem_bytes sizes it the same way).
+struct TileLayout {
+    size_t st, rowd, fellw, fl, total;
+};
+__host__ __device__ inline TileLayout tile_layout(uint32_t L, uint32_t TH, bool planes) {
+    TileLayout o;
+    const size_t sp = planes ? kPlaneTmaBoxW : kStPitch;
+    o.st = ((size_t)L * (TH + 2) * kLabPitch * 8 + 127) & ~(size_t)127;  // TMA destination: 128-byte aligned
+    o.rowd = o.st + (size_t)6 * L * TH * sp * 4;
+    o.fellw = (o.rowd + (size_t)L * TH + (size_t)L * kTW + (size_t)TH * kTW + 3) & ~(size_t)3;
+    o.fl = o.fellw + (size_t)L * TH * 4;
+    o.total = o.fl + (planes ? 0 : (size_t)L * (TH + 2) * kFlPitch);
+    return o;
+}
+
+// With PL the tile's six step-price planes come from the board's precomputed
+// planes (planes_kernel) in one TMA load: box kPlaneTmaBoxW x TH x L x 6 at column
+// tx0 rounded down to 4 (a TMA x coordinate times 4 bytes must be a multiple
+// of 16; the tile's columns then start at xo = tx0 & 3 in the box).  Cells past
+// the window and the stacks of the net's endpoints, own pads and via pads are
+// then priced exactly (exact_in_price); the push checks read the planes.
+template <int TH, bool ASYNC, bool PL>
 __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, uint32_t t, uint32_t round,
-                                             unsigned char *smem_raw) {
+                                             unsigned char *smem_raw, uint64_t *mbar, uint32_t &tma_phase) {
     const uint32_t SW = kTW + 2, SH = TH + 2;
     Tile<TH> tile;
     __shared__ uint32_t s_push[4];
@@ -409,16 +469,29 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     const DevBoard b = a.boards[f.board];
     const uint32_t L = b.layers;  // the shared tile is laid out for this board's layers
     const uint32_t nsm = L * SH * SW;  // staged cells (pitch kLabPitch in smem)
-    tile.lab = reinterpret_cast<u64 *>(smem_raw);
-    tile.st = reinterpret_cast<uint32_t *>(tile.lab + L * SH * kLabPitch);
-    tile.rowd = reinterpret_cast<uint8_t *>(tile.st + 6 * L * TH * kStPitch);
-    tile.cold = tile.rowd + L * TH;
-    tile.stackd = tile.cold + L * kTW;
-    tile.fl = tile.stackd + TH * kTW;
-    tile.L = L;
     const uint32_t ntx = (f.ww + kTW - 1) / kTW, nty = (f.wh + TH - 1) / TH;
     const uint32_t txi = t % ntx, tyi = t / ntx;
     const int tx0 = (int)(f.x0 + txi * kTW), ty0 = (int)(f.y0 + tyi * TH);
+    const TileLayout lay = tile_layout(L, TH, PL);
+    tile.lab = reinterpret_cast<u64 *>(smem_raw);
+    tile.st = reinterpret_cast<uint32_t *>(smem_raw + lay.st);
+    tile.rowd = smem_raw + lay.rowd;
+    tile.cold = tile.rowd + L * TH;
+    tile.stackd = tile.cold + L * kTW;
+    tile.fellw = reinterpret_cast<uint32_t *>(smem_raw + lay.fellw);
+    tile.fl = smem_raw + lay.fl;
+    tile.L = L;
+    tile.sp = PL ? kPlaneTmaBoxW : kStPitch;
+    tile.xo = PL ? ((uint32_t)tx0 & 3u) : 0u;
+    if constexpr (PL) {
+        // every thread is past the previous item (the caller's barrier): the
+        // planes of this tile go global -> shared while the labels are staged
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            mbar_expect_tx(mbar, 6u * L * TH * kPlaneTmaBoxW * 4u);
+            tma_load_4d(tile.st, b.tmap, tx0 & ~3, ty0, 0, 0, mbar);
+        }
+    }
     const uint32_t tw = min(kTW, f.ww - txi * kTW), th = min(TH, f.wh - tyi * TH);
     const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
     const u64 *lab = a.lab + f.lab_off;
@@ -456,6 +529,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     // +inf labels with +inf ends cannot change until a crossing line lowers one
     // of its cells, and that pass marks it.
     for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 0;
+    for (uint32_t i = tid; i < L * TH; i += blockDim.x) tile.fellw[i] = 0;
     __syncthreads();
 
     // ---- step prices into every interior cell: phase 1 -----------------
@@ -464,33 +538,35 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     // first, so they overlap the label and flag loads below.  The board is
     // read-only during the launch, so the L1-allocating cp.async is safe for it
     // (labels, which other CTAs write, keep their L2-only loads).
-    const uint32_t ncell = L * TH * kTW;
-    for (uint32_t i = tid; i < ncell; i += blockDim.x) {
-        const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-        const int gx = tx0 + (int)x, gy = ty0 + (int)y;
-        uint32_t *d0 = &tile.st[tile.si(kFromNegX, l, y, x)], *d1 = &tile.st[tile.si(kFromPosX, l, y, x)];
-        uint32_t *d2 = &tile.st[tile.si(kFromNegY, l, y, x)], *d3 = &tile.st[tile.si(kFromPosY, l, y, x)];
-        uint32_t *dc = &tile.st[tile.si(kFromBelow, l, y, x)];
-        if (gx < wx1 && gy < wy1) {
-            const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-            cp_async4(dc, b.cost + gc);
-            if (b.directed) {
-                const uint32_t *dp = reinterpret_cast<const uint32_t *>(b.directed + gc);
-                cp_async4(d0, dp + 1);  // from -x
-                cp_async4(d1, dp + 2);  // from +x
-                cp_async4(d2, dp + 0);  // from -y
-                cp_async4(d3, dp + 3);  // from +y
+    if constexpr (!PL) {  // with the planes the prices arrive by TMA
+        const uint32_t ncell = L * TH * kTW;
+        for (uint32_t i = tid; i < ncell; i += blockDim.x) {
+            const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+            const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+            uint32_t *d0 = &tile.st[tile.si(kFromNegX, l, y, x)], *d1 = &tile.st[tile.si(kFromPosX, l, y, x)];
+            uint32_t *d2 = &tile.st[tile.si(kFromNegY, l, y, x)], *d3 = &tile.st[tile.si(kFromPosY, l, y, x)];
+            uint32_t *dc = &tile.st[tile.si(kFromBelow, l, y, x)];
+            if (gx < wx1 && gy < wy1) {
+                const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                cp_async4(dc, b.cost + gc);
+                if (b.directed) {
+                    const uint32_t *dp = reinterpret_cast<const uint32_t *>(b.directed + gc);
+                    cp_async4(d0, dp + 1);  // from -x
+                    cp_async4(d1, dp + 2);  // from +x
+                    cp_async4(d2, dp + 0);  // from -y
+                    cp_async4(d3, dp + 3);  // from +y
+                } else {
+                    *d0 = gx > wx0 ? __ldg(b.x_edge + gx - 1) : kMax;
+                    *d1 = gx + 1 < wx1 ? __ldg(b.x_edge + gx) : kMax;
+                    *d2 = gy > wy0 ? __ldg(b.y_edge + gy - 1) : kMax;
+                    *d3 = gy + 1 < wy1 ? __ldg(b.y_edge + gy) : kMax;
+                }
             } else {
-                *d0 = gx > wx0 ? __ldg(b.x_edge + gx - 1) : kMax;
-                *d1 = gx + 1 < wx1 ? __ldg(b.x_edge + gx) : kMax;
-                *d2 = gy > wy0 ? __ldg(b.y_edge + gy - 1) : kMax;
-                *d3 = gy + 1 < wy1 ? __ldg(b.y_edge + gy) : kMax;
+                *d0 = *d1 = *d2 = *d3 = *dc = kMax;
             }
-        } else {
-            *d0 = *d1 = *d2 = *d3 = *dc = kMax;
         }
+        cp_async_commit();
     }
-    cp_async_commit();
 
     // ---- stage labels and flag bytes (tile + halo ring) ---------------
     // Every thread issues the loads of kStageUnroll cells before it
@@ -525,7 +601,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
                     if (owner < 5 && s_vis[owner]) lv[k] = __ldcg(lab + lc);
                     else if (owner == 0 && gcell == f.src) lv[k] = 0;  // first visit of the source tile
                 }
-                if (b.flags) fv[k] = __ldg(b.flags + gcell);
+                if (!PL && b.flags) fv[k] = __ldg(b.flags + gcell);
             }
         }
 #pragma unroll
@@ -534,7 +610,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             if (i >= nsm) continue;
             const uint32_t sx = i % SW, r = i / SW, sy = r % SH, l = r / SH;
             tile.lab[tile.li(l, sy, sx)] = lv[k];
-            tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
+            if (!PL) tile.fl[(l * SH + sy) * kFlPitch + sx] = fv[k];
             if (lv[k] != kInf) {
                 const bool row_in = sy >= 1 && sy <= TH, col_in = sx >= 1 && sx <= kTW;
                 if (row_in) tile.rowd[l * TH + sy - 1] = 1;
@@ -543,55 +619,110 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             }
         }
     }
-    cp_async_wait_all();  // the board words copied before the label loop
-    __syncthreads();
-    // Phase 2: every step price from the staged bytes (own pads and via
-    // exemptions are the only global reads left).
-    for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
-        const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
-        const int gx = tx0 + (int)x, gy = ty0 + (int)y;
-        uint32_t s0 = kMax, s1 = kMax, s2 = kMax, s3 = kMax, s4 = kMax, s5 = kMax;
-        if (gx < wx1 && gy < wy1) {
-            const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
-            const uint8_t *flr = tile.fl + (l * SH + y + 1) * kFlPitch + x + 1;  // this cell
-            const uint8_t fc = flr[0];
-            const uint32_t cost = tile.st[tile.si(kFromBelow, l, y, x)];
-            uint32_t ec;  // cell_enter on staged values
-            if (fc & kTraceNode) ec = kMax;
-            else if (cost != kMax) ec = cost;
-            else ec = is_own_pad(gc) ? 1u : kMax;
-            if (ec != kMax) {
-                const bool dir = b.directed != nullptr;
-                auto planar = [&](uint32_t base, uint8_t fp, uint8_t out_bit, uint8_t in_bit) -> uint32_t {
-                    if (dir && base == kMax) return kMax;  // blocked directed edge
-                    if ((fp & out_bit) | (fc & in_bit)) return kMax;
-                    return capmul(base, ec);
-                };
-                if (gx > wx0) s0 = planar(tile.st[tile.si(kFromNegX, l, y, x)], flr[-1], kEdgePosX, kEdgeNegX);
-                if (gx + 1 < wx1) s1 = planar(tile.st[tile.si(kFromPosX, l, y, x)], flr[1], kEdgeNegX, kEdgePosX);
-                if (gy > wy0)
-                    s2 = planar(tile.st[tile.si(kFromNegY, l, y, x)], flr[-(int)kFlPitch], kEdgePosY, kEdgeNegY);
-                if (gy + 1 < wy1)
-                    s3 = planar(tile.st[tile.si(kFromPosY, l, y, x)], flr[kFlPitch], kEdgeNegY, kEdgePosY);
-                if (L > 1) {
-                    const bool vc = via_blk(gc, fc);
-                    if (l > 0 && ((b.via_mask >> (l - 1)) & 1u) && !vc) {
-                        const uint8_t fq = flr[-(int)(SH * kFlPitch)];
-                        if (!via_blk(gc - plane, fq)) s4 = capmul(__ldg(b.via_edge + l - 1), ec);
-                    }
-                    if (l + 1 < L && ((b.via_mask >> l) & 1u) && !vc) {
-                        const uint8_t fq = flr[SH * kFlPitch];
-                        if (!via_blk(gc + plane, fq)) s5 = capmul(__ldg(b.via_edge + l), ec);
-                    }
+    if constexpr (PL) {
+        // the planes: a bounded wait for the TMA load (a load that never lands
+        // sets the status and the launch ends without results)
+        for (uint32_t spins = 0; !mbar_try_wait(mbar, tma_phase & 1u); ++spins) {
+            if (spins == kTmaSpinLimit) {
+                if (tid == 0) atomicOr(&ctl->status, kStatusQueueOverflow);
+            } else if (spins > 2 * kTmaSpinLimit) {
+                break;
+            }
+        }
+        ++tma_phase;
+        // cells past the window: no step enters them
+        if (tw < kTW || th < TH) {
+            for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
+                const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+                if (x < tw && y < th) continue;
+#pragma unroll
+                for (int p = 0; p < 6; ++p) tile.st[tile.si(p, l, y, x)] = kMax;
+            }
+        }
+        // stacks whose prices depend on this net: its endpoints, own pads and
+        // via pads, priced exactly on every layer
+        auto exact_stack = [&](uint32_t c) {
+            const uint32_t r = c % (b.w * b.h), gy = r / b.w, gx = r - gy * b.w;
+            if (gx < (uint32_t)tx0 || gx >= (uint32_t)tx0 + tw || gy < (uint32_t)ty0 || gy >= (uint32_t)ty0 + th)
+                return;
+            for (uint32_t l = 0; l < L; ++l) {
+                const uint32_t cl = (l * b.h + gy) * b.w + gx;
+                for (int p = 0; p < 6; ++p)
+                    tile.st[tile.si(p, l, gy - ty0, gx - tx0)] = exact_in_price(b, f, a.pads, p, cl, l, gy, gx);
+            }
+        };
+        if (tid == 0) exact_stack(f.src);
+        if (tid == 1) exact_stack(f.dst);
+        if (f.n_pads | f.n_vpads) {
+            for (uint32_t j = tid; j < 2 * L * th; j += blockDim.x) {
+                const uint32_t q = j & 1u, r = j >> 1, l = r / th, y = r - l * th;
+                const uint32_t lo_c = (l * b.h + ty0 + y) * b.w + tx0, hi_c = lo_c + tw;
+                const uint32_t *list = a.pads + (q ? f.vpad_off : f.pad_off);
+                const uint32_t n = q ? f.n_vpads : f.n_pads;
+                uint32_t lo = 0, hi = n;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (__ldg(list + mid) < lo_c) lo = mid + 1;
+                    else hi = mid;
+                }
+                for (; lo < n; ++lo) {
+                    const uint32_t c = __ldg(list + lo);
+                    if (c >= hi_c) break;
+                    exact_stack(c);
                 }
             }
         }
-        tile.st[tile.si(kFromNegX, l, y, x)] = s0;
-        tile.st[tile.si(kFromPosX, l, y, x)] = s1;
-        tile.st[tile.si(kFromNegY, l, y, x)] = s2;
-        tile.st[tile.si(kFromPosY, l, y, x)] = s3;
-        tile.st[tile.si(kFromBelow, l, y, x)] = s4;
-        tile.st[tile.si(kFromAbove, l, y, x)] = s5;
+    } else {
+        cp_async_wait_all();  // the board words copied before the label loop
+        __syncthreads();
+        // Phase 2: every step price from the staged bytes (own pads and via
+        // exemptions are the only global reads left).
+        for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
+            const uint32_t x = i % kTW, r = i / kTW, y = r % TH, l = r / TH;
+            const int gx = tx0 + (int)x, gy = ty0 + (int)y;
+            uint32_t s0 = kMax, s1 = kMax, s2 = kMax, s3 = kMax, s4 = kMax, s5 = kMax;
+            if (gx < wx1 && gy < wy1) {
+                const uint32_t gc = (l * b.h + (uint32_t)gy) * b.w + (uint32_t)gx;
+                const uint8_t *flr = tile.fl + (l * SH + y + 1) * kFlPitch + x + 1;  // this cell
+                const uint8_t fc = flr[0];
+                const uint32_t cost = tile.st[tile.si(kFromBelow, l, y, x)];
+                uint32_t ec;  // cell_enter on staged values
+                if (fc & kTraceNode) ec = kMax;
+                else if (cost != kMax) ec = cost;
+                else ec = is_own_pad(gc) ? 1u : kMax;
+                if (ec != kMax) {
+                    const bool dir = b.directed != nullptr;
+                    auto planar = [&](uint32_t base, uint8_t fp, uint8_t out_bit, uint8_t in_bit) -> uint32_t {
+                        if (dir && base == kMax) return kMax;  // blocked directed edge
+                        if ((fp & out_bit) | (fc & in_bit)) return kMax;
+                        return capmul(base, ec);
+                    };
+                    if (gx > wx0) s0 = planar(tile.st[tile.si(kFromNegX, l, y, x)], flr[-1], kEdgePosX, kEdgeNegX);
+                    if (gx + 1 < wx1) s1 = planar(tile.st[tile.si(kFromPosX, l, y, x)], flr[1], kEdgeNegX, kEdgePosX);
+                    if (gy > wy0)
+                        s2 = planar(tile.st[tile.si(kFromNegY, l, y, x)], flr[-(int)kFlPitch], kEdgePosY, kEdgeNegY);
+                    if (gy + 1 < wy1)
+                        s3 = planar(tile.st[tile.si(kFromPosY, l, y, x)], flr[kFlPitch], kEdgeNegY, kEdgePosY);
+                    if (L > 1) {
+                        const bool vc = via_blk(gc, fc);
+                        if (l > 0 && ((b.via_mask >> (l - 1)) & 1u) && !vc) {
+                            const uint8_t fq = flr[-(int)(SH * kFlPitch)];
+                            if (!via_blk(gc - plane, fq)) s4 = capmul(__ldg(b.via_edge + l - 1), ec);
+                        }
+                        if (l + 1 < L && ((b.via_mask >> l) & 1u) && !vc) {
+                            const uint8_t fq = flr[SH * kFlPitch];
+                            if (!via_blk(gc + plane, fq)) s5 = capmul(__ldg(b.via_edge + l), ec);
+                        }
+                    }
+                }
+            }
+            tile.st[tile.si(kFromNegX, l, y, x)] = s0;
+            tile.st[tile.si(kFromPosX, l, y, x)] = s1;
+            tile.st[tile.si(kFromNegY, l, y, x)] = s2;
+            tile.st[tile.si(kFromPosY, l, y, x)] = s3;
+            tile.st[tile.si(kFromBelow, l, y, x)] = s4;
+            tile.st[tile.si(kFromAbove, l, y, x)] = s5;
+        }
     }
     __syncthreads();
 
@@ -613,10 +744,13 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     u64 *labw = a.lab + f.lab_off;
     // the tile is held by this CTA alone (both schedules), so plain stores;
     // indices are split by the compile-time tile shape (cells past a ragged
-    // window edge are skipped)
+    // window edge are skipped).  Only labels that fell are stored, unless the
+    // arena holds nothing valid for this tile yet (first visit, rounds form).
+    const bool all_labels = !ASYNC && !s_vis[0];
     for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
         const uint32_t tx = i % kTW, r = i / kTW, ty = r % TH, l = r / TH;
         if (tx >= tw || ty >= th) continue;
+        if (!all_labels && !((tile.fellw[l * TH + ty] >> tx) & 1u)) continue;
         const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
         labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
     }
@@ -662,6 +796,17 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         if (!exists || s_push[side]) continue;
         const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
         if (lb == kInf) continue;
+        if constexpr (PL) {
+            // the planes hold the price into the neighbour cell; an own pad or
+            // endpoint of this net there is priced exactly
+            const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
+            const int pin = side == 0 ? kInPosX : side == 1 ? kInNegX : side == 2 ? kInPosY : kInNegY;
+            const uint32_t wp = planes_pitch(b.w);
+            uint32_t step = __ldg(b.planes + (uint64_t)pin * wp * b.h * L + ((uint64_t)l * b.h + gy_n) * wp + gx_n);
+            if (step == kMax) step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
+            if (ext2(lb, step, 1) < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
+            continue;
+        }
         const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
         const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
         const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
@@ -725,7 +870,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
 
 template <int TH, int NT>
 __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ u64 s_item;
     Ctl *ctl = a.ctl;
     const uint32_t tid = threadIdx.x;
@@ -769,7 +914,9 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             __syncthreads();
             const u64 item = s_item;
             if (item == kInf) break;
-            process_item<TH, false>(a, (uint32_t)(item >> 32), (uint32_t)item, round, smem_raw);
+            uint32_t no_phase = 0;
+            process_item<TH, false, false>(a, (uint32_t)(item >> 32), (uint32_t)item, round, smem_raw, nullptr,
+                                           no_phase);
         }
         grid_barrier(ctl, gridDim.x);
     }
@@ -780,16 +927,26 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
 // queued or in flight.  The label arena is +inf-initialised (every label is
 // valid from the start), and a tile is held by one CTA at a time: improvements
 // that reach a held tile mark it dirty and its holder queues it once more.
-template <int TH, int NT>
-__global__ void __launch_bounds__(NT) relax_async_kernel(RelaxArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// 64 registers a thread: four 256-thread CTAs per SM
+template <int TH, int NT, bool PL>
+__global__ void __launch_bounds__(NT, 65536 / (NT * 64)) relax_async_kernel(RelaxArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ u64 s_item;
+    __shared__ __align__(8) uint64_t s_mbar;  // completion of the price-plane TMA loads (PL)
+    uint32_t tma_phase = 0;
+    if (PL) {
+        if (threadIdx.x == 0) {
+            mbar_init(&s_mbar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
     for (;;) {
         if (threadIdx.x == 0) s_item = async_pop(a);
         __syncthreads();
         const u64 item = s_item;
         if (item == kInf) break;
-        process_item<TH, true>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw);
+        process_item<TH, true, PL>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw, &s_mbar, tma_phase);
     }
 }
 
@@ -1226,27 +1383,28 @@ cudaError_t combine_flags_launch(uint8_t *flags, const uint8_t *via_forbidden, u
     return cudaGetLastError();
 }
 
-size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed) {
+size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed, bool planes) {
     (void)directed;  // directed prices are folded into the step planes
-    return (size_t)layers * (tile_h + 2) * kLabPitch * 8 + (size_t)6 * layers * tile_h * kStPitch * 4 +
-           (size_t)layers * tile_h + (size_t)layers * kTW + (size_t)tile_h * kTW +
-           (size_t)layers * (tile_h + 2) * kFlPitch;
+    return tile_layout(layers, tile_h, planes).total;
 }
 
 namespace {
 template <int TH>
-const void *relax_fn_th(bool wide, bool async) {
-    if (async) return wide ? (const void *)relax_async_kernel<TH, 256> : (const void *)relax_async_kernel<TH, 128>;
+const void *relax_fn_th(bool wide, bool async, bool planes) {
+    if (async && planes)
+        return wide ? (const void *)relax_async_kernel<TH, 256, true> : (const void *)relax_async_kernel<TH, 128, true>;
+    if (async)
+        return wide ? (const void *)relax_async_kernel<TH, 256, false> : (const void *)relax_async_kernel<TH, 128, false>;
     return wide ? (const void *)relax_rounds_kernel<TH, 256> : (const void *)relax_rounds_kernel<TH, 128>;
 }
 
-const void *relax_fn(uint32_t tile_h, uint32_t threads, bool async) {
+const void *relax_fn(uint32_t tile_h, uint32_t threads, bool async, bool planes) {
     const bool wide = threads >= 256;
     switch (tile_h) {
-        case 8: return relax_fn_th<8>(wide, async);
-        case 16: return relax_fn_th<16>(wide, async);
-        case 32: return relax_fn_th<32>(wide, async);
-        default: return relax_fn_th<64>(wide, async);
+        case 8: return relax_fn_th<8>(wide, async, planes);
+        case 16: return relax_fn_th<16>(wide, async, planes);
+        case 32: return relax_fn_th<32>(wide, async, planes);
+        default: return relax_fn_th<64>(wide, async, planes);
     }
 }
 
@@ -1260,18 +1418,19 @@ const void *seed_fn(uint32_t tile_h) {
 }
 }  // namespace
 
-cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async) {
-    return cudaFuncSetAttribute(relax_fn(tile_h, threads, async), cudaFuncAttributeMaxDynamicSharedMemorySize,
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async, bool planes) {
+    return cudaFuncSetAttribute(relax_fn(tile_h, threads, async, planes), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem);
 }
 
-cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h, threads, async),
+cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async,
+                            bool planes) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h, threads, async, planes),
                                                          (int)threads, smem);
 }
 
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
-                         bool async) {
+                         bool async, bool planes) {
     RelaxArgs copy = a;
     void *args[] = {&copy};
     if (async) {
@@ -1281,7 +1440,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
             cudaError_t e = cudaLaunchKernel(seed_fn(a.tile_h), dim3((a.n_fields + 255) / 256), dim3(256), args, 0, st);
             if (e != cudaSuccess) return e;
         }
-        return cudaLaunchKernel(relax_fn(a.tile_h, threads, true), dim3(grid), dim3(threads), args, smem, st);
+        return cudaLaunchKernel(relax_fn(a.tile_h, threads, true, planes), dim3(grid), dim3(threads), args, smem, st);
     }
     // Cooperative (all CTAs co-resident, checked by the CUDA runtime against occupancy);
     // the attribute form is also what stream capture records as a graph node.
@@ -1295,7 +1454,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, relax_fn(a.tile_h, threads, false), args);
+    return cudaLaunchKernelExC(&cfg, relax_fn(a.tile_h, threads, false, false), args);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {

@@ -107,4 +107,60 @@ __device__ __forceinline__ u64 async_pop(const RelaxArgs &a) {
     }
 }
 
+// Planes of step prices into a cell: from -x, +x, -y, +y, the layer below, the
+// layer above (the order of the price planes and of a staged tile's planes).
+enum { kInNegX = 0, kInPosX = 1, kInNegY = 2, kInPosY = 3, kInBelow = 4, kInAbove = 5 };
+
+// Exact price of the step into cell c (at l, y, x) from direction `dir`, with
+// the net's own pads, endpoints and via exemptions (the staging rules of the
+// CTA-wide relax kernel without price planes, negotiated.rs:2914-2966 and :3010-3043).
+static __device__ __noinline__ uint32_t exact_in_price(const DevBoard &b, const DevField &f, const uint32_t *pads, int dir, uint32_t c,
+                                   uint32_t l, uint32_t y, uint32_t x) {
+    const uint8_t fc = b.flags ? __ldg(b.flags + c) : 0;
+    const uint32_t ec = cell_enter(b, f, pads, c, fc);
+    if (ec == kMax) return kMax;
+    const uint32_t plane = b.w * b.h;
+    if (dir == kInBelow || dir == kInAbove) {
+        const bool below = dir == kInBelow;
+        if (below ? l == 0 : l + 1 >= b.layers) return kMax;
+        const uint32_t k = below ? l - 1 : l;
+        if (!((b.via_mask >> k) & 1u)) return kMax;
+        const uint32_t p = below ? c - plane : c + plane;
+        const uint8_t fp = b.flags ? __ldg(b.flags + p) : 0;
+        if ((cell_tile_flags(f, pads, c, fc) | cell_tile_flags(f, pads, p, fp)) & kViaBlocked) return kMax;
+        return capmul(__ldg(b.via_edge + k), ec);
+    }
+    uint32_t p, base;
+    uint8_t out_bit, in_bit;
+    if (dir == kInNegX) {
+        if (x == 0) return kMax;
+        p = c - 1;
+        base = b.directed ? __ldg(b.directed + c).y : __ldg(b.x_edge + x - 1);
+        out_bit = kEdgePosX;
+        in_bit = kEdgeNegX;
+    } else if (dir == kInPosX) {
+        if (x + 1 >= b.w) return kMax;
+        p = c + 1;
+        base = b.directed ? __ldg(b.directed + c).z : __ldg(b.x_edge + x);
+        out_bit = kEdgeNegX;
+        in_bit = kEdgePosX;
+    } else if (dir == kInNegY) {
+        if (y == 0) return kMax;
+        p = c - b.w;
+        base = b.directed ? __ldg(b.directed + c).x : __ldg(b.y_edge + y - 1);
+        out_bit = kEdgePosY;
+        in_bit = kEdgeNegY;
+    } else {
+        if (y + 1 >= b.h) return kMax;
+        p = c + b.w;
+        base = b.directed ? __ldg(b.directed + c).w : __ldg(b.y_edge + y);
+        out_bit = kEdgeNegY;
+        in_bit = kEdgePosY;
+    }
+    const uint8_t fp = b.flags ? __ldg(b.flags + p) : 0;
+    if ((fp & out_bit) | (fc & in_bit)) return kMax;
+    if (b.directed && base == kMax) return kMax;
+    return capmul(base, ec);
+}
+
 }  // namespace mrc

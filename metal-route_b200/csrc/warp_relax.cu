@@ -45,8 +45,7 @@ constexpr int TH = kWarpTileH;     // rows per tile
 constexpr int NW = 4;              // warps per CTA
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 constexpr uint64_t kPlaneChunk = 8192;
-
-enum { kInNegX = 0, kInPosX = 1, kInNegY = 2, kInPosY = 3, kInBelow = 4, kInAbove = 5 };
+constexpr uint32_t kMaxRounds = 8;  // relaxation rounds of one activation (see warp_item)
 
 // ---- step-price planes ------------------------------------------------------
 
@@ -64,6 +63,8 @@ __global__ void __launch_bounds__(256) planes_kernel(const DevBoard *boards, con
         const DevBoard b = boards[lo];
         const uint32_t plane = b.w * b.h;
         const uint64_t N = (uint64_t)plane * b.layers;
+        const uint32_t wp = planes_pitch(b.w);
+        const uint64_t NP = (uint64_t)wp * b.h * b.layers;  // cells of one plane, rows padded
         const uint64_t c0 = (ch - chunk_start[lo]) * kPlaneChunk, c1 = min(c0 + kPlaneChunk, N);
         uint32_t *out = b.planes;
         for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
@@ -97,71 +98,25 @@ __global__ void __launch_bounds__(256) planes_kernel(const DevBoard *boards, con
                     }
                 }
             }
+            const uint64_t o = ((uint64_t)l * b.h + y) * wp + x;
 #pragma unroll
-            for (int p = 0; p < 6; ++p) out[(uint64_t)p * N + c] = s[p];
+            for (int p = 0; p < 6; ++p) out[(uint64_t)p * NP + o] = s[p];
         }
     }
 }
 
-// Exact price of the step into cell c (at l, y, x) from direction `dir`, with
-// the net's own pads, endpoints and via exemptions (the staging rules of the
-// CTA-wide relax kernel, negotiated.rs:2914-2966 and :3010-3043).
-__device__ uint32_t exact_in_price(const DevBoard &b, const DevField &f, const uint32_t *pads, int dir, uint32_t c,
-                                   uint32_t l, uint32_t y, uint32_t x) {
-    const uint8_t fc = b.flags ? __ldg(b.flags + c) : 0;
-    const uint32_t ec = cell_enter(b, f, pads, c, fc);
-    if (ec == kMax) return kMax;
-    const uint32_t plane = b.w * b.h;
-    if (dir == kInBelow || dir == kInAbove) {
-        const bool below = dir == kInBelow;
-        if (below ? l == 0 : l + 1 >= b.layers) return kMax;
-        const uint32_t k = below ? l - 1 : l;
-        if (!((b.via_mask >> k) & 1u)) return kMax;
-        const uint32_t p = below ? c - plane : c + plane;
-        const uint8_t fp = b.flags ? __ldg(b.flags + p) : 0;
-        if ((cell_tile_flags(f, pads, c, fc) | cell_tile_flags(f, pads, p, fp)) & kViaBlocked) return kMax;
-        return capmul(__ldg(b.via_edge + k), ec);
-    }
-    uint32_t p, base;
-    uint8_t out_bit, in_bit;
-    if (dir == kInNegX) {
-        if (x == 0) return kMax;
-        p = c - 1;
-        base = b.directed ? __ldg(b.directed + c).y : __ldg(b.x_edge + x - 1);
-        out_bit = kEdgePosX;
-        in_bit = kEdgeNegX;
-    } else if (dir == kInPosX) {
-        if (x + 1 >= b.w) return kMax;
-        p = c + 1;
-        base = b.directed ? __ldg(b.directed + c).z : __ldg(b.x_edge + x);
-        out_bit = kEdgeNegX;
-        in_bit = kEdgePosX;
-    } else if (dir == kInNegY) {
-        if (y == 0) return kMax;
-        p = c - b.w;
-        base = b.directed ? __ldg(b.directed + c).x : __ldg(b.y_edge + y - 1);
-        out_bit = kEdgePosY;
-        in_bit = kEdgeNegY;
-    } else {
-        if (y + 1 >= b.h) return kMax;
-        p = c + b.w;
-        base = b.directed ? __ldg(b.directed + c).w : __ldg(b.y_edge + y);
-        out_bit = kEdgeNegY;
-        in_bit = kEdgePosY;
-    }
-    const uint8_t fp = b.flags ? __ldg(b.flags + p) : 0;
-    if ((fp & out_bit) | (fc & in_bit)) return kMax;
-    if (b.directed && base == kMax) return kMax;
-    return capmul(base, ec);
-}
-
 // ---- one tile held by one warp ---------------------------------------------
 
+// Per-warp shared memory.  The tile's labels live here rather than in
+// registers: the row loops then run with a runtime row index (one compact copy
+// of the pass code instead of fully unrolled passes, which overflowed the
+// instruction cache) and the stack pass works on the labels in place.
 struct WarpSmem {
-    u64 htb[2][128];    // halo rows above (0) and below (1) the tile, [l * TW + x]
-    u64 hlr[2][128];    // halo columns left (0) and right (1), [l * TH + y]
-    u64 row[128];       // one tile row over every layer (stack pass), [l * TW + x]
-    uint32_t spec[32];  // bit y * TW + x: the (y, x) stack holds an endpoint, own pad or via pad
+    u64 lab[TH][K][32];  // the tile: lane (l, seg) owns lab[y][0..K)[lane], x = 4 seg + i (i-major: no bank conflicts)
+    u64 htb[2][128];     // halo rows above (0) and below (1) the tile, [l * TW + x]
+    u64 hlr[2][128];     // halo columns left (0) and right (1), [l * TH + y]
+    uint32_t spec[32];   // bit y * TW + x: the (y, x) stack holds an endpoint, own pad or via pad
+    uint32_t fell[32];   // per lane: bits y * K + i of its cells that the stack pass lowered
 };
 
 struct WTile {
@@ -169,8 +124,8 @@ struct WTile {
     const DevField *fp;
     const uint32_t *pads;
     const uint32_t *planes;
-    uint64_t N;                   // cells of the board
-    uint32_t w, h;                // board plane extent
+    uint64_t NP;                  // cells of one price plane (rows padded to wp)
+    uint32_t w, h, wp;            // board plane extent, price-plane row pitch
     uint32_t L, S, TW, tw_shift;  // layers, segments per row, tile width (= 1 << tw_shift)
     uint32_t l, lc, seg, xb;      // this lane's layer (clamped copy for addresses), segment, first column
     uint32_t tx0, ty0, tw, th;    // tile origin (board coordinates) and valid extent
@@ -185,8 +140,9 @@ __device__ __noinline__ uint32_t exact_price_t(const WTile &t, int dir, uint32_t
     return exact_in_price(b, f, t.pads, dir, c, l, y, x);
 }
 
-__device__ __forceinline__ uint32_t plane_at(const WTile &t, int p, uint32_t c) {
-    return __ldg(t.planes + (uint64_t)p * t.N + c);
+// Price plane p at (layer l, board row y, board column x).
+__device__ __forceinline__ uint32_t plane_at(const WTile &t, int p, uint32_t l, uint32_t y, uint32_t x) {
+    return __ldg(t.planes + (uint64_t)p * t.NP + ((uint64_t)l * t.h + y) * t.wp + x);
 }
 
 // Price into the tile cell (layer l, tile row y, tile column x).
@@ -196,7 +152,7 @@ __device__ __forceinline__ uint32_t tile_price(const WTile &t, const WarpSmem &s
     const uint32_t c = (l * t.h + gy) * t.w + gx;
     const uint32_t bit = (y << t.tw_shift) + x;
     if ((sm.spec[bit >> 5] >> (bit & 31)) & 1u) return exact_price_t(t, p, c, l, gy, gx);
-    return plane_at(t, p, c);
+    return plane_at(t, p, l, gy, gx);
 }
 
 // Prices into this lane's K cells of tile row y: from -x, from +x and from the
@@ -206,14 +162,14 @@ __device__ __forceinline__ void row_prices(const WTile &t, int y, int pv_dir, ui
                                            uint32_t (&ppx)[K], uint32_t (&pv)[K]) {
     const uint32_t gy = min(t.ty0 + (uint32_t)y, t.wy1 - 1);
     const uint32_t rowc = (t.lc * t.h + gy) * t.w;
+    const uint32_t *row = t.planes + ((uint64_t)t.lc * t.h + gy) * t.wp;
     uint32_t gx[K];
 #pragma unroll
     for (int i = 0; i < K; ++i) {
         gx[i] = min(t.tx0 + t.xb + i, t.wx1 - 1);
-        const uint32_t c = rowc + gx[i];
-        pnx[i] = plane_at(t, kInNegX, c);
-        ppx[i] = plane_at(t, kInPosX, c);
-        pv[i] = plane_at(t, pv_dir, c);
+        pnx[i] = __ldg(row + gx[i]);
+        ppx[i] = __ldg(row + t.NP + gx[i]);
+        pv[i] = __ldg(row + (uint64_t)pv_dir * t.NP + gx[i]);
     }
     const uint32_t sb = (spec_lane >> (y * K)) & ((1u << K) - 1u);
     if (sb) {
@@ -312,31 +268,35 @@ struct RowMarks {
     uint32_t H, D, U, ST;
 };
 
-// A (+y) pass (DOWN) or a (-y) pass over the marked rows.
-template <bool DOWN>
-__device__ __forceinline__ void vert_pass(const WTile &t, const WarpSmem &sm, u64 (&v)[TH][K], RowMarks &m,
-                                          uint32_t spec_lane, uint32_t valid, uint32_t &fell, uint32_t &rows) {
-#pragma unroll
+// A (+y) pass (down) or a (-y) pass over the marked rows.  One copy of the
+// code serves both directions: only the neighbour row, its halo and the
+// vertical price plane differ.
+__device__ __forceinline__ void vert_pass(const WTile &t, WarpSmem &sm, bool down, RowMarks &m, uint32_t spec_lane,
+                                       uint32_t valid, uint32_t &fell, uint32_t &rows, uint32_t lane) {
+    const int pv_dir = down ? kInNegY : kInPosY;
+    const int step = down ? -1 : 1;  // the neighbour row relaxed from
+#pragma unroll 1
     for (int k = 0; k < TH; ++k) {
-        const int y = DOWN ? k : TH - 1 - k;
-        const uint32_t need = m.H | (DOWN ? m.D : m.U);
-        if (!((need >> y) & 1u)) continue;
+        const int y = down ? k : TH - 1 - k;
+        const uint32_t rb = 1u << y;
+        if (!((m.H | (down ? m.D : m.U)) & rb)) continue;
         if ((uint32_t)y >= t.th) {  // past the window: every label stays +inf
-            m.H &= ~(1u << y);
-            m.D &= ~(1u << y);
-            m.U &= ~(1u << y);
+            m.H &= ~rb;
+            m.D &= ~rb;
+            m.U &= ~rb;
             continue;
         }
         ++rows;
         uint32_t pnx[K], ppx[K], pv[K];
-        row_prices(t, y, DOWN ? kInNegY : kInPosY, spec_lane, pnx, ppx, pv);
-        u64 u[K];
+        row_prices(t, y, pv_dir, spec_lane, pnx, ppx, pv);
+        const int yn = y + step;
+        const bool inner = yn >= 0 && yn < TH;
+        const u64 *halo = &sm.htb[down ? 0 : 1][(t.lc << t.tw_shift) + t.xb];
+        u64 cur[K], u[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            u64 nb;
-            if (DOWN) nb = y > 0 ? v[y - 1][i] : sm.htb[0][(t.lc << t.tw_shift) + t.xb + i];
-            else nb = y < TH - 1 ? v[y + 1][i] : sm.htb[1][(t.lc << t.tw_shift) + t.xb + i];
-            u[i] = umin64(v[y][i], ext2(nb, pv[i], 1));
+            cur[i] = sm.lab[y][i][lane];
+            u[i] = umin64(cur[i], ext2(inner ? sm.lab[yn][i][lane] : halo[i], pv[i], 1));
         }
         row_close(u, pnx, ppx, sm.hlr[0][t.lc * TH + y], sm.hlr[1][t.lc * TH + y], t.S, t.seg);
         bool ch = false;
@@ -344,15 +304,14 @@ __device__ __forceinline__ void vert_pass(const WTile &t, const WarpSmem &sm, u6
         for (int i = 0; i < K; ++i) {
             const uint32_t bit = 1u << (y * K + i);
             if (!(valid & bit)) u[i] = kInf;
-            if (u[i] < v[y][i]) {
-                v[y][i] = u[i];
+            if (u[i] < cur[i]) {
+                sm.lab[y][i][lane] = u[i];
                 fell |= bit;
                 ch = true;
             }
         }
-        const uint32_t rb = 1u << y;
         m.H &= ~rb;
-        if (DOWN) m.D &= ~rb;
+        if (down) m.D &= ~rb;
         else m.U &= ~rb;
         if (__any_sync(kFull, ch)) {
             if (y + 1 < TH) m.D |= rb << 1;
@@ -362,66 +321,45 @@ __device__ __forceinline__ void vert_pass(const WTile &t, const WarpSmem &sm, u6
     }
 }
 
-// Layer stacks of the marked rows: the row of every layer goes to shared
-// memory, each lane closes whole stacks (upward, then downward) there, and the
-// lanes take back their cells.
-__device__ __forceinline__ void stack_pass(const WTile &t, WarpSmem &sm, u64 (&v)[TH][K], RowMarks &m,
-                                           uint32_t &fell, uint32_t lane, uint32_t &rows) {
-#pragma unroll
+// Layer stacks of the marked rows, in place in shared memory: lane j closes
+// the stacks of columns j, j + 32, ... (upward, then downward); a lowered cell
+// is flagged for its owner lane in sm.fell.
+__device__ __forceinline__ void stack_pass(const WTile &t, WarpSmem &sm, RowMarks &m, uint32_t lane, uint32_t &rows) {
+#pragma unroll 1
     for (int y = 0; y < TH; ++y) {
-        if (!((m.ST >> y) & 1u)) continue;
-        if ((uint32_t)y >= t.th) {  // past the window: nothing to relax, and no board row to read
-            m.ST &= ~(1u << y);
-            continue;
-        }
+        const uint32_t rb = 1u << y;
+        if (!(m.ST & rb)) continue;
+        m.ST &= ~rb;
+        if ((uint32_t)y >= t.th) continue;  // past the window: nothing to relax, and no board row to read
         ++rows;
-        if (t.act) {
-#pragma unroll
-            for (int i = 0; i < K; ++i) sm.row[(t.l << t.tw_shift) + t.xb + i] = v[y][i];
-        }
-        __syncwarp();
-        for (uint32_t x = lane; x < t.tw; x += 32) {
-            u64 prev = sm.row[x];
-            for (uint32_t l = 1; l < t.L; ++l) {
-                const uint32_t idx = (l << t.tw_shift) + x;
-                const u64 cur = sm.row[idx];
-                const u64 w = ext2(prev, tile_price(t, sm, kInBelow, l, y, x), 1);
-                if (w < cur) {
-                    sm.row[idx] = w;
-                    prev = w;
-                } else {
-                    prev = cur;
-                }
-            }
-            prev = sm.row[((t.L - 1) << t.tw_shift) + x];
-            for (int l = (int)t.L - 2; l >= 0; --l) {
-                const uint32_t idx = ((uint32_t)l << t.tw_shift) + x;
-                const u64 cur = sm.row[idx];
-                const u64 w = ext2(prev, tile_price(t, sm, kInAbove, (uint32_t)l, y, x), 1);
-                if (w < cur) {
-                    sm.row[idx] = w;
-                    prev = w;
-                } else {
-                    prev = cur;
-                }
-            }
-        }
-        __syncwarp();
+        __syncwarp();  // the row passes' stores
         bool ch = false;
-        if (t.act) {
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                const u64 nv = sm.row[(t.l << t.tw_shift) + t.xb + i];
-                if (nv < v[y][i]) {
-                    v[y][i] = nv;
-                    fell |= 1u << (y * K + i);
+        for (uint32_t x = lane; x < t.tw; x += 32) {
+            const uint32_t sg = x / K, xi = x % K;
+            u64 prev = sm.lab[y][xi][sg];
+            for (uint32_t l = 1; l < t.L; ++l) {
+                u64 &cell = sm.lab[y][xi][l * t.S + sg];
+                const u64 w = ext2(prev, tile_price(t, sm, kInBelow, l, y, x), 1);
+                if (w < cell) {
+                    cell = w;
+                    atomicOr(&sm.fell[l * t.S + sg], 1u << (y * K + xi));
                     ch = true;
                 }
+                prev = cell;
+            }
+            prev = sm.lab[y][xi][(t.L - 1) * t.S + sg];
+            for (int l = (int)t.L - 2; l >= 0; --l) {
+                u64 &cell = sm.lab[y][xi][(uint32_t)l * t.S + sg];
+                const u64 w = ext2(prev, tile_price(t, sm, kInAbove, (uint32_t)l, y, x), 1);
+                if (w < cell) {
+                    cell = w;
+                    atomicOr(&sm.fell[(uint32_t)l * t.S + sg], 1u << (y * K + xi));
+                    ch = true;
+                }
+                prev = cell;
             }
         }
-        __syncwarp();  // every lane has read the row before the next one overwrites it
-        const uint32_t rb = 1u << y;
-        m.ST &= ~rb;
+        __syncwarp();  // the stack results, before any lane reads its row again
         if (__any_sync(kFull, ch)) {
             m.H |= rb;
             if (y + 1 < TH) m.D |= rb << 1;
@@ -444,7 +382,7 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *a, uint32_t 
 // of a neighbour tile, from direction `dir` as seen from c.
 __device__ __forceinline__ uint32_t neighbour_price(const WTile &t, int dir, uint32_t c, uint32_t l, uint32_t gy,
                                                     uint32_t gx) {
-    const uint32_t p = plane_at(t, dir, c);
+    const uint32_t p = plane_at(t, dir, l, gy, gx);
     // only an own obstacle pad or endpoint can be priced differently for this net
     if (p == kMax) return exact_price_t(t, dir, c, l, gy, gx);
     return p;
@@ -478,7 +416,8 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
     t.S = warp_segments(t.L);
     t.TW = K * t.S;
     t.tw_shift = (uint32_t)(__ffs((int)t.TW) - 1);
-    t.N = (uint64_t)t.w * t.h * t.L;
+    t.wp = planes_pitch(t.w);
+    t.NP = (uint64_t)t.wp * t.h * t.L;
     t.l = lane / t.S;
     t.seg = lane & (t.S - 1);
     t.act = t.l < t.L;
@@ -508,38 +447,44 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
     };
 
     // ---- stage: halo ring to shared memory, the tile into registers --------
-    for (uint32_t j = lane; j < (t.L << t.tw_shift); j += 32) {
-        const uint32_t l = j >> t.tw_shift, x = j & (t.TW - 1);
-        u64 top = kInf, bot = kInf;
-        if (x < t.tw) {
-            if (t.ty0 > f.y0) top = __ldcg(lab + lidx(l, t.ty0 - 1, t.tx0 + x));
-            if (t.ty0 + t.th < t.wy1) bot = __ldcg(lab + lidx(l, t.ty0 + t.th, t.tx0 + x));
+    auto stage_halo = [&]() {
+        for (uint32_t j = lane; j < (t.L << t.tw_shift); j += 32) {
+            const uint32_t l = j >> t.tw_shift, x = j & (t.TW - 1);
+            u64 top = kInf, bot = kInf;
+            if (x < t.tw) {
+                if (t.ty0 > f.y0) top = __ldcg(lab + lidx(l, t.ty0 - 1, t.tx0 + x));
+                if (t.ty0 + t.th < t.wy1) bot = __ldcg(lab + lidx(l, t.ty0 + t.th, t.tx0 + x));
+            }
+            sm.htb[0][j] = top;
+            sm.htb[1][j] = bot;
         }
-        sm.htb[0][j] = top;
-        sm.htb[1][j] = bot;
-    }
-    for (uint32_t j = lane; j < t.L * TH; j += 32) {
-        const uint32_t l = j / TH, y = j % TH;
-        u64 lft = kInf, rgt = kInf;
-        if (y < t.th) {
-            if (t.tx0 > f.x0) lft = __ldcg(lab + lidx(l, t.ty0 + y, t.tx0 - 1));
-            if (t.tx0 + t.tw < t.wx1) rgt = __ldcg(lab + lidx(l, t.ty0 + y, t.tx0 + t.tw));
+        for (uint32_t j = lane; j < t.L * TH; j += 32) {
+            const uint32_t l = j / TH, y = j % TH;
+            u64 lft = kInf, rgt = kInf;
+            if (y < t.th) {
+                if (t.tx0 > f.x0) lft = __ldcg(lab + lidx(l, t.ty0 + y, t.tx0 - 1));
+                if (t.tx0 + t.tw < t.wx1) rgt = __ldcg(lab + lidx(l, t.ty0 + y, t.tx0 + t.tw));
+            }
+            sm.hlr[0][j] = lft;
+            sm.hlr[1][j] = rgt;
         }
-        sm.hlr[0][j] = lft;
-        sm.hlr[1][j] = rgt;
-    }
+    };
+    stage_halo();
     sm.spec[lane] = 0;
-    u64 v[TH][K];
+    sm.fell[lane] = 0;
     uint32_t valid = 0;
 #pragma unroll
     for (int y = 0; y < TH; ++y) {
+        u64 v[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             const uint32_t x = t.xb + i;
             const bool ok = t.act && x < t.tw && (uint32_t)y < t.th;
             if (ok) valid |= 1u << (y * K + i);
-            v[y][i] = ok ? __ldcg(lab + lidx(t.l, t.ty0 + y, t.tx0 + x)) : kInf;
+            v[i] = ok ? __ldcg(lab + lidx(t.l, t.ty0 + y, t.tx0 + x)) : kInf;
         }
+#pragma unroll
+        for (int i = 0; i < K; ++i) sm.lab[y][i][lane] = v[i];
     }
     __syncwarp();
     // stacks whose prices depend on this net: endpoints, own pads, via pads
@@ -597,101 +542,125 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
             if (t.act && t.l == sl && x >= t.xb && x < t.xb + K) fell |= 1u << ((sy - t.ty0) * K + (x - t.xb));
         }
     }
-    // start with the vertical direction whose entry halo is closer to the source
-    uint32_t dtop = kMax, dbot = kMax;
+    // One activation may run several rounds: when a neighbour improved this
+    // tile's halo while the warp held it (the state word says held-and-dirty),
+    // the warp re-stages the halo only and relaxes again from the labels still
+    // in shared memory, instead of releasing the tile to the queue and staging
+    // all of it again later.  The number of such rounds is bounded; after the
+    // last one a dirty tile is queued again as usual.
+    for (uint32_t round = 0;; ++round) {
+        // start with the vertical direction whose entry halo is closer to the source
+        uint32_t dtop = kMax, dbot = kMax;
 #pragma unroll
-    for (int i = 0; i < K; ++i) {
-        dtop = min(dtop, (uint32_t)(sm.htb[0][(t.lc << t.tw_shift) + t.xb + i] >> 32));
-        dbot = min(dbot, (uint32_t)(sm.htb[1][(t.lc << t.tw_shift) + t.xb + i] >> 32));
-    }
-    dtop = __reduce_min_sync(kFull, dtop);
-    dbot = __reduce_min_sync(kFull, dbot);
-    // passes cycle (first vertical direction, the other one, stacks)
-    bool down = dtop <= dbot;
-    uint32_t passes = 0, rows = 0;
-    const uint32_t pass_limit = 12u * TH * t.TW * t.L + 48u;
-    for (uint32_t step = 0;; ++step) {
-        const uint32_t phase = step % 3;
-        if (phase < 2) {
-            if (down) vert_pass<true>(t, sm, v, m, spec_lane, valid, fell, rows);
-            else vert_pass<false>(t, sm, v, m, spec_lane, valid, fell, rows);
-            down = !down;
-        } else if (t.L > 1) {
-            stack_pass(t, sm, v, m, fell, lane, rows);
-        } else {
-            m.ST = 0;
+        for (int i = 0; i < K; ++i) {
+            dtop = min(dtop, (uint32_t)(sm.htb[0][(t.lc << t.tw_shift) + t.xb + i] >> 32));
+            dbot = min(dbot, (uint32_t)(sm.htb[1][(t.lc << t.tw_shift) + t.xb + i] >> 32));
         }
-        ++passes;
-        if (!(m.H | m.D | m.U | m.ST)) break;
-        if (passes > pass_limit) {
-            if (lane == 0) atomicOr(&ctl->status, kStatusRoundLimit);
-            break;
+        dtop = __reduce_min_sync(kFull, dtop);
+        dbot = __reduce_min_sync(kFull, dbot);
+        // passes cycle (first vertical direction, the other one, stacks)
+        bool down = dtop <= dbot;
+        uint32_t passes = 0, rows = 0;
+        const uint32_t pass_limit = 12u * TH * t.TW * t.L + 48u;
+        for (uint32_t step = 0;; ++step) {
+            const uint32_t phase = step % 3;
+            if (phase < 2) {
+                vert_pass(t, sm, down, m, spec_lane, valid, fell, rows, lane);
+                down = !down;
+            } else if (t.L > 1) {
+                stack_pass(t, sm, m, lane, rows);
+            } else {
+                m.ST = 0;
+            }
+            ++passes;
+            if (!(m.H | m.D | m.U | m.ST)) break;
+            if (passes > pass_limit) {
+                if (lane == 0) atomicOr(&ctl->status, kStatusRoundLimit);
+                break;
+            }
         }
-    }
 
-    // ---- write back the labels that fell; queue the neighbours they improve --
-    bool pl = false, pr = false, pt = false, pb = false;
-    if (t.act && fell) {
-#pragma unroll
-        for (int y = 0; y < TH; ++y) {
-#pragma unroll
-            for (int i = 0; i < K; ++i)
-                if ((fell >> (y * K + i)) & 1u) lab[lidx(t.l, t.ty0 + y, t.tx0 + t.xb + i)] = v[y][i];
-        }
-        // Only a border label that fell can improve a neighbour: an unchanged one
-        // was checked when it was written.  Compare with the halo as staged.
-        const uint32_t l = t.l;
-        if (txi > 0 && t.seg == 0) {
-#pragma unroll
+        // ---- write back the labels that fell; queue the neighbours they improve --
+        __syncwarp();
+        fell |= sm.fell[lane];  // cells lowered by the stack pass of another lane
+        bool pl = false, pr = false, pt = false, pb = false;
+        const auto v = sm.lab;  // the converged tile
+        if (t.act && fell) {
+#pragma unroll 1
             for (int y = 0; y < TH; ++y) {
-                if (!((fell >> (y * K)) & 1u)) continue;
-                const uint32_t gy = t.ty0 + y, gx = t.tx0 - 1, c = (l * t.h + gy) * t.w + gx;
-                const u64 cand = ext2(v[y][0], neighbour_price(t, kInPosX, c, l, gy, gx), 1);
-                pl |= cand < sm.hlr[0][l * TH + y];
-            }
-        }
-        if (txi + 1 < ntx && t.seg == t.S - 1) {  // not the last tile column: tw == TW
 #pragma unroll
-            for (int y = 0; y < TH; ++y) {
-                if (!((fell >> (y * K + K - 1)) & 1u)) continue;
-                const uint32_t gy = t.ty0 + y, gx = t.tx0 + t.TW, c = (l * t.h + gy) * t.w + gx;
-                const u64 cand = ext2(v[y][K - 1], neighbour_price(t, kInNegX, c, l, gy, gx), 1);
-                pr |= cand < sm.hlr[1][l * TH + y];
+                for (int i = 0; i < K; ++i)
+                    if ((fell >> (y * K + i)) & 1u) lab[lidx(t.l, t.ty0 + y, t.tx0 + t.xb + i)] = v[y][i][lane];
             }
-        }
-        if (tyi > 0) {
+            // Only a border label that fell can improve a neighbour: an unchanged one
+            // was checked when it was written.  Compare with the halo as staged.
+            const uint32_t l = t.l;
+            if (txi > 0 && t.seg == 0) {
+#pragma unroll 1
+                for (int y = 0; y < TH; ++y) {
+                    if (!((fell >> (y * K)) & 1u)) continue;
+                    const uint32_t gy = t.ty0 + y, gx = t.tx0 - 1, c = (l * t.h + gy) * t.w + gx;
+                    const u64 cand = ext2(v[y][0][lane], neighbour_price(t, kInPosX, c, l, gy, gx), 1);
+                    pl |= cand < sm.hlr[0][l * TH + y];
+                }
+            }
+            if (txi + 1 < ntx && t.seg == t.S - 1) {  // not the last tile column: tw == TW
+#pragma unroll 1
+                for (int y = 0; y < TH; ++y) {
+                    if (!((fell >> (y * K + K - 1)) & 1u)) continue;
+                    const uint32_t gy = t.ty0 + y, gx = t.tx0 + t.TW, c = (l * t.h + gy) * t.w + gx;
+                    const u64 cand = ext2(v[y][K - 1][lane], neighbour_price(t, kInNegX, c, l, gy, gx), 1);
+                    pr |= cand < sm.hlr[1][l * TH + y];
+                }
+            }
+            if (tyi > 0) {
 #pragma unroll
-            for (int i = 0; i < K; ++i) {
-                if (!((fell >> i) & 1u)) continue;
-                const uint32_t gy = t.ty0 - 1, gx = t.tx0 + t.xb + i, c = (l * t.h + gy) * t.w + gx;
-                const u64 cand = ext2(v[0][i], neighbour_price(t, kInPosY, c, l, gy, gx), 1);
-                pt |= cand < sm.htb[0][(l << t.tw_shift) + t.xb + i];
+                for (int i = 0; i < K; ++i) {
+                    if (!((fell >> i) & 1u)) continue;
+                    const uint32_t gy = t.ty0 - 1, gx = t.tx0 + t.xb + i, c = (l * t.h + gy) * t.w + gx;
+                    const u64 cand = ext2(v[0][i][lane], neighbour_price(t, kInPosY, c, l, gy, gx), 1);
+                    pt |= cand < sm.htb[0][(l << t.tw_shift) + t.xb + i];
+                }
             }
-        }
-        if (tyi + 1 < nty) {  // not the last tile row: th == TH
+            if (tyi + 1 < nty) {  // not the last tile row: th == TH
 #pragma unroll
-            for (int i = 0; i < K; ++i) {
-                if (!((fell >> ((TH - 1) * K + i)) & 1u)) continue;
-                const uint32_t gy = t.ty0 + TH, gx = t.tx0 + t.xb + i, c = (l * t.h + gy) * t.w + gx;
-                const u64 cand = ext2(v[TH - 1][i], neighbour_price(t, kInNegY, c, l, gy, gx), 1);
-                pb |= cand < sm.htb[1][(l << t.tw_shift) + t.xb + i];
+                for (int i = 0; i < K; ++i) {
+                    if (!((fell >> ((TH - 1) * K + i)) & 1u)) continue;
+                    const uint32_t gy = t.ty0 + TH, gx = t.tx0 + t.xb + i, c = (l * t.h + gy) * t.w + gx;
+                    const u64 cand = ext2(v[TH - 1][i][lane], neighbour_price(t, kInNegY, c, l, gy, gx), 1);
+                    pb |= cand < sm.htb[1][(l << t.tw_shift) + t.xb + i];
+                }
             }
         }
-    }
-    __threadfence();  // labels before the pushes and the release
-    pl = __any_sync(kFull, pl);
-    pr = __any_sync(kFull, pr);
-    pt = __any_sync(kFull, pt);
-    pb = __any_sync(kFull, pb);
+        __threadfence();  // labels before the pushes and the release
+        pl = __any_sync(kFull, pl);
+        pr = __any_sync(kFull, pr);
+        pt = __any_sync(kFull, pt);
+        pb = __any_sync(kFull, pb);
+        if (lane == 0) {
+            ws.passes += passes;
+            ws.rows += rows;
+            if (pl) async_push(a, fi, f.tile_off, tile - 1);
+            if (pr) async_push(a, fi, f.tile_off, tile + 1);
+            if (pt) async_push(a, fi, f.tile_off, tile - ntx);
+            if (pb) async_push(a, fi, f.tile_off, tile + ntx);
+        }
+        // improved while held?  take the new halo in place of a re-activation
+        bool again = false;
+        if (round + 1 < kMaxRounds && lane == 0)
+            again = atomicCAS(a.tstamp + f.tile_off + tile, kTileHeldDirty, kTileHeld) == kTileHeldDirty;
+        again = __shfl_sync(kFull, again, 0);
+        if (!again) break;
+        __threadfence();  // the neighbour's labels, written before it marked the tile
+        stage_halo();
+        sm.fell[lane] = 0;
+        __syncwarp();
+        m = RowMarks{all, 1u, 1u << (TH - 1), 0u};
+        fell = 0;
+    }  // rounds
     if (lane == 0) {
         ws.acts += 1;
-        ws.passes += passes;
-        ws.rows += rows;
         if (ws.acts == 32) flush_stats(a, ws);
-        if (pl) async_push(a, fi, f.tile_off, tile - 1);
-        if (pr) async_push(a, fi, f.tile_off, tile + 1);
-        if (pt) async_push(a, fi, f.tile_off, tile - ntx);
-        if (pb) async_push(a, fi, f.tile_off, tile + ntx);
         __threadfence();
         async_release(a, fi, f.tile_off, tile);  // this item is done: its own pushes are already counted
         atomicSub(&ctl->count[1], 1u);
@@ -700,8 +669,8 @@ __device__ void warp_item(const RelaxArgs &a, uint32_t fi, uint32_t tile, WarpSm
 }
 
 __global__ void __launch_bounds__(NW * 32, 4) relax_warp_kernel(RelaxArgs a) {
-    __shared__ WarpSmem smem[NW];
-    WarpSmem &sm = smem[threadIdx.x >> 5];
+    extern __shared__ __align__(16) unsigned char smem_raw[];  // NW x WarpSmem
+    WarpSmem &sm = reinterpret_cast<WarpSmem *>(smem_raw)[threadIdx.x >> 5];
     const uint32_t lane = threadIdx.x & 31;
     WarpStats ws;
     for (;;) {
@@ -749,8 +718,13 @@ cudaError_t planes_launch(const DevBoard *boards, const uint64_t *chunk_start, u
 
 uint32_t warp_relax_threads() { return NW * 32; }
 
+static constexpr size_t kWarpSmemBytes = NW * sizeof(WarpSmem);
+
 cudaError_t warp_relax_occupancy(int *blocks_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_warp_kernel, NW * 32, 0);
+    cudaError_t e = cudaFuncSetAttribute(relax_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kWarpSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_warp_kernel, NW * 32, kWarpSmemBytes);
 }
 
 cudaError_t warp_relax_launch(const RelaxArgs &a, uint32_t grid, cudaStream_t st) {
@@ -758,7 +732,7 @@ cudaError_t warp_relax_launch(const RelaxArgs &a, uint32_t grid, cudaStream_t st
     warp_seed_kernel<<<(a.n_fields + 255) / 256, 256, 0, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    relax_warp_kernel<<<grid, NW * 32, 0, st>>>(a);
+    relax_warp_kernel<<<grid, NW * 32, kWarpSmemBytes, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -21,6 +21,7 @@ import array
 import ctypes as C
 import os
 import threading
+import weakref
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
@@ -487,6 +488,7 @@ class Board:
         engine._check(engine.lib.mrc_board_create(engine.ctx, C.byref(m.grid(grid)),
                                                   C.byref(m.edges(x, y, vias, directed)), C.byref(h)))
         self.handle = h
+        engine._adopt(self)
 
     def close(self):
         if self.handle:
@@ -531,6 +533,7 @@ class Batch:
                                                   m.arr(nb) if nb.size else None, len(nets), m.windows(windows),
                                                   flags, C.byref(h)))
         self.handle = h
+        e._adopt(self)
 
     def capture_graph(self) -> None:
         """Record the launch sequence as a CUDA graph; later launches replay it."""
@@ -636,6 +639,7 @@ class Negotiation:
             engine._check(engine.lib.mrc_negotiation_create_shard(engine.ctx, C.byref(r), prm, m.arr(mask),
                                                                   C.byref(h)))
         self.handle = h
+        engine._adopt(self)
         try:
             self._set_groups(req, groups)
         except Exception:
@@ -745,6 +749,7 @@ class Server:
         prm = _ServerParams(hbm_fraction, slots, max_batch_requests, max_batch_cells, max_layers, merge_ratio)
         engine._check(engine.lib.mrc_server_create(engine.ctx, C.byref(prm), C.byref(h)))
         self.handle = h
+        engine._adopt(self)
         self._live = {}
         self._lock = threading.Lock()
 
@@ -824,11 +829,22 @@ class Engine:
         self.lib = load_library()
         ctx = C.c_void_p()
         self.ctx = None
+        self._children = weakref.WeakSet()  # boards, batches, servers, negotiations made on this context
         self._check(self.lib.mrc_context_create(int(device), C.byref(ctx)))
         self.ctx = ctx
 
+    def _adopt(self, obj) -> None:
+        """Register an object whose handle lives in this context: it is closed
+        before the context is, whatever order the garbage collector takes."""
+        self._children.add(obj)
+
     def close(self):
         if self.ctx:
+            for child in list(self._children):
+                try:
+                    child.close()
+                except Exception:
+                    pass
             self.lib.mrc_context_destroy(self.ctx)
             self.ctx = None
 
