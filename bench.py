@@ -334,10 +334,15 @@ def measure_batch(args, name, eng, rank, world, local, dist, nets=0, steps=None,
     relax_avg = statistics.fmean(relax_ms) if relax_ms and min(relax_ms) > 0 else ms
     achieved = alg_bytes / (relax_avg / 1000.0) / 1e9
     sched = batch.config()
-    kname = {0: "relax_rounds_kernel", 1: "relax_async_kernel", 2: "relax_warp_kernel"}[sched["schedule"]]
-    kfull = "relax_warp_kernel" if sched["schedule"] == 2 else f"{kname}<{sched['tile_h']},{sched['threads']}>"
+    kname = {0: "relax_rounds_kernel", 1: "relax_async_kernel", 2: "relax_warp_kernel",
+             3: "relax_async_kernel"}[sched["schedule"]]
+    # the queue kernel's third template argument: step prices staged from the price planes by TMA
+    kfull = {0: f"relax_rounds_kernel<{sched['tile_h']},{sched['threads']}>",
+             1: f"relax_async_kernel<{sched['tile_h']},{sched['threads']},true>",
+             2: "relax_warp_kernel",
+             3: f"relax_async_kernel<{sched['tile_h']},{sched['threads']},false>"}[sched["schedule"]]
     # DRAM bytes and instruction counts of one launch, from the ncu capture of this kernel and workload
-    prof = _profile_figures(kname, name)
+    prof = _profile_figures(kfull.split("<")[0] + ("_tma" if sched["schedule"] == 1 else ""), name)
     acts = max(work["activations"], 1)
     counters = {"tile_activations": work["activations"], "tiles": work["tiles"],
                 "activations_per_tile": work["activations"] / max(work["tiles"], 1),
