@@ -221,16 +221,20 @@ mrc_status mrc_batch_autotune(mrc_context *ctx, mrc_batch *batch, uint32_t *tile
 mrc_status mrc_batch_set_config(mrc_context *ctx, mrc_batch *batch, uint32_t tile_h, uint32_t threads);
 /* The relax schedule: 0 = bulk-synchronous rounds over a shared tile list
  * (cooperative launch, grid barrier between rounds); 1 = one asynchronous
- * work queue (no rounds; a tile held by one CTA at a time); 2 = the same queue
- * with one warp per tile (tiles of 4 S x 8 cells over every layer, S = 32 /
- * next_pow2(layers), labels held in registers; boards of at most 16 layers,
- * else MRC_ERR_LIMIT).  All give the same labels and paths.  The autotuner
- * tries every one.  These replace the per-round dispatch loop of
- * crates/mr-metal/src/gpu.rs:1630-2039. */
+ * work queue (no rounds; a tile held by one CTA at a time), step prices brought
+ * to each tile by one TMA load from per-board price planes computed once per
+ * launch; 2 = the same queue with one warp per tile (tiles of 4 S x 8 cells
+ * over every layer, S = 32 / next_pow2(layers), labels in shared memory;
+ * boards of at most 16 layers, else MRC_ERR_LIMIT; a batch whose nets carry
+ * negotiation price overrides runs 1 instead); 3 = the queue of 1 with step
+ * prices formed per tile from the staged board words (no planes).  All give
+ * the same labels and paths.  The autotuner tries every one.  These replace
+ * the per-round dispatch loop of crates/mr-metal/src/gpu.rs:1630-2039. */
 mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t schedule);
 /* Schedule of batches built on this context while it holds no autotuned
- * configuration for their layer count and price form: 1 (the default) or 2
- * (see mrc_batch_set_schedule); batches with more than 16 layers keep 1. */
+ * configuration for their layer count and price form: 0, 1 (the default), 2
+ * or 3 (see mrc_batch_set_schedule); with 2, batches with more than 16 layers
+ * run 1. */
 mrc_status mrc_context_set_schedule(mrc_context *ctx, uint32_t schedule);
 /* The batch's current tile height, CTA width and schedule. */
 mrc_status mrc_batch_config(const mrc_batch *batch, uint32_t *tile_h, uint32_t *threads, uint32_t *schedule);
@@ -364,6 +368,34 @@ mrc_status mrc_negotiation_round(mrc_context *ctx, mrc_negotiation *neg, mrc_rou
  * round; not on a shard, whose nets see only part of the paths.  Without this
  * call every net is its own group. */
 mrc_status mrc_negotiation_set_groups(mrc_context *ctx, mrc_negotiation *neg, const uint32_t *groups);
+
+/* Clearance-halo pricing: the reference's clearance-active snapshot iteration
+ * (crates/mr-cpu/src/negotiated.rs:1565-1568 and :1610-1812 with
+ * clearance_active, route_negotiated's pricing :2778-2797, footprints
+ * for_each_halo_cell :3184-3271), on a uniform grid where a radius is a count of
+ * cells.  The footprint of a path is the (2r+1)^2 box around every path cell on
+ * its own layer (r = clearance_cells) and the box of radius
+ * max(clearance_cells, via_keepout_cells) on both layers of every via, clipped
+ * to the board, base obstacles skipped, counted with multiplicity; halo[c] is
+ * the number of footprint visits of every net's current path on cell c.  With
+ * a clearance set (either radius > 0) each round:
+ *   - routes every net (until a round ends with no overused edge: then the
+ *     dirty set is empty, the reference's convergence break);
+ *   - rips nothing up before pricing: the snapshot holds every net's current
+ *     path; the shared price is base + history + pfac * present_weight *
+ *     present + pfac * halo_weight * halo[c] (capped at MAX - 1);
+ *   - prices each net with its own contribution subtracted:
+ *     base + history + pfac * present_weight * (present - own path slot)
+ *     + pfac * halo_weight * (halo[c] - own footprint visits of c);
+ *   - merges: every routed net's old path and footprint leave, its new ones
+ *     enter (an unrouted net contributes nothing).
+ * Overuse, history and groups are unchanged (copper only).  halo_weight is the
+ * reference's CLEARANCE_NEG_WEIGHT (16).  Radii up to 255 cells; called before
+ * the first round; not on a shard.  Both radii 0 turns it off. */
+mrc_status mrc_negotiation_set_clearance(mrc_context *ctx, mrc_negotiation *neg, uint32_t clearance_cells,
+                                         uint32_t via_keepout_cells, uint32_t halo_weight);
+/* Copies halo[c] (one u32 per cell) to a host buffer (a clearance must be set). */
+mrc_status mrc_negotiation_read_halo(mrc_context *ctx, mrc_negotiation *neg, uint32_t *halo);
 
 /* Sharded rounds (one shard per GPU, each routing its own nets of the same
  * board).  A shard keeps the occupancy of its own paths ("local") and a global

@@ -49,6 +49,11 @@ struct DevBoard {
     const uint4 *directed;      // nullable: in-prices from -y, -x, +x, +y
     uint32_t *planes;           // nullable: 6 planes of step prices, rows padded (written by planes_kernel)
     const void *tmap;           // nullable: TMA tensor map (CUtensorMap, 64-byte aligned) over `planes`
+    // nullable: per-field directed in-price overrides (the negotiation's prices
+    // with each net's own path and clearance footprint subtracted), sorted by
+    // cell inside each field's range DevField::over_off .. + n_over
+    const uint32_t *over_cells;
+    const uint4 *over_price;
 };
 
 // One field = one net solved inside one window.
@@ -61,6 +66,8 @@ struct DevField {
     uint32_t out;               // output slot (the net's request index)
     uint32_t tile_off;          // first tile of this field in the tile-state arrays
     uint32_t board;             // index of this field's board in the batch's board array
+    uint32_t n_over;            // directed-price overrides of this field (DevBoard::over_cells)
+    uint32_t over_off;
     uint32_t pad_;
 };
 
@@ -106,6 +113,30 @@ __device__ __forceinline__ bool sorted_has(const uint32_t *a, uint32_t n, uint32
         else hi = mid;
     }
     return lo < n && a[lo] == key;
+}
+
+// First index of a sorted list whose entry is >= key.
+__device__ __forceinline__ uint32_t over_lower_bound(const uint32_t *a, uint32_t n, uint32_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Directed in-price slot s (0 from -y, 1 from -x, 2 from +x, 3 from +y) of
+// cell c as field f sees it: the field's own override at c when it has one,
+// else the board's plane (which must be present).
+__device__ __forceinline__ uint32_t field_directed(const DevBoard &b, const DevField &f, uint32_t c, int s) {
+    if (f.n_over) {
+        const uint32_t *oc = b.over_cells + f.over_off;
+        const uint32_t lo = over_lower_bound(oc, f.n_over, c);
+        if (lo < f.n_over && __ldg(oc + lo) == c)
+            return __ldg(reinterpret_cast<const uint32_t *>(b.over_price + f.over_off + lo) + s);
+    }
+    return __ldg(reinterpret_cast<const uint32_t *>(b.directed + c) + s);
 }
 
 // enter weight of a cell inside the window, kMax when the node is blocked.

@@ -261,6 +261,7 @@ struct NetCopy {
     uint32_t src, dst;
     std::vector<uint32_t> pads, vpads;  // sorted, unique
     uint32_t board = 0;                 // index into the batch's boards
+    uint32_t over_off = 0, n_over = 0;  // directed-price overrides on the board (negotiation with clearance)
 };
 
 bool sorted_contains(const std::vector<uint32_t> &v, uint32_t c) { return std::binary_search(v.begin(), v.end(), c); }
@@ -687,6 +688,7 @@ struct mrc_batch {
     std::vector<const mrc_board *> boards;  // a batch may span many boards
     uint32_t max_layers = 1;
     bool directed_any = false;
+    bool has_over = false;         // some net prices its own directed overrides (not the warp schedule)
     uint32_t flags = 0;
     std::vector<NetCopy> nets;
     std::vector<mrc_window> windows;
@@ -789,6 +791,10 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
         bt->graph = nullptr;
     }
     if (bt->warp && bt->max_layers > kWarpMaxLayers) bt->warp = false;  // too many layers for one warp tile
+    if (bt->warp && bt->has_over) {  // per-net price overrides are staged by the CTA queue form
+        bt->warp = false;
+        bt->cta_planes = true;
+    }
     if (bt->warp) bt->async_q = true;
     const bool cta_pl = bt->async_q && !bt->warp && bt->cta_planes;
     bt->tile_h = bt->warp ? kWarpTileH : tile_h;
@@ -876,6 +882,8 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         bt->directed_any = bt->directed_any || b->directed;
     }
     const uint32_t n = (uint32_t)bt->nets.size();
+    bt->has_over = false;
+    for (const NetCopy &nc : bt->nets) bt->has_over = bt->has_over || nc.n_over;
     uint32_t tile_h = 0, threads = kRelaxThreads;
     size_t smem = 0;
     auto tuned = ctx->tuned.find(tune_key(bt->max_layers, bt->directed_any));
@@ -890,8 +898,9 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         bt->cta_planes = tuned->second[2] != 3;
     } else {
         MRC_TRY(choose_tile(ctx, bt->max_layers, bt->directed_any, &tile_h, &smem));
-        bt->async_q = true;
+        bt->async_q = ctx->default_schedule != 0;
         bt->warp = ctx->default_schedule == 2;
+        bt->cta_planes = ctx->default_schedule != 3;
     }
     // largest windows first: the persistent CTAs then finish together
     std::vector<uint32_t> order(n);
@@ -926,6 +935,8 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
         f.out = i;
         f.tile_off = 0;
         f.board = nc.board;
+        f.n_over = nc.n_over;
+        f.over_off = nc.over_off;
         f.pad_ = 0;
         if (pads.size() > 0xFFFFFFF0u) return fail(MRC_ERR_LIMIT, "pad lists exceed 2^32 entries");
     }
@@ -1639,7 +1650,7 @@ mrc_status mrc_batch_set_schedule(mrc_context *ctx, mrc_batch *batch, uint32_t s
 
 mrc_status mrc_context_set_schedule(mrc_context *ctx, uint32_t schedule) {
     if (!ctx) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (schedule != 1 && schedule != 2) return fail(MRC_ERR_INVALID_ARGUMENT, "default schedule must be 1 or 2");
+    if (schedule > 3) return fail(MRC_ERR_INVALID_ARGUMENT, "default schedule must be 0, 1, 2 or 3");
     Lock lock(ctx, 0);
     ctx->default_schedule = schedule;
     return MRC_OK;
@@ -1715,6 +1726,13 @@ struct mrc_negotiation {
     DBuf d_global;                     // sharded: sum of every shard's d_present
     bool grouped = false;              // overuse counts connection groups, not nets
     DBuf d_group, d_first, d_over;     // group of every net; per slot: first group seen, overused flag
+    // clearance-active rounds (mrc_negotiation_set_clearance): footprint counts
+    // per cell and the per-net price overrides of the round being routed
+    bool clear = false;
+    uint32_t clearance = 0, via_keepout = 0, halo_weight = 16;
+    DBuf d_halo, d_emit_off, d_via_off, d_via_k, d_keys, d_vals, d_keys2, d_vals2, d_run_keys, d_run_vals, d_nruns;
+    DBuf d_cub, d_over_cells, d_over_price, d_range;
+    size_t cub_bytes = 0;
     const uint4 *global() const { return sharded ? d_global.as<uint4>() : d_present.as<uint4>(); }
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~mrc_negotiation() {
@@ -1740,6 +1758,118 @@ mrc_status negotiation_upload_paths(mrc_negotiation *ng) {
     for (auto &p : ng->paths) ng->cells.insert(ng->cells.end(), p.begin(), p.end());
     MRC_TRY(upload(ctx, ng->d_off, ng->offsets.data(), ng->offsets.size() * 8, "upload path offsets"));
     MRC_TRY(upload(ctx, ng->d_cells, ng->cells.data(), ng->cells.size() * 4, "upload path cells"));
+    return MRC_OK;
+}
+
+HaloArgs negotiation_halo(mrc_negotiation *ng, uint32_t n_list, bool add) {
+    HaloArgs a;
+    a.offsets = ng->d_off.as<unsigned long long>();
+    a.cells = ng->d_cells.as<uint32_t>();
+    a.list = ng->d_list.as<uint32_t>();
+    a.n_list = n_list;
+    a.w = ng->base->view.w;
+    a.h = ng->base->view.h;
+    a.layers = ng->base->view.layers;
+    a.cost = ng->base->dev.cost;
+    a.r = ng->clearance;
+    a.vr = std::max(ng->clearance, ng->via_keepout);
+    a.halo = ng->d_halo.as<uint32_t>();
+    a.add = add;
+    return a;
+}
+
+// Each dirty net's own path slots and clearance footprint, as directed-price
+// overrides of the snapshot (the net's prices with its own contribution
+// subtracted); `range` gets (first, end) of every dirty net's run of
+// overrides, in dirty-list order.  The dirty list is on the device (d_list)
+// and d_off/d_cells still hold the paths of the previous round.
+mrc_status negotiation_overrides(mrc_negotiation *ng, uint32_t pfac, std::vector<uint32_t> *range) {
+    mrc_context *ctx = ng->ctx;
+    cudaStream_t s = ctx->stream;
+    const GridView &g = ng->base->view;
+    const uint32_t plane = g.w * g.h;
+    const uint32_t n_dirty = (uint32_t)ng->dirty.size();
+    const uint64_t r = ng->clearance, vr = std::max(ng->clearance, ng->via_keepout);
+    const uint64_t B = r ? (2 * r + 1) * (2 * r + 1) : 0, BV = vr ? (2 * vr + 1) * (2 * vr + 1) : 0;
+    std::vector<uint64_t> emit_off(n_dirty + 1, 0), via_off(n_dirty + 1, 0);
+    std::vector<uint32_t> via_k;
+    uint64_t total = 0;
+    for (uint32_t j = 0; j < n_dirty; ++j) {
+        const std::vector<uint32_t> &p = ng->paths[ng->dirty[j]];
+        emit_off[j] = total;
+        via_off[j] = via_k.size();
+        for (size_t k = 0; k + 1 < p.size(); ++k)
+            if (p[k] % plane == p[k + 1] % plane) via_k.push_back((uint32_t)k);
+        total += p.size() * B + p.size() + (via_k.size() - via_off[j]) * 2 * BV;
+    }
+    emit_off[n_dirty] = total;
+    via_off[n_dirty] = via_k.size();
+    range->assign((size_t)2 * n_dirty, 0);
+    if (total == 0) return MRC_OK;
+    if (total > 0xFFFFFFF0ull) return fail(MRC_ERR_LIMIT, "clearance footprints exceed 2^32 entries");
+    MRC_TRY(upload(ctx, ng->d_emit_off, emit_off.data(), emit_off.size() * 8, "upload footprint offsets"));
+    MRC_TRY(upload(ctx, ng->d_via_off, via_off.data(), via_off.size() * 8, "upload via offsets"));
+    MRC_TRY(upload(ctx, ng->d_via_k, via_k.data(), via_k.size() * 4, "upload via steps"));
+    MRC_TRY(ng->d_keys.get(ctx, total * 8, "footprint keys"));
+    MRC_TRY(ng->d_vals.get(ctx, total * 4, "footprint values"));
+    MRC_TRY(ng->d_keys2.get(ctx, total * 8, "sorted footprint keys"));
+    MRC_TRY(ng->d_vals2.get(ctx, total * 4, "sorted footprint values"));
+    MRC_TRY(ng->d_run_keys.get(ctx, total * 8, "footprint runs"));
+    MRC_TRY(ng->d_run_vals.get(ctx, total * 4, "footprint run values"));
+    MRC_TRY(ng->d_nruns.get(ctx, 8, "run count"));
+    MRC_TRY(ng->d_over_cells.get(ctx, total * 4, "override cells"));
+    MRC_TRY(ng->d_over_price.get(ctx, total * 16, "override prices"));
+    MRC_TRY(ng->d_range.get(ctx, (size_t)2 * n_dirty * 4, "override ranges"));
+    MRC_CUDA(cudaMemsetAsync(ng->d_range.p, 0, (size_t)2 * n_dirty * 4, s), "clear override ranges");
+    EmitArgs ea;
+    ea.offsets = ng->d_off.as<unsigned long long>();
+    ea.cells = ng->d_cells.as<uint32_t>();
+    ea.list = ng->d_list.as<uint32_t>();
+    ea.n_list = n_dirty;
+    ea.emit_off = ng->d_emit_off.as<unsigned long long>();
+    ea.via_off = ng->d_via_off.as<unsigned long long>();
+    ea.via_k = ng->d_via_k.as<uint32_t>();
+    ea.w = g.w;
+    ea.h = g.h;
+    ea.layers = g.layers;
+    ea.cost = ng->base->dev.cost;
+    ea.r = (uint32_t)r;
+    ea.vr = (uint32_t)vr;
+    ea.keys = ng->d_keys.as<unsigned long long>();
+    ea.vals = ng->d_vals.as<uint32_t>();
+    MRC_CUDA(emit_launch(ea, s), "emit footprints");
+    size_t need = 0;
+    auto reduce = [&](void *temp, size_t *bytes) {
+        return footprint_reduce(ng->d_keys.as<unsigned long long>(), ng->d_vals.as<uint32_t>(),
+                                ng->d_keys2.as<unsigned long long>(), ng->d_vals2.as<uint32_t>(),
+                                ng->d_run_keys.as<unsigned long long>(), ng->d_run_vals.as<uint32_t>(),
+                                ng->d_nruns.as<uint32_t>(), total, 64, temp, bytes, s);
+    };
+    MRC_CUDA(reduce(nullptr, &need), "size the footprint sort");
+    if (ng->cub_bytes < need || !ng->d_cub.p) {
+        MRC_TRY(ng->d_cub.get(ctx, std::max<size_t>(need, 16), "footprint sort scratch"));
+        ng->cub_bytes = std::max<size_t>(need, 16);
+    }
+    size_t have = ng->cub_bytes;
+    MRC_CUDA(reduce(ng->d_cub.p, &have), "sort and sum footprints");
+    OverrideArgs oa;
+    oa.keys = ng->d_run_keys.as<unsigned long long>();
+    oa.vals = ng->d_run_vals.as<uint32_t>();
+    oa.n_runs = ng->d_nruns.as<uint32_t>();
+    oa.cap = total;
+    oa.base = ng->base->dev.directed;
+    oa.present = ng->global();
+    oa.history = ng->d_history.as<uint4>();
+    oa.halo = ng->d_halo.as<uint32_t>();
+    oa.pf = (uint64_t)pfac * ng->params.present_weight;
+    oa.hf = (uint64_t)pfac * ng->halo_weight;
+    oa.out_cells = ng->d_over_cells.as<uint32_t>();
+    oa.out_price = ng->d_over_price.as<uint4>();
+    oa.range = ng->d_range.as<uint32_t>();
+    MRC_CUDA(override_launch(oa, s), "price overrides");
+    MRC_CUDA(cudaMemcpyAsync(range->data(), ng->d_range.p, (size_t)2 * n_dirty * 4, cudaMemcpyDeviceToHost, s),
+             "read override ranges");
+    MRC_CUDA(cudaStreamSynchronize(s), "price overrides");
     return MRC_OK;
 }
 
@@ -1860,7 +1990,7 @@ mrc_status mrc_negotiation_ripup(mrc_context *ctx, mrc_negotiation *ng) {
     ng->pending.dirty = n_dirty;
     cudaStream_t s = ctx->stream;
     MRC_CUDA(cudaEventRecord(ng->ev0, s), "record event");
-    if (n_dirty) {
+    if (n_dirty && !ng->clear) {  // with a clearance every path stays in the snapshot until the merge
         MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
         MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, false), s), "rip-up");
     }
@@ -1885,10 +2015,12 @@ mrc_status mrc_negotiation_route(mrc_context *ctx, mrc_negotiation *ng, mrc_roun
     sa.base = ng->base->dev.directed;
     sa.present = ng->global();
     sa.history = ng->d_history.as<uint4>();
+    sa.halo = ng->clear ? ng->d_halo.as<uint32_t>() : nullptr;
     sa.out = ng->d_snap.as<uint4>();
     sa.n = g.n;
     sa.pfac = st->pfac;
     sa.weight = ng->params.present_weight;
+    sa.halo_weight = ng->halo_weight;
     MRC_CUDA(snapshot_launch(sa, s), "price snapshot");
     if (n_dirty) {
         std::vector<NetCopy> nets;
@@ -1898,9 +2030,28 @@ mrc_status mrc_negotiation_route(mrc_context *ctx, mrc_negotiation *ng, mrc_roun
             nets.push_back(ng->nets[i]);
             wins.push_back(ng->windows[i]);
         }
+        if (ng->clear) {
+            MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
+            std::vector<uint32_t> range;
+            MRC_TRY(negotiation_overrides(ng, st->pfac, &range));
+            for (uint32_t k = 0; k < n_dirty; ++k) {
+                nets[k].over_off = range[2 * k];
+                nets[k].n_over = range[2 * k + 1] - range[2 * k];
+            }
+            ng->snap->dev.over_cells = ng->d_over_cells.as<uint32_t>();
+            ng->snap->dev.over_price = ng->d_over_price.as<uint4>();
+        }
         mrc_result *raw = nullptr;
-        MRC_TRY(solve(ctx, {ng->snap.get()}, std::move(nets), std::move(wins), MRC_FLAG_RETRY_FULL, &raw, nullptr));
+        const mrc_status rs =
+            solve(ctx, {ng->snap.get()}, std::move(nets), std::move(wins), MRC_FLAG_RETRY_FULL, &raw, nullptr);
+        ng->snap->dev.over_cells = nullptr;
+        ng->snap->dev.over_price = nullptr;
+        MRC_TRY(rs);
         std::unique_ptr<mrc_result> res(raw);
+        if (ng->clear) {  // the routed nets' old copper and footprints leave before the new ones enter
+            MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, false), s), "rip-up old paths");
+            MRC_CUDA(halo_launch(negotiation_halo(ng, n_dirty, false), s), "remove old footprints");
+        }
         for (uint32_t k = 0; k < n_dirty; ++k) {
             const uint32_t i = ng->dirty[k];
             ng->paths[i].assign(res->cells.begin() + res->offsets[k], res->cells.begin() + res->offsets[k + 1]);
@@ -1914,6 +2065,7 @@ mrc_status mrc_negotiation_route(mrc_context *ctx, mrc_negotiation *ng, mrc_roun
         MRC_TRY(negotiation_upload_paths(ng));
         MRC_TRY(upload(ctx, ng->d_list, ng->dirty.data(), (size_t)n_dirty * 4, "upload dirty nets"));
         MRC_CUDA(occupancy_launch(negotiation_occupancy(ng, n_dirty, true), s), "merge paths");
+        if (ng->clear) MRC_CUDA(halo_launch(negotiation_halo(ng, n_dirty, true), s), "add footprints");
     }
     MRC_CUDA(cudaStreamSynchronize(s), "route");
     ng->phase = 2;
@@ -1975,8 +2127,13 @@ mrc_status mrc_negotiation_settle(mrc_context *ctx, mrc_negotiation *ng, mrc_rou
     MRC_CUDA(cudaStreamSynchronize(s), "negotiation round");
     MRC_CUDA(cudaEventElapsedTime(&st->round_ms, ng->ev0, ng->ev1), "round time");
     ng->dirty.clear();
-    for (uint32_t i = 0; i < n; ++i)
-        if (flags[i] && ng->owned[i]) ng->dirty.push_back(i);  // the dirty scan marks unrouted nets too
+    if (ng->clear) {  // every net again until a round ends without overuse (negotiated.rs:1631-1634, :1986)
+        if (slots)
+            for (uint32_t i = 0; i < n; ++i) ng->dirty.push_back(i);
+    } else {
+        for (uint32_t i = 0; i < n; ++i)
+            if (flags[i] && ng->owned[i]) ng->dirty.push_back(i);  // the dirty scan marks unrouted nets too
+    }
     st->overused_edges = slots / 2;
     st->next_dirty = (uint32_t)ng->dirty.size();
     st->path_cells = ng->cells.size();
@@ -2002,6 +2159,38 @@ mrc_status mrc_negotiation_set_groups(mrc_context *ctx, mrc_negotiation *ng, con
     MRC_TRY(ng->d_over.get(ctx, std::max<size_t>(cells * 4, 16), "overuse flags"));
     MRC_CUDA(cudaStreamSynchronize(ctx->stream), "upload connection groups");
     ng->grouped = true;
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_set_clearance(mrc_context *ctx, mrc_negotiation *ng, uint32_t clearance_cells,
+                                         uint32_t via_keepout_cells, uint32_t halo_weight) {
+    if (!ctx || !ng) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ng->sharded) return fail(MRC_ERR_INVALID_ARGUMENT, "clearance pricing needs every path: not on a shard");
+    if (ng->round != 0 || ng->phase != 0)
+        return fail(MRC_ERR_INVALID_ARGUMENT, "the clearance is set before the first round");
+    if (clearance_cells > kMaxClearanceCells || via_keepout_cells > kMaxClearanceCells)
+        return fail(MRC_ERR_INVALID_ARGUMENT, "clearance radius above 255 cells");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    ng->clearance = clearance_cells;
+    ng->via_keepout = via_keepout_cells;
+    ng->halo_weight = halo_weight;
+    ng->clear = clearance_cells > 0 || via_keepout_cells > 0;
+    if (ng->clear) {
+        const size_t bytes = std::max<size_t>((size_t)ng->base->view.n * 4, 16);
+        MRC_TRY(ng->d_halo.get(ctx, bytes, "clearance footprints"));
+        MRC_CUDA(cudaMemsetAsync(ng->d_halo.p, 0, bytes, ctx->stream), "clear footprints");
+        MRC_CUDA(cudaStreamSynchronize(ctx->stream), "clear footprints");
+    }
+    return MRC_OK;
+}
+
+mrc_status mrc_negotiation_read_halo(mrc_context *ctx, mrc_negotiation *ng, uint32_t *halo) {
+    if (!ctx || !ng || !halo) return fail(MRC_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!ng->clear) return fail(MRC_ERR_INVALID_ARGUMENT, "no clearance set");
+    Lock lock(ctx, 0);
+    MRC_TRY(set_device(ctx));
+    MRC_CUDA(cudaMemcpy(halo, ng->d_halo.p, (size_t)ng->base->view.n * 4, cudaMemcpyDeviceToHost), "read footprints");
     return MRC_OK;
 }
 

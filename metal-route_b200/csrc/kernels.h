@@ -75,9 +75,67 @@ struct OccupancyArgs {
 
 struct SnapshotArgs {
     const uint4 *base, *present, *history;
+    const uint32_t *halo;               // nullable: clearance footprints covering each cell
     uint4 *out;
     uint64_t n;                         // cells
-    uint32_t pfac, weight;
+    uint32_t pfac, weight, halo_weight;
+};
+
+// Clearance footprints (for_each_halo_cell, negotiated.rs:3184-3271, on a
+// uniform grid): the (2r+1)^2 box around every path cell on its own layer and
+// the box of radius vr = max(r, keepout) on both layers of every via, clipped
+// to the board, base obstacles (cost == MAX) skipped, with multiplicity.
+struct HaloArgs {
+    const unsigned long long *offsets;  // path CSR of every net
+    const uint32_t *cells;
+    const uint32_t *list;               // nets to apply
+    uint32_t n_list;
+    uint32_t w, h, layers;
+    const uint32_t *cost;               // base cell costs
+    uint32_t r, vr;
+    uint32_t *halo;                     // 1 per cell
+    bool add;
+};
+
+// One entry per (listed net, visit): key = list index << 32 | cell, value = 1
+// per footprint visit, or 1 << (24 + slot) for each in-edge slot of the cell
+// that the net's own path uses.  A visit outside the board or onto an obstacle
+// emits the key kNoKey.  The host lays the entries of list index j out from
+// emit_off[j]: path cells x (2r+1)^2 boxes, then the path cells, then 2 boxes
+// of (2vr+1)^2 per via (via_k: the path index k of each via step k -> k+1).
+constexpr unsigned long long kNoKey = ~0ull;
+constexpr uint32_t kOwnHaloMask = 0x00FFFFFFu;  // footprint visits of one net on one cell stay below 2^24
+constexpr uint32_t kMaxClearanceCells = 255;      // ... for radii up to this many cells
+struct EmitArgs {
+    const unsigned long long *offsets;  // path CSR of every net
+    const uint32_t *cells;
+    const uint32_t *list;
+    uint32_t n_list;
+    const unsigned long long *emit_off; // n_list + 1
+    const unsigned long long *via_off;  // n_list + 1, into via_k
+    const uint32_t *via_k;
+    uint32_t w, h, layers;
+    const uint32_t *cost;
+    uint32_t r, vr;
+    unsigned long long *keys;
+    uint32_t *vals;
+};
+
+// Overrides from the reduced (key, value) runs: for run i the net's own price
+// of every slot of the cell, base == MAX ? MAX : min(base + history
+// + pf * (present - own_slot) + hf * (halo - own_halo), MAX - 1), and the range
+// of each list index (range[2 j], range[2 j + 1]; zeroed before).
+struct OverrideArgs {
+    const unsigned long long *keys;
+    const uint32_t *vals;
+    const uint32_t *n_runs;             // device count of runs
+    uint64_t cap;                       // launch bound on runs
+    const uint4 *base, *present, *history;
+    const uint32_t *halo;
+    uint64_t pf, hf;                    // pfac * present weight, pfac * halo weight
+    uint32_t *out_cells;
+    uint4 *out_price;
+    uint32_t *range;
 };
 
 struct OveruseArgs {
@@ -116,6 +174,15 @@ cudaError_t snapshot_launch(const SnapshotArgs &a, cudaStream_t st);
 cudaError_t overuse_launch(const OveruseArgs &a, cudaStream_t st);
 cudaError_t dirty_launch(const DirtyArgs &a, cudaStream_t st);
 cudaError_t group_overuse_launch(const GroupArgs &a, cudaStream_t st);
+cudaError_t halo_launch(const HaloArgs &a, cudaStream_t st);
+cudaError_t emit_launch(const EmitArgs &a, cudaStream_t st);
+// Sort (keys, vals) by key and sum the values of equal keys into (run_keys,
+// run_vals, *n_runs); temp is resized as needed (bytes in *temp_bytes).
+cudaError_t footprint_reduce(const unsigned long long *keys, const uint32_t *vals, unsigned long long *keys_sorted,
+                             uint32_t *vals_sorted, unsigned long long *run_keys, uint32_t *run_vals,
+                             uint32_t *n_runs, uint64_t n, int end_bit, void *temp, size_t *temp_bytes,
+                             cudaStream_t st);
+cudaError_t override_launch(const OverrideArgs &a, cudaStream_t st);
 
 // Warp schedule (warp_relax.cu): one warp per tile of (4 S) x 8 cells over all
 // layers, S = 32 / next_pow2(layers) segments per row; boards of up to 16 layers.

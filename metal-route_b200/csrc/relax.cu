@@ -448,6 +448,38 @@ __host__ __device__ inline TileLayout tile_layout(uint32_t L, uint32_t TH, bool 
     return o;
 }
 
+// A field's directed-price overrides inside its tile (a negotiation net's own
+// prices on its own footprint), into the shared planes laid out as Tile::si:
+// the raw directed words before the step prices are formed (exact = false), or
+// the four planar in-prices priced exactly (exact = true, over the price planes).
+// Out of line: it runs only for overriding fields and keeps the staging's
+// registers free.
+static __device__ __noinline__ void stage_overrides(const DevBoard &b, const DevField &f, const uint32_t *pads,
+                                                    uint32_t *st, uint32_t L, uint32_t TH, uint32_t sp, uint32_t xo,
+                                                    int tx0, int ty0, uint32_t tw, uint32_t th, bool exact) {
+    const uint32_t *oc = b.over_cells + f.over_off;
+    auto si = [&](int p, uint32_t l, uint32_t y, uint32_t x) { return (((uint32_t)p * L + l) * TH + y) * sp + x + xo; };
+    for (uint32_t j = threadIdx.x; j < L * th; j += blockDim.x) {
+        const uint32_t l = j / th, y = j - l * th;
+        const uint32_t lo_c = (l * b.h + (uint32_t)ty0 + y) * b.w + (uint32_t)tx0, hi_c = lo_c + tw;
+        for (uint32_t k = over_lower_bound(oc, f.n_over, lo_c); k < f.n_over; ++k) {
+            const uint32_t c = __ldg(oc + k);
+            if (c >= hi_c) break;
+            const uint32_t x = c - lo_c;
+            if (exact) {
+                for (int p = kInNegX; p <= kInPosY; ++p)
+                    st[si(p, l, y, x)] = exact_in_price(b, f, pads, p, c, l, (uint32_t)ty0 + y, (uint32_t)tx0 + x);
+            } else {
+                const uint4 d = __ldg(b.over_price + f.over_off + k);
+                st[si(kFromNegX, l, y, x)] = d.y;
+                st[si(kFromPosX, l, y, x)] = d.z;
+                st[si(kFromNegY, l, y, x)] = d.x;
+                st[si(kFromPosY, l, y, x)] = d.w;
+            }
+        }
+    }
+}
+
 // With PL the tile's six step-price planes come from the board's precomputed
 // planes (planes_kernel) in one TMA load: box kPlaneTmaBoxW x TH x L x 6 at column
 // tx0 rounded down to 4 (a TMA x coordinate times 4 bytes must be a multiple
@@ -672,9 +704,19 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
                 }
             }
         }
+        // cells where this net's own directed prices differ from the board's
+        // (negotiation overrides): their four planar in-prices priced exactly
+        // (the same values an overlapping exact stack writes)
+        if (f.n_over) stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, true);
     } else {
         cp_async_wait_all();  // the board words copied before the label loop
         __syncthreads();
+        // this net's own directed prices (negotiation overrides) replace the
+        // board's words before the step prices are formed
+        if (f.n_over) {
+            stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, false);
+            __syncthreads();
+        }
         // Phase 2: every step price from the staged bytes (own pads and via
         // exemptions are the only global reads left).
         for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
@@ -803,7 +845,8 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             const int pin = side == 0 ? kInPosX : side == 1 ? kInNegX : side == 2 ? kInPosY : kInNegY;
             const uint32_t wp = planes_pitch(b.w);
             uint32_t step = __ldg(b.planes + (uint64_t)pin * wp * b.h * L + ((uint64_t)l * b.h + gy_n) * wp + gx_n);
-            if (step == kMax) step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
+            if (step == kMax || f.n_over)
+                step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
             if (ext2(lb, step, 1) < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
             continue;
         }
@@ -814,7 +857,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
         const uint32_t cn = __ldg(b.cost + gn);
         uint32_t base;
-        if (b.directed) base = __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
+        if (b.directed) base = field_directed(b, f, gn, (int)dir);
         else if (side == 0) base = __ldg(b.x_edge + gx_n);
         else if (side == 1) base = __ldg(b.x_edge + gx_n - 1);
         else if (side == 2) base = __ldg(b.y_edge + gy_n);
@@ -1061,19 +1104,19 @@ __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevFiel
     if (kind == 1) {  // p at -y: p moves +y
         out_bit = kEdgePosY;
         in_bit = kEdgeNegY;
-        base = b.directed ? __ldg(b.directed + cur).x : __ldg(b.y_edge + y - 1);
+        base = b.directed ? field_directed(b, f, cur, 0) : __ldg(b.y_edge + y - 1);
     } else if (kind == 2) {  // p at -x: p moves +x
         out_bit = kEdgePosX;
         in_bit = kEdgeNegX;
-        base = b.directed ? __ldg(b.directed + cur).y : __ldg(b.x_edge + x - 1);
+        base = b.directed ? field_directed(b, f, cur, 1) : __ldg(b.x_edge + x - 1);
     } else if (kind == 3) {  // p at +x: p moves -x
         out_bit = kEdgeNegX;
         in_bit = kEdgePosX;
-        base = b.directed ? __ldg(b.directed + cur).z : __ldg(b.x_edge + x);
+        base = b.directed ? field_directed(b, f, cur, 2) : __ldg(b.x_edge + x);
     } else {  // p at +y: p moves -y
         out_bit = kEdgeNegY;
         in_bit = kEdgePosY;
-        base = b.directed ? __ldg(b.directed + cur).w : __ldg(b.y_edge + y);
+        base = b.directed ? field_directed(b, f, cur, 3) : __ldg(b.y_edge + y);
     }
     if ((fp & out_bit) | (fc & in_bit)) return kMax;
     if (b.directed && base == kMax) return kMax;
@@ -1090,7 +1133,7 @@ __device__ __forceinline__ uint32_t walk_step(const DevBoard &b, const DevField 
     uint32_t base = 0;
     if (kind == 0) base = __ldg(b.via_edge + l - 1);
     else if (kind == 5) base = __ldg(b.via_edge + l);
-    else if (b.directed) base = __ldg(reinterpret_cast<const uint32_t *>(b.directed + cur) + (kind == 1 ? 0 : kind == 2 ? 1 : kind == 3 ? 2 : 3));
+    else if (b.directed) base = field_directed(b, f, cur, kind == 1 ? 0 : kind == 2 ? 1 : kind == 3 ? 2 : 3);
     else if (kind == 1) base = __ldg(b.y_edge + y - 1);
     else if (kind == 2) base = __ldg(b.x_edge + x - 1);
     else if (kind == 3) base = __ldg(b.x_edge + x);

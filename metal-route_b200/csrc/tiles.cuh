@@ -112,7 +112,7 @@ __device__ __forceinline__ u64 async_pop(const RelaxArgs &a) {
 enum { kInNegX = 0, kInPosX = 1, kInNegY = 2, kInPosY = 3, kInBelow = 4, kInAbove = 5 };
 
 // Exact price of the step into cell c (at l, y, x) from direction `dir`, with
-// the net's own pads, endpoints and via exemptions (the staging rules of the
+// the net's own pads, endpoints, via exemptions and directed-price overrides (the staging rules of the
 // CTA-wide relax kernel without price planes, negotiated.rs:2914-2966 and :3010-3043).
 static __device__ __noinline__ uint32_t exact_in_price(const DevBoard &b, const DevField &f, const uint32_t *pads, int dir, uint32_t c,
                                    uint32_t l, uint32_t y, uint32_t x) {
@@ -135,25 +135,25 @@ static __device__ __noinline__ uint32_t exact_in_price(const DevBoard &b, const 
     if (dir == kInNegX) {
         if (x == 0) return kMax;
         p = c - 1;
-        base = b.directed ? __ldg(b.directed + c).y : __ldg(b.x_edge + x - 1);
+        base = b.directed ? field_directed(b, f, c, 1) : __ldg(b.x_edge + x - 1);
         out_bit = kEdgePosX;
         in_bit = kEdgeNegX;
     } else if (dir == kInPosX) {
         if (x + 1 >= b.w) return kMax;
         p = c + 1;
-        base = b.directed ? __ldg(b.directed + c).z : __ldg(b.x_edge + x);
+        base = b.directed ? field_directed(b, f, c, 2) : __ldg(b.x_edge + x);
         out_bit = kEdgeNegX;
         in_bit = kEdgePosX;
     } else if (dir == kInNegY) {
         if (y == 0) return kMax;
         p = c - b.w;
-        base = b.directed ? __ldg(b.directed + c).x : __ldg(b.y_edge + y - 1);
+        base = b.directed ? field_directed(b, f, c, 0) : __ldg(b.y_edge + y - 1);
         out_bit = kEdgePosY;
         in_bit = kEdgeNegY;
     } else {
         if (y + 1 >= b.h) return kMax;
         p = c + b.w;
-        base = b.directed ? __ldg(b.directed + c).w : __ldg(b.y_edge + y);
+        base = b.directed ? field_directed(b, f, c, 3) : __ldg(b.y_edge + y);
         out_bit = kEdgeNegY;
         in_bit = kEdgePosY;
     }

@@ -197,6 +197,8 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
             "mrc_negotiation_dirty": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32p)]),
             "mrc_negotiation_destroy": (None, [vp]),
             "mrc_negotiation_set_groups": (C.c_int, [vp, vp, vp]),
+            "mrc_negotiation_set_clearance": (C.c_int, [vp, vp, u32, u32, u32]),
+            "mrc_negotiation_read_halo": (C.c_int, [vp, vp, vp]),
             "mrc_negotiation_create_shard": (C.c_int, [vp, C.POINTER(_Request), C.POINTER(_NegParams), vp,
                                                        C.POINTER(vp)]),
             "mrc_negotiation_ripup": (C.c_int, [vp, vp]),
@@ -562,7 +564,8 @@ class Batch:
 
     def set_schedule(self, schedule: int) -> None:
         """0 = bulk-synchronous rounds, 1 = asynchronous work queue (a CTA per
-        tile), 2 = the queue with a warp per tile."""
+        tile, prices from the TMA-loaded price planes), 2 = the queue with a warp
+        per tile, 3 = the CTA queue with prices formed per tile."""
         e = self.engine
         e._check(e.lib.mrc_batch_set_schedule(e.ctx, self.handle, int(schedule)))
 
@@ -615,10 +618,18 @@ class Negotiation:
     round rips up the dirty nets, prices a frozen snapshot
     base + history + pfac * present_weight * present per directed planar edge
     slot, routes the dirty nets alone on it, merges them back and adds
-    history_step to every edge two or more nets use."""
+    history_step to every edge two or more nets use.
+
+    With a clearance (`clearance` cells around every path cell, `via_keepout`
+    cells around every via) the rounds are the reference's clearance-active
+    iteration: every net is routed every round, nothing is ripped up before
+    pricing, the snapshot adds pfac * halo_weight * halo (the footprints of
+    every net's path covering a cell) and each net is priced with its own path
+    and footprint subtracted (mrc_negotiation_set_clearance)."""
 
     def __init__(self, engine: "Engine", req: IsolatedRouteRequest, present_weight: int = 16,
-                 history_step: int = 1, owned: Optional[Sequence[bool]] = None, groups=None):
+                 history_step: int = 1, owned: Optional[Sequence[bool]] = None, groups=None,
+                 clearance: int = 0, via_keepout: int = 0, halo_weight: int = 16):
         """`groups`: None (every net its own group), "connections" (the
         reference's connection groups from the net names and shared endpoints),
         or one group id per net; with groups an edge is overused only when nets
@@ -642,6 +653,9 @@ class Negotiation:
         engine._adopt(self)
         try:
             self._set_groups(req, groups)
+            if clearance or via_keepout:
+                engine._check(engine.lib.mrc_negotiation_set_clearance(engine.ctx, self.handle, int(clearance),
+                                                                       int(via_keepout), int(halo_weight)))
         except Exception:
             self.close()
             raise
@@ -717,6 +731,14 @@ class Negotiation:
         e = self.engine
         e._check(e.lib.mrc_negotiation_read(e.ctx, self.handle, m.arr(out[0]), m.arr(out[1]), m.arr(out[2])))
         return tuple(out)
+
+    def read_halo(self) -> np.ndarray:
+        """Footprint visits per cell (uint32, one per cell); needs a clearance."""
+        out = np.zeros(len(self.dims), np.uint32)
+        m = _Marshal()
+        e = self.engine
+        e._check(e.lib.mrc_negotiation_read_halo(e.ctx, self.handle, m.arr(out)))
+        return out
 
     def dirty(self) -> List[int]:
         n, p = C.c_uint32(), C.POINTER(C.c_uint32)()
@@ -856,7 +878,7 @@ class Engine:
 
     def set_schedule(self, schedule: int) -> None:
         """Relax schedule of batches this engine builds without an autotuned
-        configuration: 1 = a CTA per tile (the default), 2 = a warp per tile."""
+        configuration: 0, 1 (the default), 2 or 3, as Batch.set_schedule."""
         self._check(self.lib.mrc_context_set_schedule(self.ctx, int(schedule)))
 
     def _check(self, status: int) -> None:
@@ -977,10 +999,12 @@ class Engine:
         return Server(self, **kw)
 
     def negotiation(self, req: IsolatedRouteRequest, present_weight: int = 16, history_step: int = 1,
-                    owned: Optional[Sequence[bool]] = None, groups=None) -> Negotiation:
+                    owned: Optional[Sequence[bool]] = None, groups=None, clearance: int = 0,
+                    via_keepout: int = 0, halo_weight: int = 16) -> Negotiation:
         """An unsharded negotiation, or (with `owned`) this GPU's shard of one;
-        `groups` as in Negotiation."""
-        return Negotiation(self, req, present_weight, history_step, owned, groups)
+        `groups` and the clearance radii as in Negotiation."""
+        return Negotiation(self, req, present_weight, history_step, owned, groups, clearance, via_keepout,
+                           halo_weight)
 
 
 def net_windows(dims, nets: Sequence[NetEndpoints]) -> List[IsolatedRouteWindow]:

@@ -24,10 +24,13 @@ def engine(request):
     e.close()
 
 
-def _run_both(engine, oracle, req, rounds, weight=16, step=1, check_arrays=True, groups=None):
-    dev = engine.negotiation(req, present_weight=weight, history_step=step, groups=groups)
+def _run_both(engine, oracle, req, rounds, weight=16, step=1, check_arrays=True, groups=None, clearance=0,
+              via_keepout=0):
+    dev = engine.negotiation(req, present_weight=weight, history_step=step, groups=groups, clearance=clearance,
+                             via_keepout=via_keepout)
     cpu_groups = mrcuda.connection_group_ids(req.nets) if groups == "connections" else groups
-    cpu = SnapshotNegotiation(oracle, req, present_weight=weight, history_step=step, groups=cpu_groups)
+    cpu = SnapshotNegotiation(oracle, req, present_weight=weight, history_step=step, groups=cpu_groups,
+                              clearance=clearance, via_keepout=via_keepout)
     history = []
     for r in range(rounds):
         a = dev.round()
@@ -44,6 +47,8 @@ def _run_both(engine, oracle, req, rounds, weight=16, step=1, check_arrays=True,
             np.testing.assert_array_equal(present, cpu.present, err_msg=f"present, round {r}")
             np.testing.assert_array_equal(hist, cpu.history, err_msg=f"history, round {r}")
             np.testing.assert_array_equal(snap, cpu.snapshot, err_msg=f"snapshot, round {r}")
+            if clearance or via_keepout:
+                np.testing.assert_array_equal(dev.read_halo(), cpu.halo, err_msg=f"halo, round {r}")
         history.append(a)
     dev.close()
     return history
@@ -141,3 +146,72 @@ def test_connection_groups_are_checked(engine):
         shard.engine._check(shard.engine.lib.mrc_negotiation_set_groups(shard.engine.ctx, shard.handle,
                                                                         g.ctypes.data))
     shard.close()
+
+
+# ---- clearance-halo pricing ------------------------------------------------------
+
+
+def test_clearance_rounds_match_the_oracle(engine, oracle):
+    """The reference's clearance-active iteration: every net routed every
+    round against the snapshot of all current paths plus their footprints,
+    each net priced with its own copper and footprint subtracted (per-net
+    overrides on the device).  Paths, dirty sets, occupancy, history, the
+    shared snapshot and the footprint counts match the oracle every round."""
+    wl = W.snapshot_board(seed=4, w=96, h=80, layers=2, n_nets=24, median=30)
+    hist = _run_both(engine, oracle, wl.request(), rounds=5, clearance=1, via_keepout=2)
+    assert hist[0]["dirty"] == 24 and hist[1]["dirty"] == 24
+    _run_both(engine, oracle, wl.request(), rounds=3, clearance=2, via_keepout=0)
+    _run_both(engine, oracle, wl.request(), rounds=3, clearance=0, via_keepout=1)
+
+
+def test_clearance_corridor_and_retry(engine, oracle):
+    """A corridor both nets must share (overuse never clears: both stay
+    dirty), and tight windows whose nets need the full-board retry, which then
+    runs with the same per-net overrides."""
+    dims = Dims(9, 5, 1)
+    cost = np.full((5, 9), 0xFFFFFFFF, np.uint32)
+    cost[:, 0] = 1
+    cost[:, 8] = 1
+    cost[2, :] = 1
+    nets = [NetEndpoints("a", dims.idx(0, 0), dims.idx(8, 0)), NetEndpoints("b", dims.idx(0, 4), dims.idx(8, 4))]
+    req = IsolatedRouteRequest(Grid(dims, cost.reshape(-1)), nets, [IsolatedRouteWindow.full(dims)] * 2, [10] * 8,
+                               [10] * 4, [])
+    hist = _run_both(engine, oracle, req, rounds=4, clearance=1)
+    assert all(h["dirty"] == 2 for h in hist)
+    dims = Dims(40, 20, 2)
+    cost = np.ones((2, 20, 40), np.uint32)
+    cost[:, 0:18, 20] = 0xFFFFFFFF
+    nets = [NetEndpoints(f"w{i}", dims.idx3(2 + i, 2 + i, 0), dims.idx3(37 - i, 3 + i, i % 2)) for i in range(8)]
+    wins = [IsolatedRouteWindow(0, 0, 39, 12)] * len(nets)
+    req = IsolatedRouteRequest(Grid(dims, cost.reshape(-1)), nets, wins, [10] * 39, [10] * 19, [30])
+    hist = _run_both(engine, oracle, req, rounds=4, clearance=1, via_keepout=1)
+    assert hist[1]["retried"] == len(nets)
+
+
+@pytest.mark.parametrize("schedule", [0, 3])
+def test_clearance_on_the_staged_word_schedules(oracle, schedule):
+    """The rounds form and the queue form without price planes patch the
+    staged directed words with the per-net overrides."""
+    e = mrcuda.Engine(0)
+    try:
+        e.set_schedule(schedule)
+        wl = W.snapshot_board(seed=6, w=80, h=64, layers=3, n_nets=20, median=24)
+        _run_both(e, oracle, wl.request(), rounds=4, clearance=1, via_keepout=1)
+    finally:
+        e.close()
+
+
+def test_clearance_is_checked(engine):
+    wl = W.snapshot_board(w=64, h=48, layers=2, n_nets=6, median=20)
+    req = wl.request()
+    with pytest.raises(mrcuda.InvalidArgument):
+        engine.negotiation(req, clearance=256)
+    neg = engine.negotiation(req)
+    with pytest.raises(mrcuda.InvalidArgument):  # no clearance set
+        neg.read_halo()
+    neg.round()
+    with pytest.raises(mrcuda.InvalidArgument):  # only before the first round
+        neg.engine._check(neg.engine.lib.mrc_negotiation_set_clearance(neg.engine.ctx, neg.handle, 1, 0, 16))
+    neg.close()
+    with pytest.raises(mrcuda.InvalidArgument):  # a shard sees only part of the paths
+        engine.negotiation(req, owned=[True] * 6, clearance=1)

@@ -127,3 +127,88 @@ def test_same_group_nets_share_a_corridor_without_overuse(oracle):
     for r in range(3):
         neg3.round()
     np.testing.assert_array_equal(neg3.history, neg2.history)
+
+
+# ---- clearance-halo pricing (the reference's clearance-active iteration) ----
+
+from snapshot_oracle import halo_footprint  # noqa: E402
+
+
+def test_halo_footprint_boxes_vias_and_obstacles():
+    """for_each_halo_cell on a uniform grid (negotiated.rs:3184-3271): a
+    (2r+1)^2 box per path cell on its own layer, clipped to the board, base
+    obstacles skipped, repeats kept; a via adds the keepout box on both layers."""
+    dims = Dims(6, 5, 2)
+    cost = np.ones(len(dims), np.uint32)
+    cost[dims.idx3(3, 1, 0)] = COST_MAX
+    path = [dims.idx3(0, 0, 0), dims.idx3(1, 0, 0)]
+    h = halo_footprint(path, dims, cost, 1, 0)
+    # (0,0): box x 0..1, y 0..1 = 4 cells; (1,0): x 0..2, y 0..1 = 6 cells
+    assert h.size == 10
+    cnt = np.bincount(h, minlength=len(dims))
+    assert cnt[dims.idx3(0, 0, 0)] == 2 and cnt[dims.idx3(2, 1, 0)] == 1 and cnt[dims.idx3(2, 2, 0)] == 0
+    path = [dims.idx3(2, 1, 0), dims.idx3(2, 1, 1)]
+    h = halo_footprint(path, dims, cost, 1, 2)
+    cnt = np.bincount(h, minlength=len(dims))
+    assert cnt[dims.idx3(3, 1, 0)] == 0  # an obstacle is never claimed
+    # layer 0: the r = 1 box of (2,1,0) (9 cells, one obstacle) + the r = 2 via box
+    # (x 0..4, y 0..3 = 20 cells, one obstacle); layer 1: the r = 1 box + the via box
+    assert int((cnt[:dims.plane] > 0).sum()) == 19 and int(cnt[:dims.plane].sum()) == 8 + 19
+    assert int(cnt[dims.plane:].sum()) == 9 + 20
+    assert halo_footprint(path, dims, cost, 0, 0).size == 0  # both radii 0: no footprint
+
+
+def _open_request(dims, pairs):
+    grid = Grid.filled(dims, 1)
+    nets = [NetEndpoints(f"n{i}", a, b) for i, (a, b) in enumerate(pairs)]
+    return IsolatedRouteRequest(grid, nets, [IsolatedRouteWindow.full(dims)] * len(nets), [16] * (dims.w - 1),
+                                [16] * (dims.h - 1), [40] * (dims.layers - 1))
+
+
+def test_clearance_rounds_subtract_the_nets_own_footprint(oracle):
+    """A lone net re-priced against its own path: with its own copper and
+    footprint subtracted it sees the bare board and keeps its path; without
+    the subtraction its own halo would push it to the other corner."""
+    dims = Dims(8, 8, 1)
+    req = _open_request(dims, [(dims.idx(0, 0), dims.idx(6, 6))])
+    neg = SnapshotNegotiation(oracle, req, clearance=1)
+    st = neg.round()
+    assert st["dirty"] == 1 and st["overused_edges"] == 0 and st["next_dirty"] == 0  # converged
+    first = list(neg.paths[0])
+    neg.dirty = [0]  # route it once more against a snapshot that holds its own path
+    neg.round()
+    assert neg.paths[0] == first
+    own = halo_footprint(first, dims, req.grid.cost, 1, 0)
+    np.testing.assert_array_equal(neg.halo, np.bincount(own, minlength=len(dims)).astype(np.uint32))
+    # the shared snapshot does carry the net's own footprint
+    cell = first[len(first) // 2]
+    finite = neg.snapshot[cell][neg.snapshot[cell] != COST_MAX]
+    assert finite.size and (finite > 16).all()
+    # ... and routed on it unsubtracted the net leaves its own path
+    shared = IsolatedRouteRequest(req.grid, req.nets, req.windows, req.x_edge_costs, req.y_edge_costs,
+                                  req.via_edge_costs, neg.snapshot.reshape(-1))
+    assert oracle.isolated_batch(shared, retry_full=True, mode="astar")[0][0] != first
+
+
+def test_clearance_rounds_route_every_net_until_no_overuse(oracle):
+    """Clearance-active rounds route every net every round (no rip-up before
+    pricing) while edges are overused; the halo and occupancy always equal a
+    recount of the current paths; the corridor keeps both nets dirty."""
+    dims, req = _corridor_request(["a", "b"])
+    neg = SnapshotNegotiation(oracle, req, clearance=1, via_keepout=0)
+    for _ in range(3):
+        st = neg.round()
+        assert st["dirty"] == 2 and st["next_dirty"] == 2 and st["overused_edges"] == 8
+        np.testing.assert_array_equal(neg.present, _recount(neg))
+        recount = np.zeros(len(dims), np.int64)
+        for p in neg.paths:
+            np.add.at(recount, halo_footprint(p, dims, req.grid.cost, 1, 0), 1)
+        np.testing.assert_array_equal(neg.halo, recount.astype(np.uint32))
+    wl = W.snapshot_board(w=64, h=48, layers=2, n_nets=14, median=20)
+    neg = SnapshotNegotiation(oracle, wl.request(), clearance=2, via_keepout=3)
+    for _ in range(6):
+        st = neg.round()
+        if not st["dirty"]:
+            break
+        assert st["dirty"] == 14
+        assert st["next_dirty"] in (0, 14) and (st["next_dirty"] == 0) == (st["overused_edges"] == 0)
