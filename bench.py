@@ -531,7 +531,8 @@ def measure_snapshot(args, eng, local, rounds, warmup, cpu):
                                        nt.passable_pads, nt.via_passable_pads) for i, nt in enumerate(wl.nets)]
         groups = "connections"
     req = wl.request()
-    warm = eng.negotiation(req, groups=groups)
+    clear = dict(clearance=args.clearance, via_keepout=args.via_keepout)
+    warm = eng.negotiation(req, groups=groups, **clear)
     for _ in range(warmup):
         warm.round()
     warm.close()
@@ -539,7 +540,7 @@ def measure_snapshot(args, eng, local, rounds, warmup, cpu):
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
-    neg = eng.negotiation(req, groups=groups)
+    neg = eng.negotiation(req, groups=groups, **clear)
     n_rounds = rounds
     rounds = []
     for _ in range(n_rounds):
@@ -566,6 +567,9 @@ def measure_snapshot(args, eng, local, rounds, warmup, cpu):
         "config": {"workload": wl.meta["workload"], "rounds": len(rounds), "nets_routed": routed,
                    "groups": (f"connection groups: '#'-siblings of {args.groups} nets, plus shared endpoints"
                               if args.groups else "every net its own group"),
+                   "clearance": ({"radius_cells": args.clearance, "via_keepout_cells": args.via_keepout,
+                                  "rounds": "every net every round, own copper and footprint subtracted"}
+                                 if args.clearance or args.via_keepout else None),
                    "window_cells": cells, "l2": "inputs larger than L2 (25M-cell board, 400 MB price planes)",
                    "per_round": [{k: r[k] for k in ("round", "dirty", "routed", "retried", "overused_edges",
                                                      "round_ms")} for r in rounds]},
@@ -592,7 +596,9 @@ def measure_snapshot(args, eng, local, rounds, warmup, cpu):
                                 "sample": f"{ns} nets of round 0 (snapshot = base prices), search with h = 0 "
                                           f"(directed prices), {cores} host threads, {dt:.2f} s"}
     # gpu launches: per round 4 negotiation kernels + the batch sequence (+ a retry batch)
-    line["gpu_launches"] = sum(4 + 4 + (4 if r["retried"] else 0) + (1 if groups else 0) for r in rounds)
+    # with a clearance: the footprint kernels (old out, new in), the override emit and pricing kernels
+    line["gpu_launches"] = sum(4 + 4 + (4 if r["retried"] else 0) + (1 if groups else 0)
+                               + (4 if args.clearance or args.via_keepout else 0) for r in rounds)
     neg.close()
     return line
 
@@ -806,6 +812,9 @@ def main():
     ap.add_argument("--shards", action="store_true", help="snapshot: run the sharded rounds even on one rank")
     ap.add_argument("--groups", type=int, default=0,
                     help="snapshot: group nets into '#'-sibling connection groups of this size (0 = none)")
+    ap.add_argument("--clearance", type=int, default=0,
+                    help="snapshot: clearance-halo rounds with this planar radius in cells (0 = off)")
+    ap.add_argument("--via-keepout", type=int, default=0, help="snapshot: via keepout radius in cells")
     ap.add_argument("--nets", type=int, default=0, help="route only the first N nets (0 = all)")
     ap.add_argument("--cpu-sample", type=int, default=0, help="nets timed on the CPU (0 = workload default)")
     ap.add_argument("--plain-sample", type=int, default=0, help="nets timed one per launch (0 = workload default)")

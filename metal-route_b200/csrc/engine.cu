@@ -706,6 +706,7 @@ struct mrc_batch {
     // fixed tile configuration, a shared-memory floor (every concurrent batch
     // has the same per-CTA footprint) and a divisor of the co-resident grid.
     uint32_t force_tile_h = 0, force_threads = 0, grid_num = 1, grid_div = 1;
+    bool grid_by_work = false;  // the grid may grow past grid_num/grid_div up to what the tiles can use
     bool async_q = false;  // relax schedule: asynchronous work queue instead of rounds
     bool warp = false;     // the warp-per-tile schedule (implies the queue and a +inf-filled arena)
     bool cta_planes = true;  // the CTA queue form stages step prices from the price planes by TMA
@@ -791,9 +792,13 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
         bt->graph = nullptr;
     }
     if (bt->warp && bt->max_layers > kWarpMaxLayers) bt->warp = false;  // too many layers for one warp tile
-    if (bt->warp && bt->has_over) {  // per-net price overrides are staged by the CTA queue form
-        bt->warp = false;
-        bt->cta_planes = true;
+    if (bt->has_over) {  // per-net price overrides: CTA tiles of one shape (the kernels compiled with them)
+        if (bt->warp) {
+            bt->warp = false;
+            bt->cta_planes = true;
+        }
+        tile_h = kOverTileH;
+        threads = kOverThreads;
     }
     if (bt->warp) bt->async_q = true;
     const bool cta_pl = bt->async_q && !bt->warp && bt->cta_planes;
@@ -817,13 +822,19 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     if (bt->warp) {
         MRC_CUDA(warp_relax_occupancy(&per_sm), "relax occupancy");
     } else {
-        MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q, cta_pl), "configure relax kernel");
-        MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q, cta_pl), "relax occupancy");
+        MRC_CUDA(relax_configure(tile_h, threads, bt->smem, bt->async_q, cta_pl, bt->has_over),
+                 "configure relax kernel");
+        MRC_CUDA(relax_occupancy(tile_h, threads, bt->smem, &per_sm, bt->async_q, cta_pl, bt->has_over),
+                 "relax occupancy");
     }
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
     // cooperative launch: every CTA must be co-resident
-    bt->grid = std::max<uint32_t>(
-        1u, (uint32_t)((uint64_t)ctx->sms * (uint32_t)per_sm * bt->grid_num / std::max(1u, bt->grid_div)));
+    const uint64_t full = (uint64_t)ctx->sms * (uint32_t)per_sm;
+    uint64_t grid = full * bt->grid_num / std::max(1u, bt->grid_div);
+    // a launch with work for the whole device takes it (its CTAs start as the
+    // CTAs of launches already in flight exit: the queue form needs no co-residency)
+    if (bt->grid_by_work && bt->async_q) grid = std::max(grid, std::min<uint64_t>(full, toff / kTilesPerCta));
+    bt->grid = (uint32_t)std::max<uint64_t>(1u, grid);
     // board table, with the step-price planes of every board (warp schedule,
     // CTA queue form) and their tensor maps (CTA queue form)
     if (bt->warp || cta_pl) {
@@ -1021,7 +1032,7 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
             MRC_CUDA(warp_relax_launch(ra, bt->grid, st), "launch relax kernel");
             launches += 2;  // seeds, relax
         } else {
-            MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q, cta_pl),
+            MRC_CUDA(relax_launch(ra, bt->grid, bt->threads, bt->smem, st, bt->async_q, cta_pl, bt->has_over),
                      "launch relax kernel");
             launches += bt->async_q ? 2 : 1;  // (+ the seed kernel)
         }
@@ -2412,6 +2423,7 @@ mrc_status server_launch(mrc_server *s, ServerBatch *b) {
     b->bt->async_q = true;  // the queue schedule: no grid barrier, no co-residency needed
     b->bt->grid_num = (uint32_t)b->slots.size();
     b->bt->grid_div = s->p.slots;
+    b->bt->grid_by_work = true;
     b->bt->smem_floor = s->smem_floor;
     MRC_TRY(batch_build(ctx, std::move(boards), std::move(nets), std::move(wins), b->flags, b->bt.get()));
     cudaStream_t st = s->streams[b->slots[0]];

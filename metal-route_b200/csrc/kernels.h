@@ -11,6 +11,7 @@
 namespace mrc {
 
 constexpr int kRelaxThreads = 256;  // default CTA width of the relax kernel
+constexpr uint64_t kTilesPerCta = 8;  // tiles per CTA at which a queue launch can use one more CTA
 
 // Status bits reported through Ctl::status / PathArgs::status.
 constexpr uint32_t kStatusActivationLimit = 1u << 0;
@@ -219,11 +220,15 @@ size_t relax_smem_bytes(uint32_t layers, uint32_t tile_h, bool directed, bool pl
 // `async` selects the queue-driven form (relax_async_kernel) over the
 // bulk-synchronous rounds (relax_rounds_kernel); the async form needs the label
 // arena filled with 0xFF and the queue tags (lists[cap, 2 cap)) zeroed.
-cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async = false, bool planes = false);
+// over: the fields carry directed-price overrides (DevField::n_over); those
+// kernels exist for kOverTileH-row tiles and kOverThreads threads only.
+constexpr uint32_t kOverTileH = 8, kOverThreads = 256;
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async = false, bool planes = false,
+                            bool over = false);
 cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async = false,
-                            bool planes = false);
+                            bool planes = false, bool over = false);
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
-                         bool async = false, bool planes = false);
+                         bool async = false, bool planes = false, bool over = false);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);

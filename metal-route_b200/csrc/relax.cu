@@ -486,7 +486,10 @@ static __device__ __noinline__ void stage_overrides(const DevBoard &b, const Dev
 // of 16; the tile's columns then start at xo = tx0 & 3 in the box).  Cells past
 // the window and the stacks of the net's endpoints, own pads and via pads are
 // then priced exactly (exact_in_price); the push checks read the planes.
-template <int TH, bool ASYNC, bool PL>
+// OV: the batch carries per-net directed-price overrides (negotiation with a
+// clearance; always 8-row tiles, 256 threads); without it none of the override
+// lookups is compiled in.
+template <int TH, bool ASYNC, bool PL, bool OV>
 __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, uint32_t t, uint32_t round,
                                              unsigned char *smem_raw, uint64_t *mbar, uint32_t &tma_phase) {
     const uint32_t SW = kTW + 2, SH = TH + 2;
@@ -707,13 +710,13 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         // cells where this net's own directed prices differ from the board's
         // (negotiation overrides): their four planar in-prices priced exactly
         // (the same values an overlapping exact stack writes)
-        if (f.n_over) stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, true);
+        if (OV && f.n_over) stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, true);
     } else {
         cp_async_wait_all();  // the board words copied before the label loop
         __syncthreads();
         // this net's own directed prices (negotiation overrides) replace the
         // board's words before the step prices are formed
-        if (f.n_over) {
+        if (OV && f.n_over) {
             stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, false);
             __syncthreads();
         }
@@ -845,7 +848,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             const int pin = side == 0 ? kInPosX : side == 1 ? kInNegX : side == 2 ? kInPosY : kInNegY;
             const uint32_t wp = planes_pitch(b.w);
             uint32_t step = __ldg(b.planes + (uint64_t)pin * wp * b.h * L + ((uint64_t)l * b.h + gy_n) * wp + gx_n);
-            if (step == kMax || f.n_over)
+            if (step == kMax || (OV && f.n_over))
                 step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
             if (ext2(lb, step, 1) < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
             continue;
@@ -857,7 +860,9 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
         const uint32_t cn = __ldg(b.cost + gn);
         uint32_t base;
-        if (b.directed) base = field_directed(b, f, gn, (int)dir);
+        if (b.directed)
+            base = OV ? field_directed(b, f, gn, (int)dir)
+                      : __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
         else if (side == 0) base = __ldg(b.x_edge + gx_n);
         else if (side == 1) base = __ldg(b.x_edge + gx_n - 1);
         else if (side == 2) base = __ldg(b.y_edge + gy_n);
@@ -911,7 +916,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     }
 }
 
-template <int TH, int NT>
+template <int TH, int NT, bool OV>
 __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ u64 s_item;
@@ -958,7 +963,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             const u64 item = s_item;
             if (item == kInf) break;
             uint32_t no_phase = 0;
-            process_item<TH, false, false>(a, (uint32_t)(item >> 32), (uint32_t)item, round, smem_raw, nullptr,
+            process_item<TH, false, false, OV>(a, (uint32_t)(item >> 32), (uint32_t)item, round, smem_raw, nullptr,
                                            no_phase);
         }
         grid_barrier(ctl, gridDim.x);
@@ -971,7 +976,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
 // valid from the start), and a tile is held by one CTA at a time: improvements
 // that reach a held tile mark it dirty and its holder queues it once more.
 // 64 registers a thread: four 256-thread CTAs per SM
-template <int TH, int NT, bool PL>
+template <int TH, int NT, bool PL, bool OV>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 64)) relax_async_kernel(RelaxArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ u64 s_item;
@@ -989,7 +994,7 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 64)) relax_async_kernel(Rela
         __syncthreads();
         const u64 item = s_item;
         if (item == kInf) break;
-        process_item<TH, true, PL>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw, &s_mbar, tma_phase);
+        process_item<TH, true, PL, OV>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw, &s_mbar, tma_phase);
     }
 }
 
@@ -1435,13 +1440,21 @@ namespace {
 template <int TH>
 const void *relax_fn_th(bool wide, bool async, bool planes) {
     if (async && planes)
-        return wide ? (const void *)relax_async_kernel<TH, 256, true> : (const void *)relax_async_kernel<TH, 128, true>;
+        return wide ? (const void *)relax_async_kernel<TH, 256, true, false>
+                    : (const void *)relax_async_kernel<TH, 128, true, false>;
     if (async)
-        return wide ? (const void *)relax_async_kernel<TH, 256, false> : (const void *)relax_async_kernel<TH, 128, false>;
-    return wide ? (const void *)relax_rounds_kernel<TH, 256> : (const void *)relax_rounds_kernel<TH, 128>;
+        return wide ? (const void *)relax_async_kernel<TH, 256, false, false>
+                    : (const void *)relax_async_kernel<TH, 128, false, false>;
+    return wide ? (const void *)relax_rounds_kernel<TH, 256, false> : (const void *)relax_rounds_kernel<TH, 128, false>;
 }
 
-const void *relax_fn(uint32_t tile_h, uint32_t threads, bool async, bool planes) {
+const void *relax_fn(uint32_t tile_h, uint32_t threads, bool async, bool planes, bool over) {
+    if (over) {  // the override variants exist for the 8 x 256 configuration only
+        if (tile_h != kOverTileH || threads != kOverThreads) return nullptr;
+        if (async && planes) return (const void *)relax_async_kernel<kOverTileH, kOverThreads, true, true>;
+        if (async) return (const void *)relax_async_kernel<kOverTileH, kOverThreads, false, true>;
+        return (const void *)relax_rounds_kernel<kOverTileH, kOverThreads, true>;
+    }
     const bool wide = threads >= 256;
     switch (tile_h) {
         case 8: return relax_fn_th<8>(wide, async, planes);
@@ -1461,19 +1474,23 @@ const void *seed_fn(uint32_t tile_h) {
 }
 }  // namespace
 
-cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async, bool planes) {
-    return cudaFuncSetAttribute(relax_fn(tile_h, threads, async, planes), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+cudaError_t relax_configure(uint32_t tile_h, uint32_t threads, size_t smem, bool async, bool planes, bool over) {
+    const void *fn = relax_fn(tile_h, threads, async, planes, over);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int *blocks_per_sm, bool async,
-                            bool planes) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, relax_fn(tile_h, threads, async, planes),
-                                                         (int)threads, smem);
+                            bool planes, bool over) {
+    const void *fn = relax_fn(tile_h, threads, async, planes, over);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, (int)threads, smem);
 }
 
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
-                         bool async, bool planes) {
+                         bool async, bool planes, bool over) {
+    const void *fn = relax_fn(a.tile_h, threads, async, planes, over);
+    if (!fn) return cudaErrorInvalidValue;
     RelaxArgs copy = a;
     void *args[] = {&copy};
     if (async) {
@@ -1483,7 +1500,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
             cudaError_t e = cudaLaunchKernel(seed_fn(a.tile_h), dim3((a.n_fields + 255) / 256), dim3(256), args, 0, st);
             if (e != cudaSuccess) return e;
         }
-        return cudaLaunchKernel(relax_fn(a.tile_h, threads, true, planes), dim3(grid), dim3(threads), args, smem, st);
+        return cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, st);
     }
     // Cooperative (all CTAs co-resident, checked by the CUDA runtime against occupancy);
     // the attribute form is also what stream capture records as a graph node.
@@ -1497,7 +1514,7 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, relax_fn(a.tile_h, threads, false, false), args);
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {
