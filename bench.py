@@ -782,6 +782,9 @@ def measure_serving(args, eng, local, rates, seconds, max_requests, repeats=1):
                              "largest_launch": st["largest_launch"], "peak_gb": st["peak_bytes"] / 1e9})
             lat, cells = np.array(lat), np.array(cells)
             row[name] = {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                         # the median over the repeats of each run's own p99: one host stall in one
+                         # run moves the pooled p99 above, not this one
+                         "p99_ms_median_run": float(np.median([r["p99_ms"] for r in runs])),
                          "nets_per_s": float(np.mean([r["nets_per_s"] for r in runs])),
                          "req_per_s": float(np.mean([r["req_per_s"] for r in runs])),
                          "by_size": {c: {"requests": int(((cells >= lo) & (cells < hi)).sum()),

@@ -696,6 +696,7 @@ struct mrc_batch {
     uint64_t total_cells = 0;
     uint32_t total_tiles = 0, max_tiles = 0, tile_h = 32, threads = kRelaxThreads, grid = 1;
     size_t smem = 0;
+    DBuf d_tover;                  // per tile: holds price overrides of its field (has_over batches)
     DBuf d_boards, d_fields, d_pads, d_lab, d_tstamp, d_tvisit, d_lists, d_costs, d_lens, d_offsets, d_cells, d_ctl,
         d_out;
     uint32_t launches = 0;
@@ -875,6 +876,8 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
     MRC_TRY(upload(ctx, bt->d_fields, bt->fields.data(), bt->fields.size() * sizeof(DevField), "upload fields"));
     MRC_TRY(bt->d_tstamp.get(ctx, (size_t)bt->total_tiles * 4, "tile stamps"));
     MRC_TRY(bt->d_tvisit.get(ctx, (size_t)bt->total_tiles * 4, "tile flags"));
+    if (bt->has_over) MRC_TRY(bt->d_tover.get(ctx, (size_t)bt->total_tiles, "override tile flags"));
+    else bt->d_tover.reset();
     MRC_TRY(bt->d_lists.get(ctx, (size_t)bt->total_tiles * 3 * 8, "tile lists"));
     return MRC_OK;
 }
@@ -972,13 +975,14 @@ mrc_status batch_build(mrc_context *ctx, std::vector<const mrc_board *> boards, 
 }
 
 PathArgs path_args(const mrc_batch *bt) {
-    PathArgs pa;
+    PathArgs pa{};
     pa.boards = bt->d_boards.as<DevBoard>();
     pa.fields = bt->d_fields.as<DevField>();
     pa.n_fields = (uint32_t)bt->fields.size();
     pa.pads = bt->d_pads.as<uint32_t>();
     pa.lab = bt->d_lab.as<u64>();
     pa.tvisit = bt->d_tvisit.as<uint32_t>();
+    pa.tover = bt->has_over ? bt->d_tover.as<uint8_t>() : nullptr;
     pa.tile_h = bt->tile_h;
     pa.arena_filled = bt->async_q ? 1u : 0u;
     pa.costs = bt->d_costs.as<uint32_t>();
@@ -998,7 +1002,7 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
     MRC_CUDA(cudaMemsetAsync(bt->d_ctl.p, 0, sizeof(Ctl), st), "reset control block");
     MRC_CUDA(cudaMemsetAsync(bt->d_tstamp.p, 0, (size_t)bt->total_tiles * 4, st), "reset tile stamps");
     MRC_CUDA(cudaMemsetAsync(bt->d_tvisit.p, 0, (size_t)bt->total_tiles * 4, st), "reset tile flags");
-    RelaxArgs ra;
+    RelaxArgs ra{};
     ra.boards = bt->d_boards.as<DevBoard>();
     ra.max_layers = bt->max_layers;
     ra.fields = bt->d_fields.as<DevField>();
@@ -1007,6 +1011,15 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
     ra.lab = bt->d_lab.as<u64>();
     ra.tstamp = bt->d_tstamp.as<uint32_t>();
     ra.tvisit = bt->d_tvisit.as<uint32_t>();
+    ra.tover = nullptr;
+    if (bt->has_over && n) {
+        MRC_CUDA(cudaMemsetAsync(bt->d_tover.p, 0, (size_t)bt->total_tiles, st), "reset override tile flags");
+        MRC_CUDA(mark_over_tiles_launch(bt->d_fields.as<DevField>(), n, bt->d_boards.as<DevBoard>(), bt->tile_h,
+                                        bt->d_tover.as<uint8_t>(), st),
+                 "mark override tiles");
+        ++launches;
+        ra.tover = bt->d_tover.as<uint8_t>();
+    }
     ra.lists = bt->d_lists.as<u64>();
     ra.list_cap = bt->total_tiles;
     ra.ctl = bt->d_ctl.as<Ctl>();
@@ -2882,7 +2895,7 @@ mrc_status plain_one(mrc_context *ctx, const mrc_board *board, const NetCopy &ne
     MRC_TRY(d_lens.get(ctx, 4, "plain len"));
     MRC_TRY(d_off.get(ctx, 16, "plain offsets"));
     MRC_TRY(d_cells.get(ctx, wc * 4, "plain path"));
-    PathArgs pt;
+    PathArgs pt{};
     pt.boards = d_board.as<DevBoard>();
     pt.fields = d_field.as<DevField>();
     pt.n_fields = 1;
@@ -3169,7 +3182,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     MRC_CUDA(relax_configure(tile_h, kRelaxThreads, smem), "configure relax kernel");
     MRC_CUDA(relax_occupancy(tile_h, kRelaxThreads, smem, &per_sm), "relax occupancy");
     if (per_sm < 1) return fail(MRC_ERR_LIMIT, "relax kernel does not fit on one SM");
-    RelaxArgs ra;
+    RelaxArgs ra{};
     ra.boards = reinterpret_cast<const DevBoard *>(s + o_btab);
     ra.max_layers = g.layers;
     ra.fields = reinterpret_cast<const DevField *>(s + o_fields);
@@ -3185,7 +3198,7 @@ extern "C" mrc_status mrc_route_isolated_batch_noalloc(const mrc_isolated_reques
     ra.round_limit = 64u * max_tiles + 4096u;
     ra.activation_limit = ~0ull;
     MRC_CUDA(relax_launch(ra, (uint32_t)dev->sms * (uint32_t)per_sm, kRelaxThreads, smem, st), "launch relax kernel");
-    PathArgs pa;
+    PathArgs pa{};
     pa.boards = ra.boards;
     pa.fields = ra.fields;
     pa.n_fields = n;

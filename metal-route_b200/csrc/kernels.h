@@ -29,6 +29,7 @@ struct RelaxArgs {
     u64 *lab;                   // label arena (dist << 32 | hops)
     uint32_t *tstamp;           // per tile: last round it was queued for, + 1 (zeroed)
     uint32_t *tvisit;           // per tile: labels valid (zeroed)
+    const uint8_t *tover;       // nullable: per tile, 1 = its field has directed-price overrides inside it
     u64 *lists;                 // 3 rotating lists of (field << 32 | tile)
     uint32_t list_cap;          // total tiles of the batch
     Ctl *ctl;                   // zeroed before launch
@@ -44,6 +45,7 @@ struct PathArgs {
     const uint32_t *pads;
     const u64 *lab;
     const uint32_t *tvisit;
+    const uint8_t *tover;            // nullable: as RelaxArgs::tover
     uint32_t tile_h;
     uint32_t arena_filled;           // 1: the label arena was +inf-filled (queue schedule), tvisit not needed
     uint32_t *costs;                 // [n] by output slot
@@ -229,6 +231,10 @@ cudaError_t relax_occupancy(uint32_t tile_h, uint32_t threads, size_t smem, int 
                             bool planes = false, bool over = false);
 cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
                          bool async = false, bool planes = false, bool over = false);
+// tover[f.tile_off + t] = 1 for every tile t of every field that holds one of
+// the field's directed-price overrides (tover zeroed before).
+cudaError_t mark_over_tiles_launch(const DevField *fields, uint32_t n_fields, const DevBoard *boards, uint32_t tile_h,
+                                   uint8_t *tover, cudaStream_t st);
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st);
 cudaError_t fields_launch(const PathArgs &a, uint32_t *out, uint64_t total, cudaStream_t st);
 cudaError_t plain_round_launch(const PlainArgs &a, uint64_t wcells, cudaStream_t st);

@@ -710,13 +710,14 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         // cells where this net's own directed prices differ from the board's
         // (negotiation overrides): their four planar in-prices priced exactly
         // (the same values an overlapping exact stack writes)
-        if (OV && f.n_over) stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, true);
+        if (OV && f.n_over && a.tover[f.tile_off + t])
+            stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, true);
     } else {
         cp_async_wait_all();  // the board words copied before the label loop
         __syncthreads();
         // this net's own directed prices (negotiation overrides) replace the
         // board's words before the step prices are formed
-        if (OV && f.n_over) {
+        if (OV && f.n_over && a.tover[f.tile_off + t]) {
             stage_overrides(b, f, a.pads, tile.st, L, TH, tile.sp, tile.xo, tx0, ty0, tw, th, false);
             __syncthreads();
         }
@@ -841,6 +842,12 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         if (!exists || s_push[side]) continue;
         const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
         if (lb == kInf) continue;
+        // the neighbour tile holds cells this net prices with its own overrides
+        bool nb_over = false;
+        if constexpr (OV) {
+            const uint32_t u = side == 0 ? t - 1 : side == 1 ? t + 1 : side == 2 ? t - ntx : t + ntx;
+            nb_over = f.n_over && a.tover[f.tile_off + u];
+        }
         if constexpr (PL) {
             // the planes hold the price into the neighbour cell; an own pad or
             // endpoint of this net there is priced exactly
@@ -848,7 +855,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             const int pin = side == 0 ? kInPosX : side == 1 ? kInNegX : side == 2 ? kInPosY : kInNegY;
             const uint32_t wp = planes_pitch(b.w);
             uint32_t step = __ldg(b.planes + (uint64_t)pin * wp * b.h * L + ((uint64_t)l * b.h + gy_n) * wp + gx_n);
-            if (step == kMax || (OV && f.n_over))
+            if (step == kMax || nb_over)
                 step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
             if (ext2(lb, step, 1) < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
             continue;
@@ -861,8 +868,8 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         const uint32_t cn = __ldg(b.cost + gn);
         uint32_t base;
         if (b.directed)
-            base = OV ? field_directed(b, f, gn, (int)dir)
-                      : __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
+            base = nb_over ? field_directed(b, f, gn, (int)dir)
+                           : __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
         else if (side == 0) base = __ldg(b.x_edge + gx_n);
         else if (side == 1) base = __ldg(b.x_edge + gx_n - 1);
         else if (side == 2) base = __ldg(b.y_edge + gy_n);
@@ -1131,14 +1138,20 @@ __device__ __forceinline__ uint32_t global_step(const DevBoard &b, const DevFiel
 // global_step for the path walk with every load issued before any is used
 // (the flags of both cells, the enter cost and the base price), so a step costs
 // one memory round trip instead of a chain of dependent ones.
+// own: cur's tile holds directed-price overrides of this field.
 __device__ __forceinline__ uint32_t walk_step(const DevBoard &b, const DevField &f, const uint32_t *pads,
-                                              uint32_t p, uint32_t cur, uint32_t x, uint32_t y, uint32_t l, int kind) {
+                                              uint32_t p, uint32_t cur, uint32_t x, uint32_t y, uint32_t l, int kind,
+                                              bool own) {
     const uint8_t fc = b.flags ? __ldg(b.flags + cur) : 0, fp = b.flags ? __ldg(b.flags + p) : 0;
     const uint32_t cc = __ldg(b.cost + cur);
     uint32_t base = 0;
     if (kind == 0) base = __ldg(b.via_edge + l - 1);
     else if (kind == 5) base = __ldg(b.via_edge + l);
-    else if (b.directed) base = field_directed(b, f, cur, kind == 1 ? 0 : kind == 2 ? 1 : kind == 3 ? 2 : 3);
+    else if (b.directed) {
+        const int slot = kind == 1 ? 0 : kind == 2 ? 1 : kind == 3 ? 2 : 3;
+        base = own ? field_directed(b, f, cur, slot)
+                   : __ldg(reinterpret_cast<const uint32_t *>(b.directed + cur) + slot);
+    }
     else if (kind == 1) base = __ldg(b.y_edge + y - 1);
     else if (kind == 2) base = __ldg(b.x_edge + x - 1);
     else if (kind == 3) base = __ldg(b.x_edge + x);
@@ -1212,7 +1225,10 @@ __device__ __forceinline__ bool walk_try(const PathArgs &a, const DevField &f, c
     if (!walk_inside(f, b, px, py, pl)) return false;
     *q = ((uint32_t)pl * b.h + (uint32_t)py) * b.w + (uint32_t)px;
     *lq = walk_label(a, f, ntx, tile_shift, px, py, pl);
-    const uint32_t st = walk_step(b, f, a.pads, *q, t, (uint32_t)tx, (uint32_t)ty, (uint32_t)tl, kind);
+    bool own = false;
+    if (a.tover && f.n_over)
+        own = a.tover[f.tile_off + (((uint32_t)ty - f.y0) >> tile_shift) * ntx + ((uint32_t)tx - f.x0) / kTW] != 0;
+    const uint32_t st = walk_step(b, f, a.pads, *q, t, (uint32_t)tx, (uint32_t)ty, (uint32_t)tl, kind, own);
     return *lq != kInf && extend(*lq, st) == need;
 }
 
@@ -1515,6 +1531,34 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+namespace {
+// One warp per field: every override cell inside the window flags its tile.
+__global__ void mark_over_tiles_kernel(const DevField *fields, uint32_t n_fields, const DevBoard *boards,
+                                       uint32_t tile_h, uint8_t *tover) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t fi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; fi < n_fields; fi += warps) {
+        const DevField f = fields[fi];
+        if (!f.n_over) continue;
+        const DevBoard b = boards[f.board];
+        const uint32_t plane = b.w * b.h, ntx = (f.ww + kTW - 1) / kTW;
+        for (uint32_t k = lane; k < f.n_over; k += 32) {
+            const uint32_t c = b.over_cells[f.over_off + k], r = c % plane, x = r % b.w, y = r / b.w;
+            if (x < f.x0 || x >= f.x0 + f.ww || y < f.y0 || y >= f.y0 + f.wh) continue;
+            tover[f.tile_off + ((y - f.y0) / tile_h) * ntx + (x - f.x0) / kTW] = 1;
+        }
+    }
+}
+}  // namespace
+
+cudaError_t mark_over_tiles_launch(const DevField *fields, uint32_t n_fields, const DevBoard *boards, uint32_t tile_h,
+                                   uint8_t *tover, cudaStream_t st) {
+    if (!n_fields) return cudaSuccess;
+    const uint32_t blocks = (uint32_t)std::min<uint64_t>(((uint64_t)n_fields * 32 + 255) / 256, 148ull * 16);
+    mark_over_tiles_kernel<<<blocks, 256, 0, st>>>(fields, n_fields, boards, tile_h, tover);
+    return cudaGetLastError();
 }
 
 cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {
