@@ -773,144 +773,197 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     __syncthreads();
 
     // ---- relax to local convergence ---------------------------------
+    // Queue form: a tile that a neighbour improved while this CTA held it is
+    // continued here (up to kContinueLimit times): its halo ring is read again
+    // and the sweeps resume on the staged tile, without a release, a queue
+    // round trip and a full re-staging.  Each continuation counts as an
+    // activation.
     const uint32_t sweep_limit = L * kTW * TH + 4;
-    uint32_t sweep = 0;
-    for (;;) {
-        const bool ch = relax_tile<TH>(tile);
-        ++sweep;
-        const int any = __syncthreads_or(ch ? 1 : 0);
-        if (!any) break;
-        if (sweep > sweep_limit) {
-            if (tid == 0) atomicOr(&ctl->status, kStatusRoundLimit);
-            break;
-        }
-    }
-
-    // ---- write back and find neighbours this tile can improve -------
-    u64 *labw = a.lab + f.lab_off;
-    // the tile is held by this CTA alone (both schedules), so plain stores;
-    // indices are split by the compile-time tile shape (cells past a ragged
-    // window edge are skipped).  Only labels that fell are stored, unless the
-    // arena holds nothing valid for this tile yet (first visit, rounds form).
-    const bool all_labels = !ASYNC && !s_vis[0];
-    for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
-        const uint32_t tx = i % kTW, r = i / kTW, ty = r % TH, l = r / TH;
-        if (tx >= tw || ty >= th) continue;
-        if (!all_labels && !((tile.fellw[l * TH + ty] >> tx) & 1u)) continue;
-        const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
-        labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
-    }
-    // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
-    const uint32_t nb = 2 * L * TH + 2 * L * kTW;
-    for (uint32_t i = tid; i < nb; i += blockDim.x) {
-        uint32_t side, l, k;
-        if (i < 2 * L * TH) {
-            side = i >= L * TH;
-            const uint32_t r = i - side * L * TH;
-            l = r / TH;
-            k = r % TH;
-            if (k >= th) continue;
-        } else {
-            const uint32_t j = i - 2 * L * TH;
-            const uint32_t hi = j >= L * kTW;
-            side = 2 + hi;
-            const uint32_t r = j - hi * L * kTW;
-            l = r / kTW;
-            k = r % kTW;
-            if (k >= tw) continue;
-        }
-        bool exists;
-        uint32_t bsx, bsy, nsx, nsy, dir;
-        uint8_t out_bit, in_bit;
-        if (side == 0) {
-            exists = txi > 0;
-            bsx = 1; bsy = k + 1; nsx = 0; nsy = bsy;
-            dir = 2; out_bit = kEdgeNegX; in_bit = kEdgePosX;
-        } else if (side == 1) {
-            exists = txi + 1 < ntx;
-            bsx = tw; bsy = k + 1; nsx = tw + 1; nsy = bsy;
-            dir = 1; out_bit = kEdgePosX; in_bit = kEdgeNegX;
-        } else if (side == 2) {
-            exists = tyi > 0;
-            bsx = k + 1; bsy = 1; nsx = bsx; nsy = 0;
-            dir = 3; out_bit = kEdgeNegY; in_bit = kEdgePosY;
-        } else {
-            exists = tyi + 1 < nty;
-            bsx = k + 1; bsy = th; nsx = bsx; nsy = th + 1;
-            dir = 0; out_bit = kEdgePosY; in_bit = kEdgeNegY;
-        }
-        if (!exists || s_push[side]) continue;
-        const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
-        if (lb == kInf) continue;
-        // the neighbour tile holds cells this net prices with its own overrides
-        bool nb_over = false;
-        if constexpr (OV) {
-            const uint32_t u = side == 0 ? t - 1 : side == 1 ? t + 1 : side == 2 ? t - ntx : t + ntx;
-            nb_over = f.n_over && a.tover[f.tile_off + u];
-        }
-        if constexpr (PL) {
-            // the planes hold the price into the neighbour cell; an own pad or
-            // endpoint of this net there is priced exactly
-            const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
-            const int pin = side == 0 ? kInPosX : side == 1 ? kInNegX : side == 2 ? kInPosY : kInNegY;
-            const uint32_t wp = planes_pitch(b.w);
-            uint32_t step = __ldg(b.planes + (uint64_t)pin * wp * b.h * L + ((uint64_t)l * b.h + gy_n) * wp + gx_n);
-            if (step == kMax || nb_over)
-                step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
-            if (ext2(lb, step, 1) < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
-            continue;
-        }
-        const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
-        const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
-        const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
-        // the neighbour's enter cost and in-price, both loaded before either is used
-        const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
-        const uint32_t cn = __ldg(b.cost + gn);
-        uint32_t base;
-        if (b.directed)
-            base = nb_over ? field_directed(b, f, gn, (int)dir)
-                           : __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
-        else if (side == 0) base = __ldg(b.x_edge + gx_n);
-        else if (side == 1) base = __ldg(b.x_edge + gx_n - 1);
-        else if (side == 2) base = __ldg(b.y_edge + gy_n);
-        else base = __ldg(b.y_edge + gy_n - 1);
-        uint32_t en = kMax;  // cell_enter of the neighbour
-        if (!(fn & kTraceNode)) en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
-        if (en == kMax) continue;
-        uint32_t step = kMax;  // planar_step_g on the loaded values
-        if (!((fb & out_bit) | (fn & in_bit)) && !(b.directed && base == kMax)) step = capmul(base, en);
-        const u64 cand = ext2(lb, step, 1);
-        if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
-    }
-    __syncthreads();
-    if (tid < 5) {
-        __threadfence();  // labels before the visited flag and the queue entries
-        if (tid == 4) {
-            if constexpr (ASYNC) {
-                if (!__ldcg(a.tvisit + f.tile_off + t)) atomicExch(a.tvisit + f.tile_off + t, 1u);
-                if (atomicAdd(&ctl->activations, 1ull) >= a.activation_limit)
-                    atomicOr(&ctl->status, kStatusActivationLimit);
-            } else {
-                if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
-                atomicAdd(&ctl->activations, 1ull);
+    __shared__ uint32_t s_more;
+    for (uint32_t cont = 0;; ++cont) {
+        uint32_t sweep = 0;
+        for (;;) {
+            const bool ch = relax_tile<TH>(tile);
+            ++sweep;
+            const int any = __syncthreads_or(ch ? 1 : 0);
+            if (!any) break;
+            if (sweep > sweep_limit) {
+                if (tid == 0) atomicOr(&ctl->status, kStatusRoundLimit);
+                break;
             }
-            atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
-        } else if (s_push[tid]) {
-            const uint32_t u = tid == 0 ? t - 1 : tid == 1 ? t + 1 : tid == 2 ? t - ntx : t + ntx;
-            if constexpr (ASYNC) {
-                async_push(a, fi, f.tile_off, u);
+        }
+
+        // ---- write back and find neighbours this tile can improve -------
+        u64 *labw = a.lab + f.lab_off;
+        // the tile is held by this CTA alone (both schedules), so plain stores;
+        // indices are split by the compile-time tile shape (cells past a ragged
+        // window edge are skipped).  Only labels that fell are stored, unless the
+        // arena holds nothing valid for this tile yet (first visit, rounds form).
+        const bool all_labels = !ASYNC && !s_vis[0];
+        for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
+            const uint32_t tx = i % kTW, r = i / kTW, ty = r % TH, l = r / TH;
+            if (tx >= tw || ty >= th) continue;
+            if (!all_labels && !((tile.fellw[l * TH + ty] >> tx) & 1u)) continue;
+            const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
+            labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
+        }
+        // borders: 0 = left (-x), 1 = right (+x), 2 = top (-y), 3 = bottom (+y)
+        const uint32_t nb = 2 * L * TH + 2 * L * kTW;
+        for (uint32_t i = tid; i < nb; i += blockDim.x) {
+            uint32_t side, l, k;
+            if (i < 2 * L * TH) {
+                side = i >= L * TH;
+                const uint32_t r = i - side * L * TH;
+                l = r / TH;
+                k = r % TH;
+                if (k >= th) continue;
             } else {
-                const uint32_t want = round + 2;  // stamp s = queued for round s-1
-                if (atomicMax(a.tstamp + f.tile_off + u, want) < want) {
-                    const uint32_t nxt = (round + 1) % 3;
-                    const uint32_t idx = atomicAdd(&ctl->count[nxt], 1u);
-                    if (idx < cap) {
-                        a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | u;
-                    } else {
-                        atomicOr(&ctl->status, kStatusQueueOverflow);
+                const uint32_t j = i - 2 * L * TH;
+                const uint32_t hi = j >= L * kTW;
+                side = 2 + hi;
+                const uint32_t r = j - hi * L * kTW;
+                l = r / kTW;
+                k = r % kTW;
+                if (k >= tw) continue;
+            }
+            bool exists;
+            uint32_t bsx, bsy, nsx, nsy, dir;
+            uint8_t out_bit, in_bit;
+            if (side == 0) {
+                exists = txi > 0;
+                bsx = 1; bsy = k + 1; nsx = 0; nsy = bsy;
+                dir = 2; out_bit = kEdgeNegX; in_bit = kEdgePosX;
+            } else if (side == 1) {
+                exists = txi + 1 < ntx;
+                bsx = tw; bsy = k + 1; nsx = tw + 1; nsy = bsy;
+                dir = 1; out_bit = kEdgePosX; in_bit = kEdgeNegX;
+            } else if (side == 2) {
+                exists = tyi > 0;
+                bsx = k + 1; bsy = 1; nsx = bsx; nsy = 0;
+                dir = 3; out_bit = kEdgeNegY; in_bit = kEdgePosY;
+            } else {
+                exists = tyi + 1 < nty;
+                bsx = k + 1; bsy = th; nsx = bsx; nsy = th + 1;
+                dir = 0; out_bit = kEdgePosY; in_bit = kEdgeNegY;
+            }
+            if (!exists || s_push[side]) continue;
+            const u64 lb = tile.lab[tile.li(l, bsy, bsx)];
+            if (lb == kInf) continue;
+            // the neighbour tile holds cells this net prices with its own overrides
+            bool nb_over = false;
+            if constexpr (OV) {
+                const uint32_t u = side == 0 ? t - 1 : side == 1 ? t + 1 : side == 2 ? t - ntx : t + ntx;
+                nb_over = f.n_over && a.tover[f.tile_off + u];
+            }
+            if constexpr (PL) {
+                // the planes hold the price into the neighbour cell; an own pad or
+                // endpoint of this net there is priced exactly
+                const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
+                const int pin = side == 0 ? kInPosX : side == 1 ? kInNegX : side == 2 ? kInPosY : kInNegY;
+                const uint32_t wp = planes_pitch(b.w);
+                uint32_t step = __ldg(b.planes + (uint64_t)pin * wp * b.h * L + ((uint64_t)l * b.h + gy_n) * wp + gx_n);
+                if (step == kMax || nb_over)
+                    step = exact_in_price(b, f, a.pads, pin, (l * b.h + gy_n) * b.w + gx_n, l, gy_n, gx_n);
+                if (ext2(lb, step, 1) < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
+                continue;
+            }
+            const uint32_t gn = (l * b.h + (uint32_t)(ty0 + (int)nsy - 1)) * b.w + (uint32_t)(tx0 + (int)nsx - 1);
+            const uint8_t fb = tile.fl[(l * SH + bsy) * kFlPitch + bsx];
+            const uint8_t fn = tile.fl[(l * SH + nsy) * kFlPitch + nsx];
+            // the neighbour's enter cost and in-price, both loaded before either is used
+            const uint32_t gx_n = (uint32_t)(tx0 + (int)nsx - 1), gy_n = (uint32_t)(ty0 + (int)nsy - 1);
+            const uint32_t cn = __ldg(b.cost + gn);
+            uint32_t base;
+            if (b.directed)
+                base = nb_over ? field_directed(b, f, gn, (int)dir)
+                               : __ldg(reinterpret_cast<const uint32_t *>(b.directed + gn) + dir);
+            else if (side == 0) base = __ldg(b.x_edge + gx_n);
+            else if (side == 1) base = __ldg(b.x_edge + gx_n - 1);
+            else if (side == 2) base = __ldg(b.y_edge + gy_n);
+            else base = __ldg(b.y_edge + gy_n - 1);
+            uint32_t en = kMax;  // cell_enter of the neighbour
+            if (!(fn & kTraceNode)) en = cn != kMax ? cn : (is_own_pad(gn) ? 1u : kMax);
+            if (en == kMax) continue;
+            uint32_t step = kMax;  // planar_step_g on the loaded values
+            if (!((fb & out_bit) | (fn & in_bit)) && !(b.directed && base == kMax)) step = capmul(base, en);
+            const u64 cand = ext2(lb, step, 1);
+            if (cand < tile.lab[tile.li(l, nsy, nsx)]) s_push[side] = 1;
+        }
+        __syncthreads();
+        if (tid < 5) {
+            __threadfence();  // labels before the visited flag and the queue entries
+            if (tid == 4) {
+                if constexpr (ASYNC) {
+                    if (!__ldcg(a.tvisit + f.tile_off + t)) atomicExch(a.tvisit + f.tile_off + t, 1u);
+                    if (atomicAdd(&ctl->activations, 1ull) >= a.activation_limit)
+                        atomicOr(&ctl->status, kStatusActivationLimit);
+                } else {
+                    if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
+                    atomicAdd(&ctl->activations, 1ull);
+                }
+                atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
+            } else if (s_push[tid]) {
+                const uint32_t u = tid == 0 ? t - 1 : tid == 1 ? t + 1 : tid == 2 ? t - ntx : t + ntx;
+                if constexpr (ASYNC) {
+                    async_push(a, fi, f.tile_off, u);
+                } else {
+                    const uint32_t want = round + 2;  // stamp s = queued for round s-1
+                    if (atomicMax(a.tstamp + f.tile_off + u, want) < want) {
+                        const uint32_t nxt = (round + 1) % 3;
+                        const uint32_t idx = atomicAdd(&ctl->count[nxt], 1u);
+                        if (idx < cap) {
+                            a.lists[(size_t)nxt * cap + idx] = ((u64)fi << 32) | u;
+                        } else {
+                            atomicOr(&ctl->status, kStatusQueueOverflow);
+                        }
                     }
                 }
             }
+        }
+        __syncthreads();
+        if constexpr (!ASYNC) {
+            break;
+        } else {
+            if (tid == 0) {
+                __threadfence();
+                s_more = cont + 1 < kContinueLimit &&
+                         atomicCAS(a.tstamp + f.tile_off + t, kTileHeldDirty, kTileHeld) == kTileHeldDirty;
+            }
+            __syncthreads();
+            if (!s_more) break;
+            __threadfence();  // the neighbours' labels were written before they marked this tile
+            if (tid < 4) s_push[tid] = 0;
+            for (uint32_t i = tid; i < L * TH; i += blockDim.x) tile.fellw[i] = 0;
+            // the halo ring again: an improved cell marks the line that ends at it
+            const uint32_t nr = 2 * L * TH + 2 * L * kTW;
+            for (uint32_t i = tid; i < nr; i += blockDim.x) {
+                uint32_t l, sx, sy;
+                bool row;
+                if (i < 2 * L * TH) {
+                    const uint32_t side = i >= L * TH, r = i - side * L * TH;
+                    l = r / TH;
+                    sy = r % TH + 1;
+                    if (sy > th || (side ? txi + 1 >= ntx : txi == 0)) continue;
+                    sx = side ? tw + 1 : 0;
+                    row = true;
+                } else {
+                    const uint32_t k = i - 2 * L * TH, side = k >= L * kTW, r = k - side * L * kTW;
+                    l = r / kTW;
+                    sx = r % kTW + 1;
+                    if (sx > tw || (side ? tyi + 1 >= nty : tyi == 0)) continue;
+                    sy = side ? th + 1 : 0;
+                    row = false;
+                }
+                const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
+                const u64 v = __ldcg(lab + ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0));
+                u64 &cur = tile.lab[tile.li(l, sy, sx)];
+                if (v < cur) {
+                    cur = v;
+                    if (row) tile.rowd[l * TH + sy - 1] = 1;
+                    else tile.cold[l * kTW + sx - 1] = 1;
+                }
+            }
+            __syncthreads();
         }
     }
     __syncthreads();

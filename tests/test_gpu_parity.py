@@ -235,7 +235,7 @@ def test_deterministic_across_calls_and_batches(engine):
     board2 = e2.board(wl.grid, wl.x, wl.y, wl.vias, wl.directed)
     batch2 = mrcuda.Batch(board2, wl.nets, wl.windows)
     tuned = batch2.autotune()
-    assert tuned["schedule"] in (0, 1, 2)
+    assert tuned["schedule"] in (0, 1, 2, 3)
     assert tuned["tile_h"] in (8, 16, 32, 64) and tuned["threads"] in (128, 256)
     batch2.launch()
     c = batch2.finish()
