@@ -410,9 +410,9 @@ def other_workloads(args, eng, local):
     out["snapshot"] = _summary(line)
     out["snapshot"]["per_round"] = line["config"]["per_round"]
     rows, clk = measure_serving(args, eng, local, rates=[20.0, 100.0, 400.0], seconds=2.0, max_requests=400,
-                                repeats=1)
-    out["serving"] = {"workload": "serving, Poisson arrivals (3 rates, 2 s of arrivals each)", "rates": rows,
-                      "clocks": clk}
+                                repeats=3)
+    out["serving"] = {"workload": "serving, Poisson arrivals (3 rates, 2 s of arrivals each, 3 draws per rate)",
+                      "rates": rows, "clocks": clk}
     return out
 
 
@@ -766,6 +766,12 @@ def measure_serving(args, eng, local, rates, seconds, max_requests, repeats=1):
 
     def pct(v, q):
         return float(np.percentile(v, q)) if len(v) else None
+
+    # warm-up, unmeasured: one short trace through each loop (first-use costs of
+    # the process: kernel modules, the engine's memory pool)
+    warm = W.serving_trace(pool, rates[0], 20, seed=999)
+    _run_trace(eng, warm, args.slots, 64, boards)
+    _run_trace(eng, warm, 1, 1, boards)
 
     for rate in rates:
         n = max(20, min(int(rate * seconds), max_requests))

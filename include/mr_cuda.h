@@ -440,7 +440,8 @@ void mrc_negotiation_destroy(mrc_negotiation *neg);
  * thread and return at once with a ticket; one dispatcher thread
  *   - admits queued requests in arrival order while the device memory they
  *     need (boards, labels, paths, tile state) fits the HBM budget
- *     (hbm_fraction of the device's memory, minus what was in use at creation),
+ *     (hbm_fraction of the device's memory, minus what was in use at creation;
+ *     the engine's own free cached blocks count as available),
  *   - merges every admitted request with the same flags, up to
  *     max_batch_requests / max_batch_cells, into ONE persistent launch over
  *     all of their boards (each request's board is uploaded into HBM and stays

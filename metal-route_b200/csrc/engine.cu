@@ -77,6 +77,7 @@ class Pool {
         if (it != free_.end() && it->first <= 2 * bytes + (8u << 20)) {
             *out = it->second;
             used_[it->second] = it->first;
+            cached_ -= it->first;
             free_.erase(it);
             return cudaSuccess;
         }
@@ -100,16 +101,21 @@ class Pool {
         auto it = used_.find(p);
         if (it == used_.end()) return;
         free_.emplace(it->second, p);
+        cached_ += it->second;
         used_.erase(it);
     }
     void trim() {
         for (auto &kv : free_) cudaFree(kv.second);
         free_.clear();
+        cached_ = 0;
     }
+    // bytes held in free blocks (device memory the pool can hand out again)
+    size_t cached() const { return cached_; }
 
    private:
     std::multimap<size_t, void *> free_;
     std::unordered_map<void *, size_t> used_;
+    size_t cached_ = 0;
 };
 
 }  // namespace
@@ -2659,10 +2665,13 @@ mrc_status mrc_server_create(mrc_context *ctx, const mrc_server_params *params, 
     {
         Lock lock(ctx, 0);
         MRC_TRY(set_device(ctx));
-        ctx->pool.trim();
+        // the pool's free blocks count as available: they are kept (not
+        // released, which would synchronise the device) so that large requests
+        // find a block instead of waiting on a fresh cudaMalloc
         size_t free_b = 0, total_b = 0;
         MRC_CUDA(cudaMemGetInfo(&free_b, &total_b), "device memory");
-        const double allowed = (double)s->p.hbm_fraction * (double)total_b - (double)(total_b - free_b);
+        const double used = (double)(total_b - free_b) - (double)ctx->pool.cached();
+        const double allowed = (double)s->p.hbm_fraction * (double)total_b - std::max(used, 0.0);
         s->budget = allowed > 0 ? (size_t)allowed : 0;
         s->tile_h = 8;
         s->threads = kRelaxThreads;

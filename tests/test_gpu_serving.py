@@ -124,11 +124,13 @@ def test_memory_admission(engine):
     srv = engine.server(slots=2, hbm_fraction=0.8)
     budget = srv.stats()["budget_bytes"]
     srv.close()
-    # a fraction that leaves about 150 MB above what is already in use
+    # a fraction that leaves about 150 MB above what is already in use (the
+    # budget counts the engine's own free pool blocks as available, so "in use"
+    # is 0.8 * total - budget, not what the driver reports as taken)
     import torch
 
-    f, t = torch.cuda.mem_get_info()
-    frac = (t - f + 150e6) / t
+    _, t = torch.cuda.mem_get_info()
+    frac = (0.8 * t - budget + 150e6) / t
     srv = engine.server(slots=2, hbm_fraction=frac)
     small = srv.stats()["budget_bytes"]
     assert 0 < small < budget
