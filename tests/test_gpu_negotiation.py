@@ -215,3 +215,15 @@ def test_clearance_is_checked(engine):
     neg.close()
     with pytest.raises(mrcuda.InvalidArgument):  # a shard sees only part of the paths
         engine.negotiation(req, owned=[True] * 6, clearance=1)
+
+
+def test_clearance_with_connection_groups(engine, oracle):
+    """Clearance rounds with group-aware overuse: prices count every other
+    net's copper and footprint, overuse counts groups (copper only)."""
+    wl = W.snapshot_board(seed=11, w=96, h=72, layers=2, n_nets=24, median=28)
+    req = wl.request()
+    nets = [NetEndpoints(f"c{i // 4}#{i % 4}", nt.src, nt.dst, nt.passable_pads, nt.via_passable_pads)
+            for i, nt in enumerate(req.nets)]
+    req = IsolatedRouteRequest(req.grid, nets, req.windows, req.x_edge_costs, req.y_edge_costs, req.via_edge_costs,
+                               req.directed_in_costs)
+    _run_both(engine, oracle, req, rounds=4, groups="connections", clearance=1, via_keepout=1)
