@@ -91,14 +91,15 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // at -x, +x, -y, +y, the layer below and the layer above.
 enum { kFromNegX = 0, kFromPosX = 1, kFromNegY = 2, kFromPosY = 3, kFromBelow = 4, kFromAbove = 5 };
 
-template <int TH>
+template <int TH, bool FB>  // FB: fell marks as bytes (the price-plane kernels)
 struct Tile {
     u64 *lab;        // [L][TH+2][34] labels with a one-cell halo ring
     uint32_t *st;    // [6][L][TH][sp] step prices into interior cells (column x at sp-offset xo + x)
     uint8_t *rowd;   // [L][TH] row needs a sweep
     uint8_t *cold;   // [L][32] column needs a sweep
     uint8_t *stackd; // [TH][32] layer stack needs a sweep
-    uint32_t *fellw; // [L][TH] bit x: the label of (l, y, x) fell in this activation
+    uint32_t *fellw; // [L][TH] bit x: the label of (l, y, x) fell in this activation (staged prices), or
+    uint8_t *fellb;  // [L][TH][32] 1 = it fell (price planes: plain byte stores, no shared atomics)
     uint8_t *fl;     // [L][TH+2][kFlPitch] board flag bytes of the tile and its halo (computed prices only)
     uint32_t L;
     uint32_t sp, xo; // price row pitch and column offset: 32, 0 computed; kPlaneTmaBoxW, tx0 & 3 from the planes
@@ -109,7 +110,8 @@ struct Tile {
         return ((plane * L + l) * TH + y) * sp + x + xo;
     }
     __device__ __forceinline__ void fell(uint32_t l, uint32_t y, uint32_t x) const {
-        atomicOr(&fellw[l * TH + y], 1u << x);
+        if constexpr (FB) fellb[(l * TH + y) * kTW + x] = 1;
+        else atomicOr(&fellw[l * TH + y], 1u << x);
     }
     // a label of interior cell (l, y, x) fell: every other line through it must be swept again
     __device__ __forceinline__ void touched_by_row(uint32_t l, uint32_t y, uint32_t x) const {
@@ -288,8 +290,8 @@ __device__ __forceinline__ bool via_blocked(const DevField &f, const uint32_t *p
     return (cell_tile_flags(f, pads, gcell, gf) & kViaBlocked) != 0;
 }
 
-template <int TH>
-__device__ __forceinline__ bool stack_pass(const Tile<TH> &t);
+template <int TH, bool FB>
+__device__ __forceinline__ bool stack_pass(const Tile<TH, FB> &t);
 
 // With 8-row tiles and 4 cells per lane, the row lanes of a layer (8 rows x 8
 // lanes) and its column lanes (32 columns x 2 lanes) fall on the same pair of
@@ -303,8 +305,8 @@ __device__ __forceinline__ void pair_barrier() {
 // One sweep of a staged tile: rows (4 lanes x 8 cells), columns (TH/8 lanes x
 // 8 cells), layer stacks (one thread each), each forward then backward, only
 // over lines whose dirty flag is set.
-template <int TH>
-__device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
+template <int TH, bool FB>
+__device__ __forceinline__ bool relax_tile(const Tile<TH, FB> &t) {
     constexpr int KC = kLaneCells;          // cells per lane in a line pass
     constexpr int SR = 32 / KC, SC = TH / KC;  // lanes per row / per column
     const uint32_t L = t.L;
@@ -343,7 +345,7 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
         [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, pos, line % 32); });
     if (L > 1) {
         __syncthreads();
-        ch |= stack_pass<TH>(t);
+        ch |= stack_pass<TH, FB>(t);
     }
     return ch;
 }
@@ -354,8 +356,8 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH> &t) {
 // shared memory.
 constexpr uint32_t kStackRegs = 4;
 
-template <int TH>
-__device__ __forceinline__ bool stack_pass(const Tile<TH> &t) {
+template <int TH, bool FB>
+__device__ __forceinline__ bool stack_pass(const Tile<TH, FB> &t) {
     const uint32_t L = t.L;
     bool ch = false;
     for (uint32_t r = threadIdx.x; r < TH * 32; r += blockDim.x) {
@@ -442,8 +444,10 @@ __host__ __device__ inline TileLayout tile_layout(uint32_t L, uint32_t TH, bool 
     const size_t sp = planes ? kPlaneTmaBoxW : kStPitch;
     o.st = ((size_t)L * (TH + 2) * kLabPitch * 8 + 127) & ~(size_t)127;  // TMA destination: 128-byte aligned
     o.rowd = o.st + (size_t)6 * L * TH * sp * 4;
+    // fell marks: bytes with the price planes (their tiles fit the same CTAs per SM
+    // either way), bits otherwise
     o.fellw = (o.rowd + (size_t)L * TH + (size_t)L * kTW + (size_t)TH * kTW + 3) & ~(size_t)3;
-    o.fl = o.fellw + (size_t)L * TH * 4;
+    o.fl = o.fellw + (size_t)L * TH * (planes ? kTW : 4);
     o.total = o.fl + (planes ? 0 : (size_t)L * (TH + 2) * kFlPitch);
     return o;
 }
@@ -493,7 +497,7 @@ template <int TH, bool ASYNC, bool PL, bool OV>
 __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, uint32_t t, uint32_t round,
                                              unsigned char *smem_raw, uint64_t *mbar, uint32_t &tma_phase) {
     const uint32_t SW = kTW + 2, SH = TH + 2;
-    Tile<TH> tile;
+    Tile<TH, PL> tile;
     __shared__ uint32_t s_push[4];
     __shared__ uint32_t s_vis[5];  // self, left, right, top, bottom
     __shared__ uint32_t s_pads[kPadCache], s_vpads[kVPadCache];
@@ -514,6 +518,8 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     tile.cold = tile.rowd + L * TH;
     tile.stackd = tile.cold + L * kTW;
     tile.fellw = reinterpret_cast<uint32_t *>(smem_raw + lay.fellw);
+    tile.fellb = PL ? smem_raw + lay.fellw : nullptr;
+    const uint32_t fell_words = L * TH * (PL ? kTW / 4 : 1);  // words of fell marks to clear
     tile.fl = smem_raw + lay.fl;
     tile.L = L;
     tile.sp = PL ? kPlaneTmaBoxW : kStPitch;
@@ -564,7 +570,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     // +inf labels with +inf ends cannot change until a crossing line lowers one
     // of its cells, and that pass marks it.
     for (uint32_t i = tid; i < L * TH + L * kTW + TH * kTW; i += blockDim.x) tile.rowd[i] = 0;
-    for (uint32_t i = tid; i < L * TH; i += blockDim.x) tile.fellw[i] = 0;
+    for (uint32_t i = tid; i < fell_words; i += blockDim.x) tile.fellw[i] = 0;
     __syncthreads();
 
     // ---- step prices into every interior cell: phase 1 -----------------
@@ -783,7 +789,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     for (uint32_t cont = 0;; ++cont) {
         uint32_t sweep = 0;
         for (;;) {
-            const bool ch = relax_tile<TH>(tile);
+            const bool ch = relax_tile<TH, PL>(tile);
             ++sweep;
             const int any = __syncthreads_or(ch ? 1 : 0);
             if (!any) break;
@@ -803,7 +809,8 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         for (uint32_t i = tid; i < L * TH * kTW; i += blockDim.x) {
             const uint32_t tx = i % kTW, r = i / kTW, ty = r % TH, l = r / TH;
             if (tx >= tw || ty >= th) continue;
-            if (!all_labels && !((tile.fellw[l * TH + ty] >> tx) & 1u)) continue;
+            if (!all_labels && !(PL ? tile.fellb[(l * TH + ty) * kTW + tx] : (tile.fellw[l * TH + ty] >> tx) & 1u))
+                continue;
             const uint64_t lc = ((uint64_t)l * f.wh + (uint32_t)(ty0 - wy0) + ty) * f.ww + (uint32_t)(tx0 - wx0) + tx;
             labw[lc] = tile.lab[tile.li(l, ty + 1, tx + 1)];
         }
@@ -933,7 +940,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             if (!s_more) break;
             __threadfence();  // the neighbours' labels were written before they marked this tile
             if (tid < 4) s_push[tid] = 0;
-            for (uint32_t i = tid; i < L * TH; i += blockDim.x) tile.fellw[i] = 0;
+            for (uint32_t i = tid; i < fell_words; i += blockDim.x) tile.fellw[i] = 0;
             // the halo ring again: an improved cell marks the line that ends at it
             const uint32_t nr = 2 * L * TH + 2 * L * kTW;
             for (uint32_t i = tid; i < nr; i += blockDim.x) {
