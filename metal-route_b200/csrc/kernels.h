@@ -12,6 +12,7 @@ namespace mrc {
 
 constexpr int kRelaxThreads = 256;  // default CTA width of the relax kernel
 constexpr uint64_t kTilesPerCta = 8;  // tiles per CTA at which a queue launch can use one more CTA
+constexpr uint32_t kCountBatch = 64;    // activations a queue CTA counts locally before adding them to the launch's
 constexpr uint32_t kContinueLimit = 4;  // activations of one held tile before it goes back to the queue
 
 // Status bits reported through Ctl::status / PathArgs::status.

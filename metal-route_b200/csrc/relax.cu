@@ -495,7 +495,8 @@ static __device__ __noinline__ void stage_overrides(const DevBoard &b, const Dev
 // lookups is compiled in.
 template <int TH, bool ASYNC, bool PL, bool OV>
 __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, uint32_t t, uint32_t round,
-                                             unsigned char *smem_raw, uint64_t *mbar, uint32_t &tma_phase) {
+                                             unsigned char *smem_raw, uint64_t *mbar, uint32_t &tma_phase,
+                                             unsigned long long *s_cnt) {
     const uint32_t SW = kTW + 2, SH = TH + 2;
     Tile<TH, PL> tile;
     __shared__ uint32_t s_push[4];
@@ -901,14 +902,24 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             __threadfence();  // labels before the visited flag and the queue entries
             if (tid == 4) {
                 if constexpr (ASYNC) {
-                    if (!__ldcg(a.tvisit + f.tile_off + t)) atomicExch(a.tvisit + f.tile_off + t, 1u);
-                    if (atomicAdd(&ctl->activations, 1ull) >= a.activation_limit)
-                        atomicOr(&ctl->status, kStatusActivationLimit);
+                    // nothing reads the visited words during a queue launch: a plain
+                    // store; the work counters are per CTA (s_cnt), added to the
+                    // launch's every kCountBatch activations and when the CTA exits,
+                    // so this thread makes no round trip to L2 here
+                    a.tvisit[f.tile_off + t] = 1u;
+                    s_cnt[1] += sweep;
+                    if (++s_cnt[0] == kCountBatch) {
+                        if (atomicAdd(&ctl->activations, (unsigned long long)kCountBatch) + kCountBatch >
+                            a.activation_limit)
+                            atomicOr(&ctl->status, kStatusActivationLimit);
+                        atomicAdd(&ctl->sweeps, s_cnt[1]);
+                        s_cnt[0] = s_cnt[1] = 0;
+                    }
                 } else {
                     if (!s_vis[0]) atomicExch(a.tvisit + f.tile_off + t, 1u);
                     atomicAdd(&ctl->activations, 1ull);
+                    atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
                 }
-                atomicAdd(&ctl->sweeps, (unsigned long long)sweep);
             } else if (s_push[tid]) {
                 const uint32_t u = tid == 0 ? t - 1 : tid == 1 ? t + 1 : tid == 2 ? t - ntx : t + ntx;
                 if constexpr (ASYNC) {
@@ -1031,7 +1042,7 @@ __global__ void __launch_bounds__(NT) relax_rounds_kernel(RelaxArgs a) {
             if (item == kInf) break;
             uint32_t no_phase = 0;
             process_item<TH, false, false, OV>(a, (uint32_t)(item >> 32), (uint32_t)item, round, smem_raw, nullptr,
-                                           no_phase);
+                                               no_phase, nullptr);
         }
         grid_barrier(ctl, gridDim.x);
     }
@@ -1048,20 +1059,27 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 64)) relax_async_kernel(Rela
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ u64 s_item;
     __shared__ __align__(8) uint64_t s_mbar;  // completion of the price-plane TMA loads (PL)
+    __shared__ unsigned long long s_cnt[2];  // this CTA's activations and sweeps not yet added to the launch's
     uint32_t tma_phase = 0;
-    if (PL) {
-        if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {
+        s_cnt[0] = s_cnt[1] = 0;
+        if (PL) {
             mbar_init(&s_mbar, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
-        __syncthreads();
     }
+    __syncthreads();
     for (;;) {
         if (threadIdx.x == 0) s_item = async_pop(a);
         __syncthreads();
         const u64 item = s_item;
         if (item == kInf) break;
-        process_item<TH, true, PL, OV>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw, &s_mbar, tma_phase);
+        process_item<TH, true, PL, OV>(a, (uint32_t)(item >> 32), (uint32_t)item, 0, smem_raw, &s_mbar, tma_phase,
+                                       s_cnt);
+    }
+    if (threadIdx.x == 0) {
+        if (s_cnt[0]) atomicAdd(&a.ctl->activations, s_cnt[0]);
+        if (s_cnt[1]) atomicAdd(&a.ctl->sweeps, s_cnt[1]);
     }
 }
 
