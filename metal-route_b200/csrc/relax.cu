@@ -943,9 +943,22 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             break;
         } else {
             if (tid == 0) {
+                // its own pushes are counted (the barrier above): release the tile
+                // with one atomic, or, if a neighbour improved it meanwhile, hold it
+                // again and continue, or queue it once more past the limit
                 __threadfence();
-                s_more = cont + 1 < kContinueLimit &&
-                         atomicCAS(a.tstamp + f.tile_off + t, kTileHeldDirty, kTileHeld) == kTileHeldDirty;
+                uint32_t *stw = a.tstamp + f.tile_off + t;
+                s_more = 0;
+                if (atomicCAS(stw, kTileHeld, kTileIdle) != kTileHeld) {  // held and dirty
+                    if (cont + 1 < kContinueLimit) {
+                        atomicExch(stw, kTileHeld);
+                        s_more = 1;
+                    } else {
+                        atomicExch(stw, kTileQueued);
+                        async_enqueue(a, fi, t);
+                    }
+                }
+                if (!s_more) async_done(ctl);  // this item leaves the in-flight count
             }
             __syncthreads();
             if (!s_more) break;
@@ -984,14 +997,7 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
             __syncthreads();
         }
     }
-    __syncthreads();
-    if constexpr (ASYNC) {
-        if (tid == 0) {  // this item is done: its own pushes are already counted
-            __threadfence();
-            async_release(a, fi, f.tile_off, t);
-            atomicSub(&ctl->count[1], 1u);
-        }
-    }
+    __syncthreads();  // (queue form: the tile was released, or queued again, inside the loop)
 }
 
 template <int TH, int NT, bool OV>

@@ -79,6 +79,9 @@ __device__ __forceinline__ void async_release(const RelaxArgs &a, uint32_t fi, u
     }
 }
 
+// An item is done: it leaves the in-flight count (after its own pushes were counted).
+__device__ __forceinline__ void async_done(Ctl *c) { atomicSub(&c->count[1], 1u); }
+
 // Next item for the calling worker (one thread), or kInf when no work is left.  The
 // wait is bounded: kQueueSpinLimit polls, then kStatusBarrier and an exit.
 __device__ __forceinline__ u64 async_pop(const RelaxArgs &a) {
