@@ -39,9 +39,10 @@ __device__ __forceinline__ u64 umin64(u64 a, u64 b) { return a < b ? a : b; }
 constexpr uint32_t kQueueSpinLimit = 1u << 24;  // polls of one wait (~16 s with the backoff below)
 
 // Tile states in the tstamp word: 0 idle, 1 queued, 2 held by a worker,
-// 3 held and improved again meanwhile (the holder queues it once more when it
-// finishes, so improvements that arrive during a relaxation share one
-// re-activation and no tile is ever relaxed by two workers at once).
+// 3 held and improved again meanwhile (the holder continues it in place, or
+// queues it once more, when it finishes, so improvements that arrive during a
+// relaxation share one re-activation and no tile is ever relaxed by two
+// workers at once).
 constexpr uint32_t kTileIdle = 0, kTileQueued = 1, kTileHeld = 2, kTileHeldDirty = 3;
 
 __device__ __forceinline__ void async_enqueue(const RelaxArgs &a, uint32_t fi, uint32_t u) {
