@@ -302,8 +302,8 @@ __device__ __forceinline__ void pair_barrier() {
     asm volatile("bar.sync %0, 64;" ::"r"(1u + (threadIdx.x >> 6)) : "memory");
 }
 
-// One sweep of a staged tile: rows (4 lanes x 8 cells), columns (TH/8 lanes x
-// 8 cells), layer stacks (one thread each), each forward then backward, only
+// One sweep of a staged tile: rows (8 lanes x 4 cells), columns (TH/4 lanes x
+// 4 cells), layer stacks (one thread each), each forward then backward, only
 // over lines whose dirty flag is set.
 template <int TH, bool FB>
 __device__ __forceinline__ bool relax_tile(const Tile<TH, FB> &t) {
