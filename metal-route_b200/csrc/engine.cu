@@ -722,6 +722,9 @@ struct mrc_batch {
     DBuf d_planes, d_pchunks;    // step-price planes of every board, chunk table of their kernel
     DBuf d_tmaps;                // one TMA tensor map per board over its planes (CTA queue form)
     uint64_t n_pchunks = 0;
+    // the planes hold prices of the batch's boards, which never change: computed by
+    // the first launch after a layout and kept for the launches that follow
+    bool planes_valid = false;
     ~mrc_batch() {
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
@@ -798,6 +801,7 @@ mrc_status batch_layout(mrc_batch *bt, uint32_t tile_h, uint32_t threads) {
         cudaGraphExecDestroy(bt->graph);
         bt->graph = nullptr;
     }
+    bt->planes_valid = false;
     if (bt->warp && bt->max_layers > kWarpMaxLayers) bt->warp = false;  // too many layers for one warp tile
     if (bt->has_over) {  // per-net price overrides: CTA tiles of one shape (the kernels compiled with them)
         if (bt->warp) {
@@ -1041,11 +1045,14 @@ mrc_status batch_enqueue(mrc_batch *bt, cudaStream_t st, bool capturing) {
         const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
         if (bt->ev0) MRC_CUDA(cudaEventRecordWithFlags(bt->ev0, st, rec), "record event");
         const bool cta_pl = bt->async_q && !bt->warp && bt->cta_planes;
-        if (bt->warp || cta_pl) {
+        if ((bt->warp || cta_pl) && !bt->planes_valid) {
             MRC_CUDA(planes_launch(bt->d_boards.as<DevBoard>(), bt->d_pchunks.as<uint64_t>(),
                                    (uint32_t)bt->devs.size(), bt->n_pchunks, (uint32_t)bt->ctx->sms, st),
                      "launch step-price planes");
             launches += 1;
+            // a captured graph recomputes them on every replay (it is captured with
+            // valid planes, see mrc_batch_capture_graph, so this is the fallback)
+            if (!capturing) bt->planes_valid = true;
         }
         if (bt->warp) {
             MRC_CUDA(warp_relax_launch(ra, bt->grid, st), "launch relax kernel");
@@ -1541,6 +1548,16 @@ mrc_status mrc_batch_capture_graph(mrc_context *ctx, mrc_batch *batch) {
     if (batch->graph) {
         cudaGraphExecDestroy(batch->graph);
         batch->graph = nullptr;
+    }
+    // the boards' price planes first, outside the graph: they stay valid for
+    // every replay of this layout
+    const bool cta_pl = batch->async_q && !batch->warp && batch->cta_planes;
+    if ((batch->warp || cta_pl) && !batch->planes_valid && !batch->fields.empty()) {
+        MRC_CUDA(planes_launch(batch->d_boards.as<DevBoard>(), batch->d_pchunks.as<uint64_t>(),
+                               (uint32_t)batch->devs.size(), batch->n_pchunks, (uint32_t)ctx->sms, ctx->stream),
+                 "launch step-price planes");
+        MRC_CUDA(cudaStreamSynchronize(ctx->stream), "step-price planes");
+        batch->planes_valid = true;
     }
     cudaStream_t cs = nullptr;
     MRC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");

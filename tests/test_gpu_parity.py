@@ -225,10 +225,11 @@ def test_deterministic_across_calls_and_batches(engine):
         batch.launch()
         c = batch.finish()
         assert c.paths == a.paths and c.search_costs == a.search_costs
-    # relax, path offsets, path walk (+ the seed kernel of the queue schedules,
-    # + the price-plane kernel of the queue and warp schedules that read planes)
+    # relax, path offsets, path walk (+ the seed kernel of the queue schedules;
+    # the price planes of the schedules that read them were computed by the
+    # first launch of this layout and are not launched again)
     sched = batch.config()["schedule"]
-    assert batch.kernel_launches == 3 + {0: 0, 1: 2, 2: 2, 3: 1}[sched]
+    assert batch.kernel_launches == 3 + {0: 0, 1: 1, 2: 1, 3: 1}[sched]
     # every configuration the autotuner tries computes the same answer (on a
     # context of its own, so the tuned choice does not steer the other tests)
     e2 = mrcuda.Engine(0)
