@@ -302,6 +302,53 @@ __device__ __forceinline__ void pair_barrier() {
     asm volatile("bar.sync %0, 64;" ::"r"(1u + (threadIdx.x >> 6)) : "memory");
 }
 
+// The row and the column pass of a sweep on their own (the reversed sweep's).
+template <int TH, bool FB>
+__device__ __forceinline__ bool row_pass(const Tile<TH, FB> &t) {
+    constexpr int KC = kLaneCells, SR = 32 / KC;  // cells per lane, lanes per row
+    return seg_pass<KC, SR>(
+        t.lab, t.st, t.rowd, t.L * TH,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *sf, uint32_t *sb) {
+            const uint32_t l = line / TH, y = line % TH;
+            *li = t.li(l, y + 1, pos + 1);
+            *sf = t.si(kFromNegX, l, y, pos);
+            *sb = t.si(kFromPosX, l, y, pos);
+        },
+        [&](uint32_t line, uint32_t *hf, uint32_t *hb) {
+            *hf = t.li(line / TH, line % TH + 1, 0);
+            *hb = t.li(line / TH, line % TH + 1, 33);
+        },
+        [&](uint32_t line, uint32_t pos) { t.touched_by_row(line / TH, line % TH, pos); });
+}
+
+template <int TH, bool FB>
+__device__ __forceinline__ bool col_pass(const Tile<TH, FB> &t) {
+    constexpr int KC = kLaneCells, SC = TH / KC;  // cells per lane, lanes per column
+    return seg_pass<KC, SC>(
+        t.lab, t.st, t.cold, t.L * 32,
+        [&](uint32_t line, uint32_t pos, uint32_t *li, uint32_t *sf, uint32_t *sb) {
+            const uint32_t l = line / 32, x = line % 32;
+            *li = t.li(l, pos + 1, x + 1);
+            *sf = t.si(kFromNegY, l, pos, x);
+            *sb = t.si(kFromPosY, l, pos, x);
+        },
+        [&](uint32_t line, uint32_t *hf, uint32_t *hb) {
+            *hf = t.li(line / 32, 0, line % 32 + 1);
+            *hb = t.li(line / 32, TH + 1, line % 32 + 1);
+        },
+        [&](uint32_t line, uint32_t pos) { t.touched_by_col(line / 32, pos, line % 32); });
+}
+
+// rows <-> columns: only the warps of the same layers exchange data
+template <int TH>
+__device__ __forceinline__ void plane_barrier() {
+    if constexpr (TH == 8 && kLaneCells == 4) {
+        pair_barrier();
+    } else {
+        __syncthreads();
+    }
+}
+
 // One sweep of a staged tile: rows (8 lanes x 4 cells), columns (TH/4 lanes x
 // 4 cells), layer stacks (one thread each), each forward then backward, only
 // over lines whose dirty flag is set.
@@ -347,6 +394,21 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH, FB> &t) {
         __syncthreads();
         ch |= stack_pass<TH, FB>(t);
     }
+    return ch;
+}
+
+// The same passes in the opposite order (stacks, columns, rows); the rounds
+// form alternates the two orders between sweeps.
+template <int TH, bool FB>
+__device__ __forceinline__ bool relax_tile_rev(const Tile<TH, FB> &t) {
+    bool ch = false;
+    if (t.L > 1) {
+        ch = stack_pass<TH, FB>(t);
+        __syncthreads();
+    }
+    ch |= col_pass(t);
+    plane_barrier<TH>();
+    ch |= row_pass(t);
     return ch;
 }
 
@@ -790,7 +852,12 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
     for (uint32_t cont = 0;; ++cont) {
         uint32_t sweep = 0;
         for (;;) {
-            const bool ch = relax_tile<TH, PL>(tile);
+            // the rounds form alternates the pass order between sweeps (fewer
+            // sweeps on the one-activation tiles it runs); the queue form keeps
+            // rows first, where alternation costs sweeps
+            bool ch;
+            if constexpr (!ASYNC) ch = (sweep & 1) ? relax_tile_rev(tile) : relax_tile(tile);
+            else ch = relax_tile(tile);
             ++sweep;
             const int any = __syncthreads_or(ch ? 1 : 0);
             if (!any) break;
