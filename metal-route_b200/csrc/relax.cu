@@ -397,6 +397,20 @@ __device__ __forceinline__ bool relax_tile(const Tile<TH, FB> &t) {
     return ch;
 }
 
+// Columns first, then rows and stacks: the queue form's order (fewer sweeps per
+// activation than rows first on its 32 x 8 tiles).
+template <int TH, bool FB>
+__device__ __forceinline__ bool relax_tile_cols_first(const Tile<TH, FB> &t) {
+    bool ch = col_pass(t);
+    plane_barrier<TH>();
+    ch |= row_pass(t);
+    if (t.L > 1) {
+        __syncthreads();
+        ch |= stack_pass<TH, FB>(t);
+    }
+    return ch;
+}
+
 // The same passes in the opposite order (stacks, columns, rows); the rounds
 // form alternates the two orders between sweeps.
 template <int TH, bool FB>
@@ -853,11 +867,11 @@ __device__ __forceinline__ void process_item(const RelaxArgs &a, uint32_t fi, ui
         uint32_t sweep = 0;
         for (;;) {
             // the rounds form alternates the pass order between sweeps (fewer
-            // sweeps on the one-activation tiles it runs); the queue form keeps
-            // rows first, where alternation costs sweeps
+            // sweeps on the one-activation tiles it runs); the queue form runs
+            // columns first, where alternation costs sweeps
             bool ch;
             if constexpr (!ASYNC) ch = (sweep & 1) ? relax_tile_rev(tile) : relax_tile(tile);
-            else ch = relax_tile(tile);
+            else ch = relax_tile_cols_first(tile);
             ++sweep;
             const int any = __syncthreads_or(ch ? 1 : 0);
             if (!any) break;
