@@ -995,6 +995,9 @@ PathArgs path_args(const mrc_batch *bt) {
     pa.tover = bt->has_over ? bt->d_tover.as<uint8_t>() : nullptr;
     pa.tile_h = bt->tile_h;
     pa.arena_filled = bt->async_q ? 1u : 0u;
+    const bool cta_pl = bt->async_q && !bt->warp && bt->cta_planes;
+    const size_t ws = walk_smem_bytes(bt->max_layers, bt->tile_h);
+    pa.walk_smem = (cta_pl && !bt->has_over && ws <= kWalkSmemLimit) ? (uint32_t)ws : 0u;
     pa.costs = bt->d_costs.as<uint32_t>();
     pa.lens = bt->d_lens.as<uint32_t>();
     pa.offsets = bt->d_offsets.as<unsigned long long>();

@@ -50,6 +50,7 @@ struct PathArgs {
     const uint8_t *tover;            // nullable: as RelaxArgs::tover
     uint32_t tile_h;
     uint32_t arena_filled;           // 1: the label arena was +inf-filled (queue schedule), tvisit not needed
+    uint32_t walk_smem;              // > 0: the tile-staged walk (price planes + TMA maps, no overrides), its smem
     uint32_t *costs;                 // [n] by output slot
     uint32_t *lens;                  // [n] by output slot
     unsigned long long *offsets;     // [n+1] by output slot
@@ -210,6 +211,17 @@ cudaError_t warp_relax_launch(const RelaxArgs &a, uint32_t grid, cudaStream_t st
 // the tile's 32 columns plus the slack of rounding its first column down to a
 // multiple of 4 (16 bytes, the TMA rule for the innermost coordinate).
 constexpr uint32_t kPlaneTmaBoxW = 36;
+// Tile-staged path walk: tiles of 32 x walk_tile_rows cells over all layers,
+// their price planes brought by TMA loads of the relax kernel's box.
+constexpr uint32_t kWalkRows = 16;          // walk tile rows (at least the relax tile height)
+constexpr size_t kWalkSmemLimit = 200u << 10;  // larger tiles take the per-step walk
+__host__ __device__ inline uint32_t walk_tile_rows(uint32_t tile_h) { return tile_h > kWalkRows ? tile_h : kWalkRows; }
+__host__ __device__ inline size_t walk_smem_planes(uint32_t layers, uint32_t tile_h) {
+    return (size_t)(walk_tile_rows(tile_h) / tile_h) * 6 * layers * tile_h * kPlaneTmaBoxW * 4;
+}
+__host__ __device__ inline size_t walk_smem_bytes(uint32_t layers, uint32_t tile_h) {
+    return walk_smem_planes(layers, tile_h) + (size_t)layers * (walk_tile_rows(tile_h) + 2) * 34 * 8;
+}
 // Rows of a price plane are padded to a multiple of 4 cells (16 bytes), so a
 // tensor map over the planes has 16-byte strides.
 __host__ __device__ inline uint32_t planes_pitch(uint32_t w) { return (w + 3u) & ~3u; }

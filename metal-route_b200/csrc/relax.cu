@@ -1698,6 +1698,142 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
     return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
+// Tile-staged walk, for batches whose boards carry price planes and a TMA map
+// (the CTA queue form) and whose nets carry no price overrides.  One CTA per
+// field stages a walk tile of 32 x WH cells over all layers — the labels with a
+// one-cell ring by plain loads, the six price planes by WH / tile_h TMA loads of
+// the relax kernel's box — and warp 0 walks inside it from shared memory,
+// re-staging when the path leaves the tile.  A step then costs shared-memory
+// reads instead of a round trip to L2 or HBM.  The step prices are the planes'
+// except on the stacks of the net's endpoints, and for every step of a net with
+// own or via pads, where walk_step prices exactly; the choice among the
+// candidates is path_walk_kernel's.
+__global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
+    extern __shared__ __align__(128) unsigned char wsm[];
+    __shared__ __align__(8) uint64_t s_mbar;
+    __shared__ int s_tile[2];   // walk tile origin (board x, y)
+    __shared__ uint32_t s_done;
+    const DevField f = a.fields[blockIdx.x];
+    const uint32_t len = a.lens[f.out];
+    if (len == 0) return;  // the same for the whole CTA
+    const DevBoard b = a.boards[f.board];
+    const uint32_t L = b.layers, TH = a.tile_h, WH = walk_tile_rows(TH), nload = WH / TH;
+    const uint32_t plane = b.w * b.h;
+    uint32_t *pl = reinterpret_cast<uint32_t *>(wsm);
+    u64 *lab = reinterpret_cast<u64 *>(wsm + walk_smem_planes(L, TH));
+    const uint32_t box_words = 6 * L * TH * kPlaneTmaBoxW;
+    const bool exact_all = (f.n_pads | f.n_vpads) != 0;
+    const uint32_t src_xy = f.src % plane, dst_xy = f.dst % plane;
+    const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t *out = a.cells + a.offsets[f.out];
+    // walk state (warp 0)
+    uint32_t cur = f.dst, pos = len - 1;
+    int cx = (int)((f.dst % plane) % b.w), cy = (int)((f.dst % plane) / b.w), cl = (int)(f.dst / plane);
+    u64 need = a.lab[f.lab_off + ((uint64_t)(uint32_t)cl * f.wh + (uint32_t)(cy - wy0)) * f.ww + (uint32_t)(cx - wx0)];
+    uint32_t phase = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&s_mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_tile[0] = wx0 + (cx - wx0) / (int)kTW * (int)kTW;
+        s_tile[1] = wy0 + (cy - wy0) / (int)WH * (int)WH;
+        s_done = 0;
+    }
+    for (;;) {
+        __syncthreads();
+        const int tx0 = s_tile[0], ty0 = s_tile[1];
+        const uint32_t xo = (uint32_t)tx0 & 3u;
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            mbar_expect_tx(&s_mbar, nload * box_words * 4u);
+            for (uint32_t j = 0; j < nload; ++j)
+                tma_load_4d(pl + j * box_words, b.tmap, tx0 & ~3, ty0 + (int)(j * TH), 0, 0, &s_mbar);
+        }
+        // labels of the tile and its ring (+inf outside the window)
+        const uint32_t nl = L * (WH + 2) * 34;
+        for (uint32_t i = threadIdx.x; i < nl; i += blockDim.x) {
+            const uint32_t sx = i % 34, r = i / 34, sy = r % (WH + 2), l = r / (WH + 2);
+            const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
+            u64 v = kInf;
+            if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1)
+                v = __ldcg(a.lab + f.lab_off + ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0));
+            lab[i] = v;
+        }
+        // bounded wait for the planes (a load that never lands breaks the path)
+        for (uint32_t spins = 0; !mbar_try_wait(&s_mbar, phase & 1u); ++spins) {
+            if (spins > kTmaSpinLimit) {
+                if (threadIdx.x == 0) {
+                    atomicOr(a.status, kStatusPathBroken);
+                    s_done = 1;
+                }
+                break;
+            }
+        }
+        ++phase;
+        __syncthreads();
+        if (s_done) return;
+        if (threadIdx.x < 32) {
+            for (;;) {
+                if (lane == 0) out[pos] = cur;
+                if (pos == 0) {
+                    if (lane == 0) {
+                        if (cur != f.src) atomicOr(a.status, kStatusPathBroken);
+                        s_done = 1;
+                    }
+                    break;
+                }
+                bool ok = false;
+                uint32_t p = 0;
+                u64 lp = kInf;
+                if (lane < 6) {
+                    int px = cx, py = cy, pz = cl;
+                    walk_offset((int)lane, px, py, pz);
+                    if (walk_inside(f, b, px, py, pz)) {
+                        p = ((uint32_t)pz * b.h + (uint32_t)py) * b.w + (uint32_t)px;
+                        lp = lab[((uint32_t)pz * (WH + 2) + (uint32_t)(py - ty0 + 1)) * 34 + (uint32_t)(px - tx0 + 1)];
+                        uint32_t st;
+                        const uint32_t cxy = cur % plane;
+                        if (exact_all || cxy == src_xy || cxy == dst_xy) {
+                            st = walk_step(b, f, a.pads, p, cur, (uint32_t)cx, (uint32_t)cy, (uint32_t)cl, (int)lane,
+                                           false);
+                        } else {
+                            // in-price plane of the move into cur from neighbour kind `lane`
+                            const int pin = lane == 0 ? kInBelow : lane == 1 ? kInNegY : lane == 2 ? kInNegX
+                                          : lane == 3 ? kInPosX : lane == 4 ? kInPosY : kInAbove;
+                            const uint32_t yy = (uint32_t)(cy - ty0), j = yy / TH;
+                            st = pl[j * box_words + (((uint32_t)pin * L + (uint32_t)cl) * TH + (yy - j * TH)) *
+                                                        kPlaneTmaBoxW + (uint32_t)(cx - tx0) + xo];
+                        }
+                        ok = lp != kInf && extend(lp, st) == need;
+                    }
+                }
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
+                if (m == 0) {
+                    if (lane == 0) {
+                        atomicOr(a.status, kStatusPathBroken);
+                        s_done = 1;
+                    }
+                    break;
+                }
+                const uint32_t win = __ffs(m) - 1;
+                cur = __shfl_sync(0xFFFFFFFFu, p, win);
+                need = __shfl_sync(0xFFFFFFFFu, lp, win);
+                walk_offset((int)win, cx, cy, cl);
+                --pos;
+                if (cx < tx0 || cx >= tx0 + (int)kTW || cy < ty0 || cy >= ty0 + (int)WH) {
+                    if (lane == 0) {  // the path left the tile: stage the one holding cur
+                        s_tile[0] = wx0 + (cx - wx0) / (int)kTW * (int)kTW;
+                        s_tile[1] = wy0 + (cy - wy0) / (int)WH * (int)WH;
+                    }
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_done) return;
+    }
+}
+
 namespace {
 // One warp per field: every override cell inside the window flags its tile.
 __global__ void mark_over_tiles_kernel(const DevField *fields, uint32_t n_fields, const DevBoard *boards,
@@ -1730,7 +1866,12 @@ cudaError_t path_launch(const PathArgs &a, cudaStream_t st) {
     path_offsets_kernel<<<1, 1024, 0, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (a.n_fields) {
+    if (a.n_fields && a.walk_smem) {
+        e = cudaFuncSetAttribute(path_walk_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)a.walk_smem);
+        if (e != cudaSuccess) return e;
+        path_walk_tiled_kernel<<<a.n_fields, 256, a.walk_smem, st>>>(a);
+    } else if (a.n_fields) {
         const uint32_t warps_per_block = 8;
         path_walk_kernel<<<(a.n_fields + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(a);
     }
