@@ -1708,6 +1708,17 @@ cudaError_t relax_launch(const RelaxArgs &a, uint32_t grid, uint32_t threads, si
 // except on the stacks of the net's endpoints, and for every step of a net with
 // own or via pads, where walk_step prices exactly; the choice among the
 // candidates is path_walk_kernel's.
+//
+// Origin of the walk tile along one axis of extent e for a walk at c heading in
+// direction d (-1, 0, +1): a few cells behind c, so most of the tile lies ahead.
+// A walk heading diagonally then leaves a tile through one side instead of two.
+__device__ __forceinline__ int walk_origin(int c, int d, int e) {
+    const int back = e / 8;
+    return d > 0 ? c - back : d < 0 ? c - (e - 1 - back) : c - e / 2;
+}
+
+__device__ __forceinline__ int walk_dir(int from, int to) { return to > from ? 1 : to < from ? -1 : 0; }
+
 __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
     extern __shared__ __align__(128) unsigned char wsm[];
     __shared__ __align__(8) uint64_t s_mbar;
@@ -1724,6 +1735,8 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
     const uint32_t box_words = 6 * L * TH * kPlaneTmaBoxW;
     const bool exact_all = (f.n_pads | f.n_vpads) != 0;
     const uint32_t src_xy = f.src % plane, dst_xy = f.dst % plane;
+    const int sx = (int)(src_xy % b.w), sy = (int)(src_xy / b.w);  // the walk heads for the source
+    const int dstx = (int)(dst_xy % b.w), dsty = (int)(dst_xy / b.w);
     const int wx0 = (int)f.x0, wy0 = (int)f.y0, wx1 = (int)(f.x0 + f.ww), wy1 = (int)(f.y0 + f.wh);
     const uint32_t lane = threadIdx.x & 31;
     uint32_t *out = a.cells + a.offsets[f.out];
@@ -1735,8 +1748,8 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
     if (threadIdx.x == 0) {
         mbar_init(&s_mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_tile[0] = wx0 + (cx - wx0) / (int)kTW * (int)kTW;
-        s_tile[1] = wy0 + (cy - wy0) / (int)WH * (int)WH;
+        s_tile[0] = walk_origin(cx, walk_dir(cx, sx), (int)kTW);
+        s_tile[1] = walk_origin(cy, walk_dir(cy, sy), (int)WH);
         s_done = 0;
     }
     for (;;) {
@@ -1749,15 +1762,25 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
             for (uint32_t j = 0; j < nload; ++j)
                 tma_load_4d(pl + j * box_words, b.tmap, tx0 & ~3, ty0 + (int)(j * TH), 0, 0, &s_mbar);
         }
-        // labels of the tile and its ring (+inf outside the window)
+        // labels of the tile and its ring (+inf outside the window), kStageBatch
+        // loads in flight per thread before any is stored
         const uint32_t nl = L * (WH + 2) * 34;
-        for (uint32_t i = threadIdx.x; i < nl; i += blockDim.x) {
-            const uint32_t sx = i % 34, r = i / 34, sy = r % (WH + 2), l = r / (WH + 2);
-            const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
-            u64 v = kInf;
-            if (gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1)
-                v = __ldcg(a.lab + f.lab_off + ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww + (uint32_t)(gx - wx0));
-            lab[i] = v;
+        constexpr uint32_t kStageBatch = 8;
+        for (uint32_t i0 = threadIdx.x; i0 < nl; i0 += kStageBatch * blockDim.x) {
+            u64 v[kStageBatch];
+#pragma unroll
+            for (uint32_t k = 0; k < kStageBatch; ++k) {
+                const uint32_t i = i0 + k * blockDim.x;
+                const uint32_t sx = i % 34, r = i / 34, sy = r % (WH + 2), l = r / (WH + 2);
+                const int gx = tx0 + (int)sx - 1, gy = ty0 + (int)sy - 1;
+                v[k] = kInf;
+                if (i < nl && gx >= wx0 && gx < wx1 && gy >= wy0 && gy < wy1)
+                    v[k] = __ldcg(a.lab + f.lab_off + ((uint64_t)l * f.wh + (uint32_t)(gy - wy0)) * f.ww +
+                                  (uint32_t)(gx - wx0));
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kStageBatch; ++k)
+                if (i0 + k * blockDim.x < nl) lab[i0 + k * blockDim.x] = v[k];
         }
         // bounded wait for the planes (a load that never lands breaks the path)
         for (uint32_t spins = 0; !mbar_try_wait(&s_mbar, phase & 1u); ++spins) {
@@ -1792,8 +1815,7 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
                         p = ((uint32_t)pz * b.h + (uint32_t)py) * b.w + (uint32_t)px;
                         lp = lab[((uint32_t)pz * (WH + 2) + (uint32_t)(py - ty0 + 1)) * 34 + (uint32_t)(px - tx0 + 1)];
                         uint32_t st;
-                        const uint32_t cxy = cur % plane;
-                        if (exact_all || cxy == src_xy || cxy == dst_xy) {
+                        if (exact_all || (cx == sx && cy == sy) || (cx == dstx && cy == dsty)) {
                             st = walk_step(b, f, a.pads, p, cur, (uint32_t)cx, (uint32_t)cy, (uint32_t)cl, (int)lane,
                                            false);
                         } else {
@@ -1821,9 +1843,11 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
                 walk_offset((int)win, cx, cy, cl);
                 --pos;
                 if (cx < tx0 || cx >= tx0 + (int)kTW || cy < ty0 || cy >= ty0 + (int)WH) {
-                    if (lane == 0) {  // the path left the tile: stage the one holding cur
-                        s_tile[0] = wx0 + (cx - wx0) / (int)kTW * (int)kTW;
-                        s_tile[1] = wy0 + (cy - wy0) / (int)WH * (int)WH;
+                    if (lane == 0) {  // the path left the tile: stage one ahead of cur
+                        const int dx = cx < tx0 ? -1 : cx >= tx0 + (int)kTW ? 1 : walk_dir(cx, sx);
+                        const int dy = cy < ty0 ? -1 : cy >= ty0 + (int)WH ? 1 : walk_dir(cy, sy);
+                        s_tile[0] = walk_origin(cx, dx, (int)kTW);
+                        s_tile[1] = walk_origin(cy, dy, (int)WH);
                     }
                     break;
                 }
