@@ -1745,6 +1745,14 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
     int cx = (int)((f.dst % plane) % b.w), cy = (int)((f.dst % plane) / b.w), cl = (int)(f.dst / plane);
     u64 need = a.lab[f.lab_off + ((uint64_t)(uint32_t)cl * f.wh + (uint32_t)(cy - wy0)) * f.ww + (uint32_t)(cx - wx0)];
     uint32_t phase = 0;
+    // Per-lane constants of a step: the neighbour offset of kind `lane` (lanes 0-5),
+    // the in-price plane of the move from it into the current cell, and the
+    // relax tile height as a shift (tile heights are powers of two).
+    int ox = 0, oy = 0, oz = 0;
+    if (lane < 6) walk_offset((int)lane, ox, oy, oz);
+    const uint32_t pin = lane == 0 ? kInBelow : lane == 1 ? kInNegY : lane == 2 ? kInNegX
+                       : lane == 3 ? kInPosX : lane == 4 ? kInPosY : kInAbove;
+    const uint32_t th_shift = (uint32_t)__ffs((int)TH) - 1u;
     if (threadIdx.x == 0) {
         mbar_init(&s_mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1808,26 +1816,21 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
                 bool ok = false;
                 uint32_t p = 0;
                 u64 lp = kInf;
-                if (lane < 6) {
-                    int px = cx, py = cy, pz = cl;
-                    walk_offset((int)lane, px, py, pz);
-                    if (walk_inside(f, b, px, py, pz)) {
-                        p = ((uint32_t)pz * b.h + (uint32_t)py) * b.w + (uint32_t)px;
-                        lp = lab[((uint32_t)pz * (WH + 2) + (uint32_t)(py - ty0 + 1)) * 34 + (uint32_t)(px - tx0 + 1)];
-                        uint32_t st;
-                        if (exact_all || (cx == sx && cy == sy) || (cx == dstx && cy == dsty)) {
-                            st = walk_step(b, f, a.pads, p, cur, (uint32_t)cx, (uint32_t)cy, (uint32_t)cl, (int)lane,
-                                           false);
-                        } else {
-                            // in-price plane of the move into cur from neighbour kind `lane`
-                            const int pin = lane == 0 ? kInBelow : lane == 1 ? kInNegY : lane == 2 ? kInNegX
-                                          : lane == 3 ? kInPosX : lane == 4 ? kInPosY : kInAbove;
-                            const uint32_t yy = (uint32_t)(cy - ty0), j = yy / TH;
-                            st = pl[j * box_words + (((uint32_t)pin * L + (uint32_t)cl) * TH + (yy - j * TH)) *
-                                                        kPlaneTmaBoxW + (uint32_t)(cx - tx0) + xo];
-                        }
-                        ok = lp != kInf && extend(lp, st) == need;
+                const int px = cx + ox, py = cy + oy, pz = cl + oz;
+                if (lane < 6 && walk_inside(f, b, px, py, pz)) {
+                    p = ((uint32_t)pz * b.h + (uint32_t)py) * b.w + (uint32_t)px;
+                    lp = lab[((uint32_t)pz * (WH + 2) + (uint32_t)(py - ty0 + 1)) * 34 + (uint32_t)(px - tx0 + 1)];
+                    uint32_t st;
+                    if (exact_all || (cx == sx && cy == sy) || (cx == dstx && cy == dsty)) {
+                        st = walk_step(b, f, a.pads, p, cur, (uint32_t)cx, (uint32_t)cy, (uint32_t)cl, (int)lane,
+                                       false);
+                    } else {
+                        // in-price plane `pin` at cur, from the TMA box of cur's relax-tile rows
+                        const uint32_t yy = (uint32_t)(cy - ty0), j = yy >> th_shift;
+                        st = pl[j * box_words + ((pin * L + (uint32_t)cl) * TH + (yy & (TH - 1u))) * kPlaneTmaBoxW +
+                                (uint32_t)(cx - tx0) + xo];
                     }
+                    ok = lp != kInf && extend(lp, st) == need;
                 }
                 const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
                 if (m == 0) {
@@ -1840,7 +1843,9 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
                 const uint32_t win = __ffs(m) - 1;
                 cur = __shfl_sync(0xFFFFFFFFu, p, win);
                 need = __shfl_sync(0xFFFFFFFFu, lp, win);
-                walk_offset((int)win, cx, cy, cl);
+                cx = __shfl_sync(0xFFFFFFFFu, px, win);
+                cy = __shfl_sync(0xFFFFFFFFu, py, win);
+                cl = __shfl_sync(0xFFFFFFFFu, pz, win);
                 --pos;
                 if (cx < tx0 || cx >= tx0 + (int)kTW || cy < ty0 || cy >= ty0 + (int)WH) {
                     if (lane == 0) {  // the path left the tile: stage one ahead of cur
