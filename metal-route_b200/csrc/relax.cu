@@ -1382,11 +1382,10 @@ __device__ __forceinline__ bool walk_inside(const DevField &f, const DevBoard &b
 // Is the neighbour `kind` of target t = (tx, ty, tl) a predecessor of t, i.e.
 // its label extended by the step into t equals `need`?  Its cell and label are
 // returned for the caller to carry forward.
+// (px, py, pl) is that neighbour, computed by the caller.
 __device__ __forceinline__ bool walk_try(const PathArgs &a, const DevField &f, const DevBoard &b, uint32_t ntx,
                                          uint32_t tile_shift, int tx, int ty, int tl, uint32_t t, u64 need, int kind,
-                                         uint32_t *q, u64 *lq) {
-    int px = tx, py = ty, pl = tl;
-    walk_offset(kind, px, py, pl);
+                                         int px, int py, int pl, uint32_t *q, u64 *lq) {
     if (!walk_inside(f, b, px, py, pl)) return false;
     *q = ((uint32_t)pl * b.h + (uint32_t)py) * b.w + (uint32_t)px;
     *lq = walk_label(a, f, ntx, tile_shift, px, py, pl);
@@ -1423,6 +1422,8 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
         cl = (int)(cur / plane);
     }
     u64 need = walk_label(a, f, ntx, tile_shift, cx, cy, cl);
+    int ox = 0, oy = 0, oz = 0;  // this lane's neighbour offset (lanes 0-5), a loop constant
+    if (lane < 6) walk_offset((int)lane, ox, oy, oz);
     for (uint32_t pos = len - 1;; --pos) {
         if (lane == 0) out[pos] = cur;
         if (pos == 0) {
@@ -1432,8 +1433,9 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
         bool ok = false;
         uint32_t p = 0;
         u64 lp = kInf;
+        const int px = cx + ox, py = cy + oy, pz = cl + oz;
         if (lane < 6) {
-            ok = walk_try(a, f, b, ntx, tile_shift, cx, cy, cl, cur, need, (int)lane, &p, &lp);
+            ok = walk_try(a, f, b, ntx, tile_shift, cx, cy, cl, cur, need, (int)lane, px, py, pz, &p, &lp);
         }
         const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
         if (m == 0) {
@@ -1443,7 +1445,9 @@ __global__ void __launch_bounds__(256) path_walk_kernel(PathArgs a) {
         const uint32_t win = __ffs(m) - 1;
         cur = __shfl_sync(0xFFFFFFFFu, p, win);
         need = __shfl_sync(0xFFFFFFFFu, lp, win);
-        walk_offset((int)win, cx, cy, cl);
+        cx = __shfl_sync(0xFFFFFFFFu, px, win);
+        cy = __shfl_sync(0xFFFFFFFFu, py, win);
+        cl = __shfl_sync(0xFFFFFFFFu, pz, win);
     }
 }
 
