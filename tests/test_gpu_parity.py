@@ -328,6 +328,48 @@ def test_queue_schedule_on_the_congestion_board(engine, oracle, tile_cfg):
     board.close()
 
 
+@pytest.mark.parametrize("directed", [False, True], ids=["axis", "directed"])
+@pytest.mark.parametrize("tile_cfg", [(8, 256), (16, 256), (32, 256)])
+def test_tiled_walk_board_edges_and_long_paths(engine, oracle, tile_cfg, directed):
+    """The queue form with price planes walks each path inside shared-memory
+    windows placed ahead of the walk, which may start left of or above the
+    board: nets between corners and along the edges of an open board, with
+    full-board windows and no own pads (so every step off the endpoints' stacks
+    reads the staged planes), must give the oracle's paths and costs."""
+    rng = np.random.default_rng(7 + tile_cfg[0] + int(directed))
+    w, h, layers = 150, 110, 3
+    dims = Dims(w, h, layers)
+    n = len(dims)
+    grid = Grid(dims, rng.integers(1, 4, n).astype(np.uint32), None, None)
+    x = rng.integers(1, 40, w - 1).astype(np.uint32)
+    y = rng.integers(1, 40, h - 1).astype(np.uint32)
+    vias = [7, 30]
+    d = rng.integers(1, 60, (n, 4)).astype(np.uint32) if directed else None
+
+    def cell(l, yy, xx):
+        return (l * h + yy) * w + xx
+
+    pairs = [(cell(0, 0, 0), cell(0, h - 1, w - 1)), (cell(0, h - 1, w - 1), cell(2, 0, 0)),
+             (cell(1, 0, w - 1), cell(1, h - 1, 0)), (cell(2, h - 1, 0), cell(0, 0, w - 1)),
+             (cell(0, 0, 3), cell(0, 0, w - 4)), (cell(1, 5, 0), cell(1, h - 6, 0)),
+             (cell(2, h - 1, 10), cell(2, h - 1, w - 11)), (cell(0, 40, w - 1), cell(2, 70, w - 1))]
+    nets = [NetEndpoints(f"edge{i}", s, t) for i, (s, t) in enumerate(pairs)]
+    wins = [IsolatedRouteWindow.full(dims) for _ in nets]
+    req = IsolatedRouteRequest(grid, nets, wins, x, y, vias, d)
+    exp = oracle.isolated_batch(req, retry_full=False, mode="field")
+    board = engine.board(grid, x, y, vias, d)
+    batch = mrcuda.Batch(board, nets, wins, retry_full=False)
+    batch.set_config(*tile_cfg)
+    batch.set_schedule(1)
+    batch.launch()
+    got = batch.finish()
+    assert (got.paths, got.search_costs) == exp, tile_cfg
+    assert all(p is not None and len(p) > 30 for p in got.paths)  # the shortest, a stack change, has 39-51 cells
+    assert batch.config()["schedule"] == 1
+    batch.close()
+    board.close()
+
+
 @pytest.mark.parametrize("layers", [1, 2, 3, 4, 5, 6, 8, 9, 12, 16])
 def test_warp_schedule_every_tile_geometry(engine, oracle, layers):
     """The warp schedule's tile width follows the layer count (4 * 32 /
