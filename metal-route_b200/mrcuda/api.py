@@ -919,12 +919,11 @@ class Engine:
 
     # -- the provider seam ---------------------------------------------------
     def _request(self, m: _Marshal, req: IsolatedRouteRequest) -> _Request:
+        """The C request for one board, written from numpy columns like the
+        instances' (no per-net ctypes objects); `m` keeps every buffer alive."""
         if len(req.windows) != len(req.nets):
             raise BackendUnavailable("isolated request windows are not net-aligned")
-        r = _Request(C.pointer(m.grid(req.grid)), m.nets(req.nets), len(req.nets), m.windows(req.windows),
-                     m.edges(req.x_edge_costs, req.y_edge_costs, req.via_edge_costs, req.directed_in_costs))
-        m.keep.append(r)
-        return r
+        return _marshal_requests(m, [req])[0]
 
     def route_isolated_batch(self, req: IsolatedRouteRequest, retry_full: bool = True, keep_fields: bool = False,
                              no_wait: bool = False) -> IsolatedBatchResult:
