@@ -1723,6 +1723,17 @@ __device__ __forceinline__ int walk_origin(int c, int d, int e) {
 
 __device__ __forceinline__ int walk_dir(int from, int to) { return to > from ? 1 : to < from ? -1 : 0; }
 
+// The exact step price, out of line: the tiled walk needs it only on the
+// endpoints' stacks and for nets with own pads, so its loads and branches stay
+// out of the common step's code.
+// It reads the board and field records from global memory (L1-resident after
+// the first call) so the caller's copies stay in registers.
+__device__ __noinline__ uint32_t walk_step_exact(const DevBoard *b, const DevField *f, const uint32_t *pads,
+                                                 uint32_t p, uint32_t cur, uint32_t x, uint32_t y, uint32_t l,
+                                                 int kind) {
+    return walk_step(*b, *f, pads, p, cur, x, y, l, kind, false);
+}
+
 __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
     extern __shared__ __align__(128) unsigned char wsm[];
     __shared__ __align__(8) uint64_t s_mbar;
@@ -1826,8 +1837,8 @@ __global__ void __launch_bounds__(256) path_walk_tiled_kernel(PathArgs a) {
                     lp = lab[((uint32_t)pz * (WH + 2) + (uint32_t)(py - ty0 + 1)) * 34 + (uint32_t)(px - tx0 + 1)];
                     uint32_t st;
                     if (exact_all || (cx == sx && cy == sy) || (cx == dstx && cy == dsty)) {
-                        st = walk_step(b, f, a.pads, p, cur, (uint32_t)cx, (uint32_t)cy, (uint32_t)cl, (int)lane,
-                                       false);
+                        st = walk_step_exact(a.boards + f.board, a.fields + blockIdx.x, a.pads, p, cur, (uint32_t)cx,
+                                             (uint32_t)cy, (uint32_t)cl, (int)lane);
                     } else {
                         // in-price plane `pin` at cur, from the TMA box of cur's relax-tile rows
                         const uint32_t yy = (uint32_t)(cy - ty0), j = yy >> th_shift;
